@@ -1,0 +1,341 @@
+"""Benchmark: DB residues x queries / s of blastp's two-hit word finding +
+ungapped X-drop extension on a B200.
+
+Workload (default): one 500-aa query vs 1,000,000 synthetic subjects
+(~360M residues, HBM-resident), BLOSUM62, word 3, T 11, window 40,
+x-drop 16 raw, cutoff 41 raw.  One step = one search of the query over the
+whole database through the engine (scan kernel + ordering of the HSP set +
+the count read-back).  The database (~0.36 GB) is larger than L2 (126 MB), so
+no explicit flush is needed between steps.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
+
+With N > 1 (launched by torch.distributed.run) each rank scans its own
+1,000,000-subject shard (weak scaling, no collective on the data path); the
+timed region is bracketed by barriers and the max over ranks is reported.
+`--impl reference` times the reference algorithm's CPU implementation on the
+host cores (the oracle port: the reference itself cannot be built here).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "blastp-cuda_b200"))
+sys.path.insert(0, ROOT)
+
+METRIC = "DB residues x queries / s (two-hit + ungapped X-drop, bit-exact HSPs)"
+UNIT = "residues*queries/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--subjects", type=int, default=1_000_000)
+    ap.add_argument("--qlen", type=int, default=500)
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--cpu-seconds", type=float, default=3.0, help="wall-clock budget of the CPU baseline sample")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def load_workload(matrix, rank, n_subjects, qlen):
+    from blastp_b200 import synth
+    return synth.shape2(matrix, rep=rank, n_subjects=n_subjects, qlen=qlen)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+            time.sleep(0.15)
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.1)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.lines:
+            return None
+        sm, mx, reasons = [], 0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profiled_traffic_per_residue():
+    """dram bytes per database residue of the scan kernel, from the committed
+    ncu summary (profiles/scan_plain_q500_vs_1M.md), or None."""
+    path = os.path.join(ROOT, "profiles", "scan_plain_q500_vs_1M.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_residue:"):
+                return float(line.split(":", 1)[1])
+    except OSError:
+        pass
+    return None
+
+
+def cpu_baseline(matrix, w, budget_s, threads):
+    """Oracle (multithreaded C) on a bounded prefix of the same database:
+    table build + scan, repeated until the budget is used."""
+    import oracle
+    q = w.queries[0]
+    n = min(w.db.n_subjects, 200_000)
+    off = w.db.offsets[:n + 1]
+    res = w.db.residues[:off[-1]]
+    done_res, t0, reps = 0, time.perf_counter(), 0
+    while True:
+        table = oracle.build_table(q, matrix, 11)
+        oracle.scan(res, off, q, table, matrix, [(0, 16, 41)], threads=threads)
+        done_res += int(off[-1])
+        reps += 1
+        if time.perf_counter() - t0 >= budget_s:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": done_res * len(q) / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": "first %d subjects (%d residues) x %d reps, query %d aa, all host threads; %.1f s wall"
+                      % (n, int(off[-1]), reps, len(q), dt)}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    sys.path.insert(0, ROOT)
+    import oracle
+    from blastp_b200 import synth
+    matrix = oracle.load_fixture_matrix()
+    w = load_workload(matrix, 0, args.subjects, args.qlen)
+    q = w.queries[0]
+    threads = os.cpu_count() or 1
+    # each step: table build + scan of a bounded sample of the workload
+    n = min(w.db.n_subjects, 100_000)
+    off = w.db.offsets[:n + 1]
+    res = w.db.residues[:off[-1]]
+    times = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        table = oracle.build_table(q, matrix, 11)
+        oracle.scan(res, off, q, table, matrix, [(0, 16, 41)], threads=threads)
+        if i >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    dt = float(np.sum(times))
+    value = int(off[-1]) * len(q) * len(times) / dt
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / len(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic (seeded; Robinson-Robinson residues, log-normal lengths, planted homologs)",
+            "config": {"workload": w.name, "query_len": len(q), "subjects": w.db.n_subjects,
+                       "residues": w.db.n_residues, "sample_subjects": n, "word": 3, "threshold": 11,
+                       "window": 40, "x_dropoff": 16, "cutoff": 41},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": "first %d subjects (%d residues) per step; the reference's CPU path is "
+                                       "NCBI BLAST 2.2.28, which is not in this image, so the oracle port of "
+                                       "its algorithm is timed" % (n, int(off[-1]))},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    rank, world, local = dist_env()
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(0)
+    import blastp_b200 as bp
+    matrix = bp.blosum62()
+    w = load_workload(matrix, rank, args.subjects, args.qlen)
+    q = w.queries[0]
+    eng = bp.Engine(local if world > 1 else 0)
+    db = eng.database(w.db.residues, w.db.offsets)
+    qry = eng.query(q)
+    stream = torch.cuda.ExternalStream(eng.stream)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    def step():
+        r = eng.search(db, qry)
+        r.wait()
+        ms = eng.last_scan_ms
+        r.close()
+        return ms
+
+    for _ in range(args.warmup):
+        step()
+    barrier()
+    scan_ms = []
+    launches0 = eng.launches
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local if world > 1 else 0) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            scan_ms.append(step())
+        ev1.record(stream)
+        barrier()
+    launches = eng.launches - launches0
+    total_ms = ev0.elapsed_time(ev1)
+    t = torch.tensor([total_ms], device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    total_ms = float(t.item())
+    units = w.db.n_residues * len(q) * world
+    value = units * args.steps / (total_ms / 1e3)
+
+    # end to end through the C ABI: pinned host buffers in and out every step
+    res_pin = torch.empty(len(w.db.residues), dtype=torch.uint8, pin_memory=True)
+    res_pin.numpy()[:] = w.db.residues
+    off_pin = torch.empty(len(w.db.offsets), dtype=torch.int64, pin_memory=True)
+    off_pin.numpy()[:] = w.db.offsets
+    n = w.db.n_subjects
+    cnt_pin = torch.empty((n, 3), dtype=torch.int32, pin_memory=True)
+    hoff_pin = torch.empty(n + 1, dtype=torch.int64, pin_memory=True)
+    ref_hsps = eng.search(db, qry).fetch()
+    cap = len(ref_hsps.hsps) + 1024
+    hsp_pin = torch.empty((cap, 6), dtype=torch.int32, pin_memory=True)
+    import ctypes
+    from blastp_b200._lib import lib, check
+    p = bp.default_params()
+    nh = ctypes.c_int64(0)
+    qarr = np.ascontiguousarray(q)
+
+    def e2e_step():
+        check(lib().bp_blastp_host(eng.h, qarr.ctypes.data, len(q), ctypes.byref(p), res_pin.data_ptr(),
+                                   len(w.db.residues), off_pin.data_ptr(), n, cnt_pin.data_ptr(),
+                                   hoff_pin.data_ptr(), hsp_pin.data_ptr(), cap, ctypes.byref(nh)), eng.h)
+
+    e2e_step()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        e2e_step()
+    barrier()
+    e2e_s = time.perf_counter() - t0
+    t = torch.tensor([e2e_s], device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    e2e_s = float(t.item())
+    h2d = len(w.db.residues) + 8 * len(w.db.offsets) + len(q)
+    d2h = 12 * n + 8 * (n + 1) + 24 * int(nh.value)
+
+    peak, peak_kind = measured_peak_hbm()
+    scan_avg_ms = float(np.mean(scan_ms))
+    alg_bytes = w.db.n_residues + 8 * (n + 1) + 12 * n
+    achieved = alg_bytes / (scan_avg_ms / 1e3) / 1e9
+    tpr = profiled_traffic_per_residue()
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic (seeded; Robinson-Robinson residues, log-normal lengths, planted homologs)",
+        "config": {"workload": w.name, "query_len": len(q), "subjects_per_gpu": n,
+                   "residues_per_gpu": w.db.n_residues, "word": 3, "threshold": 11, "window": 40,
+                   "x_dropoff": 16, "cutoff": 41, "parallelism": "shard%d" % world,
+                   "l2": "inputs larger than L2 (%.2f GB database)" % (w.db.n_residues / 1e9)},
+        "e2e": {"value": w.db.n_residues * len(q) * world * args.e2e_steps / e2e_s, "unit": UNIT,
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "ms_per_step": 1e3 * e2e_s / args.e2e_steps},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": (tpr * w.db.n_residues) if tpr else None,
+                     "kernel": "scan_plain", "kernel_ms": scan_avg_ms,
+                     "algorithmic_bytes": alg_bytes},
+        "hsps": int(len(ref_hsps.hsps)),
+    }
+    line["clocks"] = clk.summary()
+    if rank == 0:
+        sys.path.insert(0, ROOT)
+        line["cpu_baseline"] = cpu_baseline(matrix, w, args.cpu_seconds, os.cpu_count() or 1)
+        print(json.dumps(line), flush=True)
+    qry.close()
+    db.close()
+    eng.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,9 @@
+"""blastp_b200: host layer of the B200 blastp preliminary-search engine.
+
+The engine (two-hit word finding + BLOSUM62 X-drop ungapped extension) is the
+CUDA library libblastp_b200.so; this package binds its C ABI and provides the
+synthetic-data generators used by the benchmark and the tests.
+"""
+from . import synth  # noqa: F401
+from ._lib import BpError, BpParams, lib  # noqa: F401
+from .api import HSP_DTYPE, Database, Engine, PendingResult, Query, Result, blosum62, default_params  # noqa: F401

@@ -1,0 +1,93 @@
+"""ctypes bindings to libblastp_b200.so (include/blastp_b200.h and
+include/gpu_cpu_common_b200.h).
+
+The library is the product; this module only declares its signatures.  It
+fails loudly when the library is missing: there is no Python or CPU fallback.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(HERE), "lib", "libblastp_b200.so")
+
+P = ctypes.c_void_p
+i32 = ctypes.c_int32
+i64 = ctypes.c_int64
+u64 = ctypes.c_uint64
+
+BP_OK = 0
+STATUS_NAMES = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of device memory",
+                4: "input too large", 5: "device wait timed out", 6: "not ready", 7: "no CUDA device"}
+
+
+class BpParams(ctypes.Structure):
+    _fields_ = [("word_length", i32), ("threshold", i32), ("window", i32),
+                ("x_dropoff", i32), ("cutoff_score", i32)]
+
+
+class BpError(RuntimeError):
+    def __init__(self, status, msg=""):
+        self.status = status
+        super().__init__("%s (%d)%s" % (STATUS_NAMES.get(status, "?"), status, (": " + msg) if msg else ""))
+
+
+# exported symbol -> (restype, argtypes)
+SIGNATURES = {
+    "bp_params_default": (None, [P]),
+    "bp_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "bp_blosum62_ncbistdaa": (None, [P]),
+    "bp_engine_create": (ctypes.c_int, [ctypes.c_int, P]),
+    "bp_engine_destroy": (None, [P]),
+    "bp_last_error": (ctypes.c_char_p, [P]),
+    "bp_engine_stream": (P, [P]),
+    "bp_engine_launch_count": (u64, [P]),
+    "bp_engine_last_scan_ms": (ctypes.c_float, [P]),
+    "bp_engine_synchronize": (ctypes.c_int, [P]),
+    "bp_db_create": (ctypes.c_int, [P, P, i64, P, i32, P]),
+    "bp_db_create_device": (ctypes.c_int, [P, P, i64, P, i32, P]),
+    "bp_db_destroy": (None, [P]),
+    "bp_db_subjects": (i32, [P]),
+    "bp_db_residues": (i64, [P]),
+    "bp_query_create": (ctypes.c_int, [P, P, i32, P, P]),
+    "bp_query_destroy": (None, [P]),
+    "bp_query_table": (ctypes.c_int, [P, P, P, i64, P]),
+    "bp_search": (ctypes.c_int, [P, P, P, i32, i32, P]),
+    "bp_result_wait": (ctypes.c_int, [P]),
+    "bp_result_subjects": (i32, [P]),
+    "bp_result_hsps": (i64, [P]),
+    "bp_result_copy": (ctypes.c_int, [P, P, P, P]),
+    "bp_result_destroy": (None, [P]),
+    "bp_blastp_host": (ctypes.c_int, [P, P, i32, P, P, i64, P, i32, P, P, P, i64, P]),
+    # reference-compatible entry points
+    "GPU_BLASTP": (None, [P] * 8 + [ctypes.c_int, P, P, i32, P, i32] + [P] * 7),
+    "GPU_BLASTP_get_data": (None, [P, P, i32, P, P, i32, i32]),
+    "GPU_BLASTP_free_memory": (None, [P] * 9),
+    "GPU_BLASTP_check_memory": (ctypes.c_uint8, [P, P, P, ctypes.c_int, i32, i32, i32, i32, i32]),
+    "GPU_BLAST_check_availability": (ctypes.c_uint8, []),
+    "Round2Multiple": (None, [P]),
+}
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("libblastp_b200.so is not built (%s): run `make -C blastp-cuda_b200` "
+                               "or __graft_entry__.build()" % LIB_PATH)
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(status, engine=None):
+    if status != BP_OK:
+        msg = ""
+        if engine:
+            msg = (lib().bp_last_error(engine) or b"").decode(errors="replace")
+        raise BpError(status, msg)

@@ -1,0 +1,195 @@
+"""Python host layer over the native C ABI: the same operations as the C
+entry points, with numpy arrays in and out.  The work runs in
+libblastp_b200.so on the GPU; nothing here computes results.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import BpParams, check, lib
+
+HSP_DTYPE = np.dtype([("hsp_q", "<i4"), ("hsp_s", "<i4"), ("query_offset", "<i4"),
+                      ("subject_offset", "<i4"), ("hsp_len", "<i4"), ("score", "<i4")])
+
+
+def _p(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None else None
+
+
+def default_params(**kw) -> BpParams:
+    p = BpParams()
+    lib().bp_params_default(ctypes.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def blosum62() -> np.ndarray:
+    out = np.zeros(28 * 28, dtype=np.int8)
+    lib().bp_blosum62_ncbistdaa(_p(out))
+    return out.reshape(28, 28)
+
+
+class Result:
+    """Per-subject counters (hits, successful extensions, extensions) and the
+    HSP set as CSR (offsets into a structured array, discovery order)."""
+
+    def __init__(self, counters, hsp_off, hsps):
+        self.counters = counters
+        self.hsp_off = hsp_off
+        self.hsps = hsps
+
+    def hsps_as_array(self):
+        return self.hsps.view(np.int32).reshape(-1, 6)
+
+
+class Engine:
+    def __init__(self, device: int = 0):
+        h = ctypes.c_void_p()
+        check(lib().bp_engine_create(device, ctypes.byref(h)))
+        self.h = h
+        self.device = device
+
+    def close(self):
+        if self.h:
+            lib().bp_engine_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream(self) -> int:
+        return lib().bp_engine_stream(self.h) or 0
+
+    @property
+    def launches(self) -> int:
+        return int(lib().bp_engine_launch_count(self.h))
+
+    @property
+    def last_scan_ms(self) -> float:
+        return float(lib().bp_engine_last_scan_ms(self.h))
+
+    def synchronize(self):
+        check(lib().bp_engine_synchronize(self.h), self.h)
+
+    def database(self, residues: np.ndarray, offsets: np.ndarray) -> "Database":
+        return Database(self, residues, offsets)
+
+    def query(self, residues: np.ndarray, params: BpParams | None = None) -> "Query":
+        return Query(self, residues, params or default_params())
+
+    def search(self, db: "Database", q: "Query", first: int = 0, count: int = -1) -> "PendingResult":
+        h = ctypes.c_void_p()
+        check(lib().bp_search(self.h, db.h, q.h, first, count, ctypes.byref(h)), self.h)
+        return PendingResult(self, h)
+
+    def blastp_host(self, query, params, residues, offsets, hsp_cap=None):
+        """End-to-end: host buffers in, host buffers out (one C call)."""
+        q = np.ascontiguousarray(query, dtype=np.uint8)
+        res = np.ascontiguousarray(residues, dtype=np.uint8)
+        off = np.ascontiguousarray(offsets, dtype=np.int64)
+        n = len(off) - 1
+        counters = np.zeros((n, 3), dtype=np.int32)
+        hoff = np.zeros(n + 1, dtype=np.int64)
+        nh = ctypes.c_int64(0)
+        cap = hsp_cap if hsp_cap is not None else max(4096, n // 2)
+        hsps = np.zeros(cap, dtype=HSP_DTYPE)
+        st = lib().bp_blastp_host(self.h, _p(q), len(q), ctypes.byref(params), _p(res), len(res), _p(off), n,
+                                  _p(counters), _p(hoff), _p(hsps), cap, ctypes.byref(nh))
+        if st == 4 and nh.value > cap:   # too small: retry once with the exact size
+            hsps = np.zeros(nh.value, dtype=HSP_DTYPE)
+            st = lib().bp_blastp_host(self.h, _p(q), len(q), ctypes.byref(params), _p(res), len(res), _p(off), n,
+                                      _p(counters), _p(hoff), _p(hsps), nh.value, ctypes.byref(nh))
+        check(st, self.h)
+        return Result(counters, hoff, hsps[:nh.value])
+
+
+class Database:
+    def __init__(self, engine: Engine, residues, offsets):
+        res = np.ascontiguousarray(residues, dtype=np.uint8)
+        off = np.ascontiguousarray(offsets, dtype=np.int64)
+        h = ctypes.c_void_p()
+        check(lib().bp_db_create(engine.h, _p(res), len(res), _p(off), len(off) - 1, ctypes.byref(h)), engine.h)
+        self.h = h
+        self.engine = engine
+        self.n_subjects = len(off) - 1
+        self.n_residues = len(res)
+
+    def close(self):
+        if self.h:
+            lib().bp_db_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Query:
+    def __init__(self, engine: Engine, residues, params: BpParams):
+        q = np.ascontiguousarray(residues, dtype=np.uint8)
+        h = ctypes.c_void_p()
+        check(lib().bp_query_create(engine.h, _p(q), len(q), ctypes.byref(params), ctypes.byref(h)), engine.h)
+        self.h = h
+        self.engine = engine
+        self.length = len(q)
+        self.params = params
+
+    def table(self):
+        start = np.zeros((1 << 15) + 1, dtype=np.uint32)
+        n = ctypes.c_int64(0)
+        check(lib().bp_query_table(self.h, _p(start), None, 0, ctypes.byref(n)), self.engine.h)
+        ent = np.zeros(max(1, n.value), dtype=np.uint16)
+        check(lib().bp_query_table(self.h, None, _p(ent), n.value, ctypes.byref(n)), self.engine.h)
+        return start, ent[:n.value]
+
+    def close(self):
+        if self.h:
+            lib().bp_query_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class PendingResult:
+    def __init__(self, engine: Engine, h):
+        self.engine = engine
+        self.h = h
+
+    def wait(self):
+        check(lib().bp_result_wait(self.h), self.engine.h)
+        return self
+
+    def fetch(self) -> Result:
+        self.wait()
+        n = lib().bp_result_subjects(self.h)
+        k = lib().bp_result_hsps(self.h)
+        counters = np.zeros((n, 3), dtype=np.int32)
+        hoff = np.zeros(n + 1, dtype=np.int64)
+        hsps = np.zeros(max(k, 1), dtype=HSP_DTYPE)
+        check(lib().bp_result_copy(self.h, _p(counters), _p(hoff), _p(hsps)), self.engine.h)
+        return Result(counters, hoff, hsps[:k])
+
+    def close(self):
+        if self.h:
+            lib().bp_result_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

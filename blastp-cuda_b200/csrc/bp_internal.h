@@ -1,0 +1,120 @@
+// Internal declarations shared by the engine's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "blastp_b200.h"
+
+#define BP_NCELL 32768          // 3 letters x 5 bits
+#define BP_WORD 3
+#define BP_MROW 32              // device matrix row stride (28 used)
+
+// One reported HSP before ordering: owning subject (relative to the search's
+// first subject), its discovery key (index of the triggering word hit in the
+// subject's hit stream) and the record itself.
+struct HspRec {
+    int32_t oid;
+    int32_t key;
+    bp_hsp h;
+};
+
+struct bp_engine {
+    int device = 0;
+    int sm_count = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev_scan0 = nullptr, ev_scan1 = nullptr;
+    uint64_t launches = 0;
+    float last_scan_ms = 0.f;
+    std::string err;
+    int8_t* d_matrix = nullptr;          // int8 [28][32]
+    // grow-only scratch shared by searches on this engine
+    HspRec* d_recs = nullptr;
+    uint32_t rec_cap = 0;
+    uint32_t* d_counts = nullptr;        // [0] records written, [1] work cursor, [2..] spare
+    uint32_t* h_counts = nullptr;        // pinned mirror of d_counts[0..3]
+    int32_t* d_fill = nullptr;           // per-subject fill cursors
+    int32_t fill_cap = 0;
+    int64_t* d_blocksums = nullptr;
+    int32_t blocksum_cap = 0;
+};
+
+struct bp_db {
+    bp_engine* e = nullptr;
+    uint8_t* d_res = nullptr;
+    int64_t* d_off = nullptr;
+    int32_t n = 0;
+    int64_t nres = 0;
+    int32_t max_len = 0;
+};
+
+struct bp_query {
+    bp_engine* e = nullptr;
+    uint8_t* d_q = nullptr;
+    int32_t qlen = 0;
+    uint32_t* d_cell_start = nullptr;    // BP_NCELL + 1
+    uint16_t* d_entries = nullptr;
+    uint32_t* d_pv = nullptr;            // BP_NCELL / 32 words
+    int64_t n_entries = 0;
+    int32_t n_ctx = 1;
+    int32_t* d_ctx = nullptr;            // n_ctx x {query_offset, x_dropoff, cutoff}
+    bp_params p{};
+    int32_t diag_mask = 0;
+};
+
+struct bp_result {
+    bp_engine* e = nullptr;
+    int32_t n = 0;
+    int32_t* d_counters = nullptr;       // 3n
+    int64_t* d_hsp_off = nullptr;        // n+1
+    bp_hsp* d_hsps = nullptr;
+    int32_t* d_keys = nullptr;
+    uint32_t cap = 0;
+    uint32_t* h_count = nullptr;         // pinned: records written by this search
+    int64_t n_hsps = -1;
+    // to re-run on overflow
+    const bp_db* db = nullptr;
+    const bp_query* q = nullptr;
+    int32_t first = 0;
+};
+
+// Everything the scan kernel reads, by value.
+struct ScanArgs {
+    const uint8_t* db;
+    const int64_t* db_off;
+    int32_t first;              // first subject
+    int32_t n;                  // subjects to scan
+    const uint8_t* query;
+    int32_t qlen;
+    const uint32_t* cell_start;
+    const uint16_t* entries;
+    const uint32_t* pv;
+    const int32_t* ctx;
+    int32_t n_ctx;
+    const int8_t* matrix;       // [28][32]
+    int32_t window;
+    int32_t diag_mask;
+    int32_t* counters;          // 3 per scanned subject
+    HspRec* recs;
+    uint32_t rec_cap;
+    uint32_t* rec_count;
+    uint32_t* cursor;
+};
+
+// ---- host helpers (engine.cu) -------------------------------------------
+bp_status bp_set_cuda_error(bp_engine* e, cudaError_t err, const char* what);
+bp_status bp_set_error(bp_engine* e, bp_status s, const std::string& msg);
+void bp_fill_matrix28(int8_t out[28 * 28]);
+
+// ---- launchers (table.cu / scan.cu) --------------------------------------
+cudaError_t bp_launch_table_build(bp_engine* e, const uint8_t* d_q, int32_t qlen, int32_t threshold,
+                                  uint32_t* d_cell_start, uint16_t* d_entries, uint32_t* d_pv,
+                                  uint32_t* d_counts_tmp, int64_t entry_cap, int pass);
+cudaError_t bp_launch_scan(bp_engine* e, const ScanArgs& a);
+cudaError_t bp_launch_order(bp_engine* e, int32_t n, const int32_t* d_counters, int64_t* d_hsp_off,
+                            const HspRec* d_recs, uint32_t rec_cap, const uint32_t* d_rec_count,
+                            int32_t* d_fill, bp_hsp* d_out, int32_t* d_keys, int64_t* d_blocksums);
+int32_t bp_order_blocksums_needed(int32_t n);
+bp_status bp_run_search(bp_engine* e, bp_result* r);

@@ -1,0 +1,506 @@
+// Host side of the native C ABI (include/blastp_b200.h).
+//
+// Replaces the reference's host driver GPU_BLASTP / GPU_BLASTP_get_data /
+// GPU_BLASTP_free_memory (gpu_blastp.cu:16-280): instead of per-call
+// cudaMalloc of nine buffers, per-block replicas of the presence vector and
+// matrix, and a kernel launch without error checks, the engine keeps the
+// database and query tables resident, reuses grow-only scratch, checks every
+// CUDA call and returns a status.
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "bp_internal.h"
+
+#define CK(call, what)                                                 \
+    do {                                                               \
+        cudaError_t _err = (call);                                     \
+        if (_err != cudaSuccess) return bp_set_cuda_error(e, _err, what); \
+    } while (0)
+
+bp_status bp_set_cuda_error(bp_engine* e, cudaError_t err, const char* what) {
+    if (e) e->err = std::string(what) + ": " + cudaGetErrorString(err);
+    cudaGetLastError();
+    return err == cudaErrorMemoryAllocation ? BP_ERR_NOMEM : BP_ERR_CUDA;
+}
+
+bp_status bp_set_error(bp_engine* e, bp_status s, const std::string& msg) {
+    if (e) e->err = msg;
+    return s;
+}
+
+namespace {
+
+int diag_mask_for(int qlen, int window) {
+    int n = 1;
+    while (n < qlen + window) n <<= 1;
+    return n - 1;
+}
+
+bool residues_valid(const uint8_t* p, int64_t n) {
+    uint8_t bad = 0;
+    for (int64_t i = 0; i < n; ++i) bad |= (uint8_t)(p[i] >= BP_ALPHABET);
+    return bad == 0;
+}
+
+template <class T>
+cudaError_t grow(T** p, size_t* cap_elems, size_t need) {
+    if (*p && *cap_elems >= need) return cudaSuccess;
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    size_t n = std::max(need, *cap_elems * 3 / 2);
+    cudaError_t err = cudaMalloc((void**)p, n * sizeof(T));
+    *cap_elems = err == cudaSuccess ? n : 0;
+    return err;
+}
+
+}  // namespace
+
+// Enqueues scan + ordering for r (subjects r->first.. of r->db against r->q)
+// on the engine stream.  Scratch is the engine's; outputs are r's.
+bp_status bp_run_search(bp_engine* e, bp_result* r) {
+    const bp_db* db = r->db;
+    const bp_query* q = r->q;
+    const int32_t n = r->n;
+    // scratch on the engine
+    size_t cap = e->rec_cap;
+    CK(grow(&e->d_recs, &cap, std::max<size_t>(r->cap, 65536)), "cudaMalloc(records)");
+    e->rec_cap = (uint32_t)cap;
+    size_t fcap = (size_t)e->fill_cap;
+    CK(grow(&e->d_fill, &fcap, (size_t)std::max(n, 1)), "cudaMalloc(fill)");
+    e->fill_cap = (int32_t)fcap;
+    size_t bcap = (size_t)e->blocksum_cap;
+    CK(grow(&e->d_blocksums, &bcap, (size_t)bp_order_blocksums_needed(n)), "cudaMalloc(blocksums)");
+    e->blocksum_cap = (int32_t)bcap;
+    // result buffers sized to the record buffer
+    if (r->cap < e->rec_cap || !r->d_hsps) {
+        if (r->d_hsps) cudaFree(r->d_hsps);
+        if (r->d_keys) cudaFree(r->d_keys);
+        r->d_hsps = nullptr;
+        r->d_keys = nullptr;
+        r->cap = e->rec_cap;
+        CK(cudaMalloc((void**)&r->d_hsps, (size_t)r->cap * sizeof(bp_hsp)), "cudaMalloc(hsps)");
+        CK(cudaMalloc((void**)&r->d_keys, (size_t)r->cap * sizeof(int32_t)), "cudaMalloc(keys)");
+    }
+    CK(cudaMemsetAsync(e->d_counts, 0, 4 * sizeof(uint32_t), e->stream), "memset(counts)");
+
+    ScanArgs a;
+    a.db = db->d_res;
+    a.db_off = db->d_off;
+    a.first = r->first;
+    a.n = n;
+    a.query = q->d_q;
+    a.qlen = q->qlen;
+    a.cell_start = q->d_cell_start;
+    a.entries = q->d_entries;
+    a.pv = q->d_pv;
+    a.ctx = q->d_ctx;
+    a.n_ctx = q->n_ctx;
+    a.matrix = e->d_matrix;
+    a.window = q->p.window;
+    a.diag_mask = q->diag_mask;
+    a.counters = r->d_counters;
+    a.recs = e->d_recs;
+    a.rec_cap = std::min(e->rec_cap, r->cap);
+    a.rec_count = e->d_counts;
+    a.cursor = e->d_counts + 1;
+    CK(cudaEventRecord(e->ev_scan0, e->stream), "cudaEventRecord");
+    if (n > 0) CK(bp_launch_scan(e, a), "scan kernel launch");
+    CK(cudaEventRecord(e->ev_scan1, e->stream), "cudaEventRecord");
+    CK(bp_launch_order(e, n, r->d_counters, r->d_hsp_off, e->d_recs, a.rec_cap, e->d_counts, e->d_fill,
+                       r->d_hsps, r->d_keys, e->d_blocksums),
+       "order kernels launch");
+    CK(cudaMemcpyAsync(r->h_count, e->d_counts, sizeof(uint32_t), cudaMemcpyDeviceToHost, e->stream),
+       "copy counts");
+    r->n_hsps = -1;
+    return BP_OK;
+}
+
+extern "C" {
+
+void bp_params_default(bp_params* p) {
+    p->word_length = 3;
+    p->threshold = 11;
+    p->window = 40;
+    p->x_dropoff = 16;
+    p->cutoff_score = 41;
+}
+
+const char* bp_status_string(bp_status s) {
+    switch (s) {
+        case BP_OK: return "ok";
+        case BP_ERR_INVALID: return "invalid argument";
+        case BP_ERR_CUDA: return "CUDA error";
+        case BP_ERR_NOMEM: return "out of device memory";
+        case BP_ERR_TOO_LARGE: return "input too large";
+        case BP_ERR_TIMEOUT: return "device wait timed out";
+        case BP_ERR_NOT_READY: return "not ready";
+        case BP_ERR_NO_DEVICE: return "no CUDA device";
+    }
+    return "unknown status";
+}
+
+void bp_blosum62_ncbistdaa(int8_t out[BP_ALPHABET * BP_ALPHABET]) { bp_fill_matrix28(out); }
+
+bp_status bp_engine_create(int device, bp_engine** out) {
+    if (!out) return BP_ERR_INVALID;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return BP_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= count) return BP_ERR_INVALID;
+    bp_engine* e = new bp_engine();
+    e->device = device;
+    bp_status st = BP_OK;
+    do {
+        cudaError_t err;
+        if ((err = cudaSetDevice(device)) != cudaSuccess) { st = bp_set_cuda_error(e, err, "cudaSetDevice"); break; }
+        if ((err = cudaDeviceGetAttribute(&e->sm_count, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess) {
+            st = bp_set_cuda_error(e, err, "cudaDeviceGetAttribute"); break;
+        }
+        if ((err = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking)) != cudaSuccess) {
+            st = bp_set_cuda_error(e, err, "cudaStreamCreate"); break;
+        }
+        if ((err = cudaEventCreate(&e->ev_scan0)) != cudaSuccess ||
+            (err = cudaEventCreate(&e->ev_scan1)) != cudaSuccess) {
+            st = bp_set_cuda_error(e, err, "cudaEventCreate"); break;
+        }
+        int8_t m28[28 * 28], m32[28 * BP_MROW];
+        bp_fill_matrix28(m28);
+        for (int a = 0; a < 28; ++a)
+            for (int b = 0; b < BP_MROW; ++b) m32[a * BP_MROW + b] = b < 28 ? m28[a * 28 + b] : (int8_t)-128;
+        if ((err = cudaMalloc((void**)&e->d_matrix, sizeof(m32))) != cudaSuccess ||
+            (err = cudaMemcpy(e->d_matrix, m32, sizeof(m32), cudaMemcpyHostToDevice)) != cudaSuccess) {
+            st = bp_set_cuda_error(e, err, "matrix upload"); break;
+        }
+        if ((err = cudaMalloc((void**)&e->d_counts, 16 * sizeof(uint32_t))) != cudaSuccess ||
+            (err = cudaMallocHost((void**)&e->h_counts, 16 * sizeof(uint32_t))) != cudaSuccess) {
+            st = bp_set_cuda_error(e, err, "counter alloc"); break;
+        }
+    } while (0);
+    if (st != BP_OK) {
+        fprintf(stderr, "bp_engine_create: %s\n", e->err.c_str());
+        bp_engine_destroy(e);
+        return st;
+    }
+    *out = e;
+    return BP_OK;
+}
+
+void bp_engine_destroy(bp_engine* e) {
+    if (!e) return;
+    cudaSetDevice(e->device);
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    cudaFree(e->d_matrix);
+    cudaFree(e->d_recs);
+    cudaFree(e->d_counts);
+    cudaFreeHost(e->h_counts);
+    cudaFree(e->d_fill);
+    cudaFree(e->d_blocksums);
+    if (e->ev_scan0) cudaEventDestroy(e->ev_scan0);
+    if (e->ev_scan1) cudaEventDestroy(e->ev_scan1);
+    if (e->stream) cudaStreamDestroy(e->stream);
+    delete e;
+}
+
+const char* bp_last_error(const bp_engine* e) { return e ? e->err.c_str() : ""; }
+void* bp_engine_stream(bp_engine* e) { return e ? (void*)e->stream : nullptr; }
+uint64_t bp_engine_launch_count(const bp_engine* e) { return e ? e->launches : 0; }
+float bp_engine_last_scan_ms(const bp_engine* e) { return e ? e->last_scan_ms : 0.f; }
+
+bp_status bp_engine_synchronize(bp_engine* e) {
+    if (!e) return BP_ERR_INVALID;
+    CK(cudaStreamSynchronize(e->stream), "cudaStreamSynchronize");
+    return BP_OK;
+}
+
+static bp_status db_alloc(bp_engine* e, int64_t n_residues, int32_t n_subjects, bp_db** out) {
+    bp_db* db = new bp_db();
+    db->e = e;
+    db->n = n_subjects;
+    db->nres = n_residues;
+    cudaError_t err = cudaMalloc((void**)&db->d_res, (size_t)std::max<int64_t>(n_residues, 1) + 16);
+    if (err == cudaSuccess) err = cudaMalloc((void**)&db->d_off, ((size_t)n_subjects + 1) * sizeof(int64_t));
+    if (err != cudaSuccess) {
+        bp_db_destroy(db);
+        return bp_set_cuda_error(e, err, "cudaMalloc(database)");
+    }
+    *out = db;
+    return BP_OK;
+}
+
+bp_status bp_db_create(bp_engine* e, const uint8_t* residues, int64_t n_residues, const int64_t* offsets,
+                       int32_t n_subjects, bp_db** out) {
+    if (!e || !out || !offsets || n_subjects < 0 || n_residues < 0 || (n_residues > 0 && !residues))
+        return bp_set_error(e, BP_ERR_INVALID, "bp_db_create: bad argument");
+    *out = nullptr;
+    if (offsets[0] != 0 || offsets[n_subjects] != n_residues)
+        return bp_set_error(e, BP_ERR_INVALID, "bp_db_create: offsets must run from 0 to n_residues");
+    for (int32_t i = 0; i < n_subjects; ++i)
+        if (offsets[i + 1] < offsets[i] || offsets[i + 1] - offsets[i] > INT32_MAX / 2)
+            return bp_set_error(e, BP_ERR_INVALID, "bp_db_create: offsets must be non-decreasing");
+    if (!residues_valid(residues, n_residues))
+        return bp_set_error(e, BP_ERR_INVALID, "bp_db_create: residue code >= 28");
+    CK(cudaSetDevice(e->device), "cudaSetDevice");
+    bp_db* db = nullptr;
+    bp_status st = db_alloc(e, n_residues, n_subjects, &db);
+    if (st != BP_OK) return st;
+    cudaError_t err = cudaMemcpyAsync(db->d_res, residues, (size_t)n_residues, cudaMemcpyHostToDevice, e->stream);
+    if (err == cudaSuccess) err = cudaMemsetAsync(db->d_res + n_residues, 0, 16, e->stream);
+    if (err == cudaSuccess)
+        err = cudaMemcpyAsync(db->d_off, offsets, ((size_t)n_subjects + 1) * sizeof(int64_t),
+                              cudaMemcpyHostToDevice, e->stream);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
+    if (err != cudaSuccess) {
+        bp_db_destroy(db);
+        return bp_set_cuda_error(e, err, "database upload");
+    }
+    *out = db;
+    return BP_OK;
+}
+
+bp_status bp_db_create_device(bp_engine* e, const uint8_t* d_residues, int64_t n_residues,
+                              const int64_t* d_offsets, int32_t n_subjects, bp_db** out) {
+    if (!e || !out || !d_offsets || n_subjects < 0 || n_residues < 0)
+        return bp_set_error(e, BP_ERR_INVALID, "bp_db_create_device: bad argument");
+    *out = nullptr;
+    CK(cudaSetDevice(e->device), "cudaSetDevice");
+    std::vector<int64_t> off((size_t)n_subjects + 1);
+    CK(cudaMemcpy(off.data(), d_offsets, off.size() * sizeof(int64_t), cudaMemcpyDeviceToHost), "read offsets");
+    if (off[0] != 0 || off[n_subjects] != n_residues)
+        return bp_set_error(e, BP_ERR_INVALID, "bp_db_create_device: offsets must run from 0 to n_residues");
+    bp_db* db = nullptr;
+    bp_status st = db_alloc(e, n_residues, n_subjects, &db);
+    if (st != BP_OK) return st;
+    cudaError_t err = cudaMemcpyAsync(db->d_res, d_residues, (size_t)n_residues, cudaMemcpyDeviceToDevice, e->stream);
+    if (err == cudaSuccess) err = cudaMemsetAsync(db->d_res + n_residues, 0, 16, e->stream);
+    if (err == cudaSuccess)
+        err = cudaMemcpyAsync(db->d_off, d_offsets, off.size() * sizeof(int64_t), cudaMemcpyDeviceToDevice, e->stream);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
+    if (err != cudaSuccess) {
+        bp_db_destroy(db);
+        return bp_set_cuda_error(e, err, "database copy");
+    }
+    *out = db;
+    return BP_OK;
+}
+
+void bp_db_destroy(bp_db* db) {
+    if (!db) return;
+    cudaFree(db->d_res);
+    cudaFree(db->d_off);
+    delete db;
+}
+
+int32_t bp_db_subjects(const bp_db* db) { return db ? db->n : 0; }
+int64_t bp_db_residues(const bp_db* db) { return db ? db->nres : 0; }
+
+bp_status bp_query_create(bp_engine* e, const uint8_t* residues, int32_t length, const bp_params* p,
+                          bp_query** out) {
+    if (!e || !out || !p || length < 0 || (length > 0 && !residues))
+        return bp_set_error(e, BP_ERR_INVALID, "bp_query_create: bad argument");
+    *out = nullptr;
+    if (length > BP_MAX_QUERY_LENGTH)
+        return bp_set_error(e, BP_ERR_TOO_LARGE, "bp_query_create: query longer than 65535");
+    if (p->word_length != BP_WORD || p->window < 1 || p->x_dropoff < 0)
+        return bp_set_error(e, BP_ERR_INVALID, "bp_query_create: word_length must be 3, window >= 1, x_dropoff >= 0");
+    for (int32_t i = 0; i < length; ++i)
+        if (residues[i] == 0 || residues[i] >= BP_ALPHABET)
+            return bp_set_error(e, BP_ERR_INVALID, "bp_query_create: query residue codes must be 1..27");
+    CK(cudaSetDevice(e->device), "cudaSetDevice");
+    bp_query* q = new bp_query();
+    q->e = e;
+    q->qlen = length;
+    q->p = *p;
+    q->n_ctx = 1;
+    q->diag_mask = diag_mask_for(length, p->window);
+    bp_status st = BP_OK;
+    uint32_t* d_tmp = nullptr;
+    do {
+        cudaError_t err;
+        if ((err = cudaMalloc((void**)&q->d_q, (size_t)((length + 15) & ~15) + 16)) != cudaSuccess ||
+            (err = cudaMalloc((void**)&q->d_cell_start, (BP_NCELL + 1) * sizeof(uint32_t))) != cudaSuccess ||
+            (err = cudaMalloc((void**)&q->d_pv, (BP_NCELL / 32) * sizeof(uint32_t))) != cudaSuccess ||
+            (err = cudaMalloc((void**)&q->d_ctx, 3 * sizeof(int32_t))) != cudaSuccess ||
+            (err = cudaMalloc((void**)&d_tmp, BP_NCELL * sizeof(uint32_t))) != cudaSuccess) {
+            st = bp_set_cuda_error(e, err, "cudaMalloc(query)"); break;
+        }
+        if (length > 0 &&
+            (err = cudaMemcpyAsync(q->d_q, residues, (size_t)length, cudaMemcpyHostToDevice, e->stream)) != cudaSuccess) {
+            st = bp_set_cuda_error(e, err, "query upload"); break;
+        }
+        int32_t ctx[3] = {0, p->x_dropoff, p->cutoff_score};
+        if ((err = cudaMemcpyAsync(q->d_ctx, ctx, sizeof(ctx), cudaMemcpyHostToDevice, e->stream)) != cudaSuccess ||
+            (err = bp_launch_table_build(e, q->d_q, length, p->threshold, q->d_cell_start, nullptr, q->d_pv, d_tmp, 0, 0)) !=
+                cudaSuccess) {
+            st = bp_set_cuda_error(e, err, "table count"); break;
+        }
+        uint32_t total = 0;
+        if ((err = cudaMemcpyAsync(&total, q->d_cell_start + BP_NCELL, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                   e->stream)) != cudaSuccess ||
+            (err = cudaStreamSynchronize(e->stream)) != cudaSuccess) {
+            st = bp_set_cuda_error(e, err, "table size"); break;
+        }
+        q->n_entries = total;
+        if ((err = cudaMalloc((void**)&q->d_entries, (size_t)std::max<uint32_t>(total, 1) * sizeof(uint16_t))) !=
+                cudaSuccess ||
+            (err = bp_launch_table_build(e, q->d_q, length, p->threshold, q->d_cell_start, q->d_entries, q->d_pv,
+                                         d_tmp, total, 1)) != cudaSuccess ||
+            (err = cudaStreamSynchronize(e->stream)) != cudaSuccess) {
+            st = bp_set_cuda_error(e, err, "table fill"); break;
+        }
+    } while (0);
+    cudaFree(d_tmp);
+    if (st != BP_OK) {
+        bp_query_destroy(q);
+        return st;
+    }
+    *out = q;
+    return BP_OK;
+}
+
+void bp_query_destroy(bp_query* q) {
+    if (!q) return;
+    cudaFree(q->d_q);
+    cudaFree(q->d_cell_start);
+    cudaFree(q->d_entries);
+    cudaFree(q->d_pv);
+    cudaFree(q->d_ctx);
+    delete q;
+}
+
+bp_status bp_query_table(bp_query* q, uint32_t* cell_start, uint16_t* entries, int64_t cap, int64_t* n_entries) {
+    if (!q) return BP_ERR_INVALID;
+    bp_engine* e = q->e;
+    CK(cudaSetDevice(e->device), "cudaSetDevice");
+    CK(cudaStreamSynchronize(e->stream), "sync");
+    if (n_entries) *n_entries = q->n_entries;
+    if (cell_start)
+        CK(cudaMemcpy(cell_start, q->d_cell_start, (BP_NCELL + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost),
+           "copy table");
+    if (entries && q->n_entries > 0)
+        CK(cudaMemcpy(entries, q->d_entries, (size_t)std::min<int64_t>(cap, q->n_entries) * sizeof(uint16_t),
+                      cudaMemcpyDeviceToHost),
+           "copy entries");
+    return BP_OK;
+}
+
+bp_status bp_search(bp_engine* e, const bp_db* db, const bp_query* q, int32_t first, int32_t count,
+                    bp_result** out) {
+    if (!e || !db || !q || !out || first < 0 || first > db->n)
+        return bp_set_error(e, BP_ERR_INVALID, "bp_search: bad argument");
+    *out = nullptr;
+    if (count < 0 || count > db->n - first) count = db->n - first;
+    const int L = q->diag_mask + 1;
+    if ((size_t)L * 4 + 1024 + 4096 + 65552 > 227 * 1024)
+        return bp_set_error(e, BP_ERR_TOO_LARGE, "bp_search: query too long for the shared-memory diagonal array");
+    CK(cudaSetDevice(e->device), "cudaSetDevice");
+    bp_result* r = new bp_result();
+    r->e = e;
+    r->n = count;
+    r->db = db;
+    r->q = q;
+    r->first = first;
+    r->cap = 0;
+    cudaError_t err = cudaMalloc((void**)&r->d_counters, (size_t)std::max(count, 1) * 3 * sizeof(int32_t));
+    if (err == cudaSuccess) err = cudaMalloc((void**)&r->d_hsp_off, ((size_t)count + 1) * sizeof(int64_t));
+    if (err == cudaSuccess) err = cudaMallocHost((void**)&r->h_count, sizeof(uint32_t));
+    if (err != cudaSuccess) {
+        bp_result_destroy(r);
+        return bp_set_cuda_error(e, err, "cudaMalloc(result)");
+    }
+    bp_status st = bp_run_search(e, r);
+    if (st != BP_OK) {
+        bp_result_destroy(r);
+        return st;
+    }
+    *out = r;
+    return BP_OK;
+}
+
+bp_status bp_result_wait(bp_result* r) {
+    if (!r) return BP_ERR_INVALID;
+    bp_engine* e = r->e;
+    if (r->n_hsps >= 0) return BP_OK;
+    CK(cudaSetDevice(e->device), "cudaSetDevice");
+    for (int attempt = 0; attempt < 4; ++attempt) {
+        CK(cudaStreamSynchronize(e->stream), "search");
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, e->ev_scan0, e->ev_scan1) == cudaSuccess) e->last_scan_ms = ms;
+        cudaGetLastError();
+        const uint32_t count = *r->h_count;
+        if (count <= r->cap) {
+            r->n_hsps = count;
+            return BP_OK;
+        }
+        // record buffer overflowed: enlarge and run again
+        r->cap = count + count / 4 + 1024;
+        size_t cap = e->rec_cap;
+        CK(grow(&e->d_recs, &cap, r->cap), "cudaMalloc(records)");
+        e->rec_cap = (uint32_t)cap;
+        cudaFree(r->d_hsps);
+        cudaFree(r->d_keys);
+        r->d_hsps = nullptr;
+        r->d_keys = nullptr;
+        bp_status st = bp_run_search(e, r);
+        if (st != BP_OK) return st;
+    }
+    return bp_set_error(e, BP_ERR_CUDA, "bp_result_wait: record buffer kept overflowing");
+}
+
+int32_t bp_result_subjects(const bp_result* r) { return r ? r->n : 0; }
+int64_t bp_result_hsps(const bp_result* r) { return r ? r->n_hsps : -1; }
+
+bp_status bp_result_copy(bp_result* r, int32_t* counters, int64_t* hsp_off, bp_hsp* hsps) {
+    if (!r) return BP_ERR_INVALID;
+    bp_status st = bp_result_wait(r);
+    if (st != BP_OK) return st;
+    bp_engine* e = r->e;
+    if (counters && r->n > 0)
+        CK(cudaMemcpy(counters, r->d_counters, (size_t)r->n * 3 * sizeof(int32_t), cudaMemcpyDeviceToHost),
+           "copy counters");
+    if (hsp_off)
+        CK(cudaMemcpy(hsp_off, r->d_hsp_off, ((size_t)r->n + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost),
+           "copy offsets");
+    if (hsps && r->n_hsps > 0)
+        CK(cudaMemcpy(hsps, r->d_hsps, (size_t)r->n_hsps * sizeof(bp_hsp), cudaMemcpyDeviceToHost), "copy hsps");
+    return BP_OK;
+}
+
+void bp_result_destroy(bp_result* r) {
+    if (!r) return;
+    cudaFree(r->d_counters);
+    cudaFree(r->d_hsp_off);
+    cudaFree(r->d_hsps);
+    cudaFree(r->d_keys);
+    cudaFreeHost(r->h_count);
+    delete r;
+}
+
+bp_status bp_blastp_host(bp_engine* e, const uint8_t* query, int32_t qlen, const bp_params* p,
+                         const uint8_t* residues, int64_t n_residues, const int64_t* offsets, int32_t n_subjects,
+                         int32_t* counters, int64_t* hsp_off, bp_hsp* hsps, int64_t hsp_cap, int64_t* n_hsps) {
+    if (!e) return BP_ERR_INVALID;
+    bp_db* db = nullptr;
+    bp_query* q = nullptr;
+    bp_result* r = nullptr;
+    bp_status st = bp_db_create(e, residues, n_residues, offsets, n_subjects, &db);
+    if (st == BP_OK) st = bp_query_create(e, query, qlen, p, &q);
+    if (st == BP_OK) st = bp_search(e, db, q, 0, -1, &r);
+    if (st == BP_OK) st = bp_result_wait(r);
+    if (st == BP_OK) {
+        if (n_hsps) *n_hsps = r->n_hsps;
+        if (hsps && r->n_hsps > hsp_cap) st = bp_set_error(e, BP_ERR_TOO_LARGE, "bp_blastp_host: hsp_cap too small");
+        else st = bp_result_copy(r, counters, hsp_off, hsps);
+    }
+    bp_result_destroy(r);
+    bp_query_destroy(q);
+    bp_db_destroy(db);
+    return st;
+}
+
+}  // extern "C"

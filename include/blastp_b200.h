@@ -1,0 +1,135 @@
+/*
+ * blastp_b200.h -- native C ABI of the B200 blastp preliminary-search engine:
+ * two-hit word finding + BLOSUM62 X-drop ungapped extension.
+ *
+ * Everything here is extern "C", plain pointers and sizes.  The reference's
+ * own entry points (GPU_BLASTP and family) are declared in
+ * gpu_cpu_common_b200.h and implemented on top of this engine.
+ *
+ * Reference interfaces replaced (file:line into avtomaton/blastp-cuda):
+ *   bp_search            GPU_BLASTP + GPU_BLASTP_get_data
+ *                        (gpu_blastp.cu:16-259, ncbi_blast_files/gpu_cpu_common.h:44-69),
+ *                        returning the full HSP set instead of 2 slots per subject
+ *   bp_query_create      the NCBI-built lookup table it consumes
+ *                        (BlastAaLookupTable, read at gpu_blastp.cu:45-61)
+ *   bp_db_create         the .gpu volume upload (gpu_blastp.cu:139-163,
+ *                        ncbi_blast_files/functions.cpp:620-699)
+ *   bp_hsp               GPUBlastInitHitList (ncbi_blast_files/gpu_cpu_common.h:29-38)
+ *   counters             d_Hits[oid*3+{0,1,2}] (gpu_blastp_kernel.cu:310-312)
+ *
+ * Status codes replace the reference's void returns; no call falls back to
+ * the CPU.  Device memory is owned by the handles; host buffers by the caller.
+ */
+#ifndef BLASTP_B200_H
+#define BLASTP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum bp_status {
+    BP_OK = 0,
+    BP_ERR_INVALID = 1,       /* bad argument (size, residue code, parameter) */
+    BP_ERR_CUDA = 2,          /* a CUDA runtime call failed; see bp_last_error() */
+    BP_ERR_NOMEM = 3,         /* device allocation failed */
+    BP_ERR_TOO_LARGE = 4,     /* input beyond a stated limit */
+    BP_ERR_TIMEOUT = 5,       /* a bounded device wait ran out */
+    BP_ERR_NOT_READY = 6,     /* asynchronous work still in flight */
+    BP_ERR_NO_DEVICE = 7      /* no CUDA device visible */
+} bp_status;
+
+/* Search parameters.  Defaults (bp_params_default): word 3, T 11, window 40,
+ * x_dropoff 16 raw (7 bits at lambda_u 0.3176), cutoff_score 41 raw. */
+typedef struct bp_params {
+    int32_t word_length;      /* must be 3 */
+    int32_t threshold;        /* neighbour-word score threshold T */
+    int32_t window;           /* two-hit window */
+    int32_t x_dropoff;        /* raw X-drop for ungapped extension */
+    int32_t cutoff_score;     /* raw score an HSP must reach to be reported */
+} bp_params;
+
+/* One ungapped HSP; same layout and meaning as GPUBlastInitHitList. */
+typedef struct bp_hsp {
+    int32_t hsp_q;            /* query start of the HSP */
+    int32_t hsp_s;            /* subject start of the HSP */
+    int32_t query_offset;     /* query offset of the second word hit */
+    int32_t subject_offset;   /* subject offset of the second word hit */
+    int32_t hsp_len;          /* HSP length */
+    int32_t score;            /* raw ungapped score */
+} bp_hsp;
+
+typedef struct bp_engine bp_engine;   /* device, stream, scratch */
+typedef struct bp_db bp_db;           /* HBM-resident subject database */
+typedef struct bp_query bp_query;     /* device query + neighbour-word table */
+typedef struct bp_result bp_result;   /* device counters + HSP CSR */
+
+/* Limits. */
+#define BP_MAX_QUERY_LENGTH 65535     /* query offsets are stored as uint16 */
+#define BP_ALPHABET 28                /* NCBIstdaa; residue codes 0..27 */
+
+void bp_params_default(bp_params* p);
+const char* bp_status_string(bp_status s);
+
+/* Host-side copy of the int8 28x28 BLOSUM62 (NCBIstdaa order) the engine
+ * scores with.  Needs no GPU. */
+void bp_blosum62_ncbistdaa(int8_t out[BP_ALPHABET * BP_ALPHABET]);
+
+/* Engine: binds a CUDA device and creates a non-blocking stream. */
+bp_status bp_engine_create(int device, bp_engine** out);
+void bp_engine_destroy(bp_engine* e);
+const char* bp_last_error(const bp_engine* e);
+void* bp_engine_stream(bp_engine* e);               /* cudaStream_t */
+uint64_t bp_engine_launch_count(const bp_engine* e); /* kernels launched so far */
+float bp_engine_last_scan_ms(const bp_engine* e);    /* scan kernel time of the last search */
+bp_status bp_engine_synchronize(bp_engine* e);
+
+/* Database: residues (NCBIstdaa, each < 28) of n_subjects subjects laid end
+ * to end, with n_subjects+1 int64 offsets.  bp_db_create copies from host
+ * memory (synchronously); bp_db_create_device copies from device memory. */
+bp_status bp_db_create(bp_engine* e, const uint8_t* residues, int64_t n_residues,
+                       const int64_t* offsets, int32_t n_subjects, bp_db** out);
+bp_status bp_db_create_device(bp_engine* e, const uint8_t* d_residues, int64_t n_residues,
+                              const int64_t* d_offsets, int32_t n_subjects, bp_db** out);
+void bp_db_destroy(bp_db* db);
+int32_t bp_db_subjects(const bp_db* db);
+int64_t bp_db_residues(const bp_db* db);
+
+/* Query: copies the residues to the device and builds the neighbour-word
+ * table there (CSR keyed by the packed 3-letter code, plus presence bitmap). */
+bp_status bp_query_create(bp_engine* e, const uint8_t* residues, int32_t length,
+                          const bp_params* params, bp_query** out);
+void bp_query_destroy(bp_query* q);
+/* Copies the table back: cell_start[32769] (uint32) and up to cap entries. */
+bp_status bp_query_table(bp_query* q, uint32_t* cell_start, uint16_t* entries, int64_t cap,
+                         int64_t* n_entries);
+
+/* Plain search of one query against subjects [first, first+count) of db
+ * (count < 0: to the end).  Enqueued on the engine stream; the result's
+ * buffers are valid once bp_result_wait returns BP_OK. */
+bp_status bp_search(bp_engine* e, const bp_db* db, const bp_query* q, int32_t first,
+                    int32_t count, bp_result** out);
+bp_status bp_result_wait(bp_result* r);
+int32_t bp_result_subjects(const bp_result* r);
+int64_t bp_result_hsps(const bp_result* r);          /* after bp_result_wait */
+/* Copies results to host memory.  Any pointer may be NULL.
+ *   counters  int32[3*subjects]: hits, successful extensions, extensions
+ *   hsp_off   int64[subjects+1]: CSR offsets into hsps
+ *   hsps      bp_hsp[bp_result_hsps()], per subject in discovery order */
+bp_status bp_result_copy(bp_result* r, int32_t* counters, int64_t* hsp_off, bp_hsp* hsps);
+void bp_result_destroy(bp_result* r);
+
+/* One call from host buffers to host buffers: uploads the database and the
+ * query, searches, and copies the results back (the end-to-end form).
+ * hsps may be NULL to only size the result (n_hsps out). */
+bp_status bp_blastp_host(bp_engine* e, const uint8_t* query, int32_t qlen, const bp_params* p,
+                         const uint8_t* residues, int64_t n_residues, const int64_t* offsets,
+                         int32_t n_subjects, int32_t* counters, int64_t* hsp_off,
+                         bp_hsp* hsps, int64_t hsp_cap, int64_t* n_hsps);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BLASTP_B200_H */
