@@ -59,7 +59,7 @@ SIGNATURES = {
     "bp_result_destroy": (None, [P]),
     "bp_blastp_host": (ctypes.c_int, [P, P, i32, P, P, i64, P, i32, P, P, P, i64, P]),
     # reference-compatible entry points
-    "GPU_BLASTP": (None, [P] * 8 + [ctypes.c_int, P, P, i32, P, i32] + [P] * 7),
+    "GPU_BLASTP": (None, [P] * 7 + [ctypes.c_int, P, P, i32, P, i32] + [P] * 7),
     "GPU_BLASTP_get_data": (None, [P, P, i32, P, P, i32, i32]),
     "GPU_BLASTP_free_memory": (None, [P] * 9),
     "GPU_BLASTP_check_memory": (ctypes.c_uint8, [P, P, P, ctypes.c_int, i32, i32, i32, i32, i32]),

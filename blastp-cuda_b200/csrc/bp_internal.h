@@ -4,11 +4,14 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
 #include <string>
+#include <vector>
 
 #include "blastp_b200.h"
 
-#define BP_NCELL 32768          // 3 letters x 5 bits
+#define BP_NCELL 32768          // reference layout: 3 letters x 5 bits
+#define BP_NC 19683             // compact layout: 27^3 words of letters 1..27
 #define BP_WORD 3
 #define BP_MROW 32              // device matrix row stride (28 used)
 
@@ -24,6 +27,7 @@ struct HspRec {
 struct bp_engine {
     int device = 0;
     int sm_count = 0;
+    int smem_optin = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_scan0 = nullptr, ev_scan1 = nullptr;
     uint64_t launches = 0;
@@ -33,35 +37,42 @@ struct bp_engine {
     // grow-only scratch shared by searches on this engine
     HspRec* d_recs = nullptr;
     uint32_t rec_cap = 0;
-    uint32_t* d_counts = nullptr;        // [0] records written, [1] work cursor, [2..] spare
-    uint32_t* h_counts = nullptr;        // pinned mirror of d_counts[0..3]
+    uint32_t* d_counts = nullptr;        // [0] records written, [1] subject cursor, [2] error word
     int32_t* d_fill = nullptr;           // per-subject fill cursors
     int32_t fill_cap = 0;
     int64_t* d_blocksums = nullptr;
     int32_t blocksum_cap = 0;
+    // pinned 4-word slots for per-search read-backs (cudaMallocHost is slow)
+    uint32_t* h_pool = nullptr;
+    std::vector<int> pool_free;
+    std::mutex pool_mu;
 };
+
+// A pinned 4-word slot from the engine's pool (or a fresh pinned block when
+// the pool is exhausted); returned with bp_pinned_put.
+uint32_t* bp_pinned_get(bp_engine* e);
+void bp_pinned_put(bp_engine* e, uint32_t* p);
 
 struct bp_db {
     bp_engine* e = nullptr;
-    uint8_t* d_res = nullptr;
+    uint8_t* d_res = nullptr;            // residues + 16 bytes of zero padding
     int64_t* d_off = nullptr;
     int32_t n = 0;
     int64_t nres = 0;
-    int32_t max_len = 0;
 };
 
 struct bp_query {
     bp_engine* e = nullptr;
     uint8_t* d_q = nullptr;
     int32_t qlen = 0;
-    uint32_t* d_cell_start = nullptr;    // BP_NCELL + 1
+    uint32_t* d_cells = nullptr;         // BP_NC + 1 compact cell starts
     uint16_t* d_entries = nullptr;
-    uint32_t* d_pv = nullptr;            // BP_NCELL / 32 words
     int64_t n_entries = 0;
     int32_t n_ctx = 1;
     int32_t* d_ctx = nullptr;            // n_ctx x {query_offset, x_dropoff, cutoff}
     bp_params p{};
     int32_t diag_mask = 0;
+    float hits_per_residue = 0.f;        // expected word hits per subject residue (background composition)
 };
 
 struct bp_result {
@@ -72,7 +83,7 @@ struct bp_result {
     bp_hsp* d_hsps = nullptr;
     int32_t* d_keys = nullptr;
     uint32_t cap = 0;
-    uint32_t* h_count = nullptr;         // pinned: records written by this search
+    uint32_t* h_count = nullptr;         // pinned: [0] records written, [1] unused, [2] error word
     int64_t n_hsps = -1;
     // to re-run on overflow
     const bp_db* db = nullptr;
@@ -88,9 +99,9 @@ struct ScanArgs {
     int32_t n;                  // subjects to scan
     const uint8_t* query;
     int32_t qlen;
-    const uint32_t* cell_start;
+    const uint32_t* cells;      // BP_NC + 1 compact cell starts
     const uint16_t* entries;
-    const uint32_t* pv;
+    int32_t n_entries;
     const int32_t* ctx;
     int32_t n_ctx;
     const int8_t* matrix;       // [28][32]
@@ -100,18 +111,25 @@ struct ScanArgs {
     HspRec* recs;
     uint32_t rec_cap;
     uint32_t* rec_count;
-    uint32_t* cursor;
+    uint32_t* cursor;           // subject cursor (chunks of 32)
+    uint32_t* error;            // set when a bounded wait runs out
 };
 
-// ---- host helpers (engine.cu) -------------------------------------------
+// ---- host helpers ---------------------------------------------------------
 bp_status bp_set_cuda_error(bp_engine* e, cudaError_t err, const char* what);
 bp_status bp_set_error(bp_engine* e, bp_status s, const std::string& msg);
 void bp_fill_matrix28(int8_t out[28 * 28]);
+// Expected word hits per subject residue of a table under the Robinson &
+// Robinson background, from its compact cell starts (BP_NC + 1).
+float bp_expected_hits_per_residue(const uint32_t* cells);
+int bp_cell_to_code15(int cell);
+// Largest query the scan kernel can take for a given window (shared-memory
+// diagonal array of one consumer warp).
+bool bp_scan_fits(int32_t qlen, int32_t diag_mask, int64_t n_entries, int smem_optin);
 
-// ---- launchers (table.cu / scan.cu) --------------------------------------
+// ---- launchers ------------------------------------------------------------
 cudaError_t bp_launch_table_build(bp_engine* e, const uint8_t* d_q, int32_t qlen, int32_t threshold,
-                                  uint32_t* d_cell_start, uint16_t* d_entries, uint32_t* d_pv,
-                                  uint32_t* d_counts_tmp, int64_t entry_cap, int pass);
+                                  uint32_t* d_cells, uint16_t* d_entries, uint32_t* d_counts_tmp, int pass);
 cudaError_t bp_launch_scan(bp_engine* e, const ScanArgs& a);
 cudaError_t bp_launch_order(bp_engine* e, int32_t n, const int32_t* d_counters, int64_t* d_hsp_off,
                             const HspRec* d_recs, uint32_t rec_cap, const uint32_t* d_rec_count,

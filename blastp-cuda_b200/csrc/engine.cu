@@ -4,8 +4,9 @@
 // GPU_BLASTP_free_memory (gpu_blastp.cu:16-280): instead of per-call
 // cudaMalloc of nine buffers, per-block replicas of the presence vector and
 // matrix, and a kernel launch without error checks, the engine keeps the
-// database and query tables resident, reuses grow-only scratch, checks every
-// CUDA call and returns a status.
+// database and query tables resident, reuses grow-only scratch, allocates
+// per-search outputs from the stream-ordered pool, checks every CUDA call and
+// returns a status.
 #include <stdio.h>
 #include <string.h>
 
@@ -14,9 +15,9 @@
 
 #include "bp_internal.h"
 
-#define CK(call, what)                                                 \
-    do {                                                               \
-        cudaError_t _err = (call);                                     \
+#define CK(call, what)                                                    \
+    do {                                                                  \
+        cudaError_t _err = (call);                                        \
         if (_err != cudaSuccess) return bp_set_cuda_error(e, _err, what); \
     } while (0)
 
@@ -39,10 +40,23 @@ int diag_mask_for(int qlen, int window) {
     return n - 1;
 }
 
-bool residues_valid(const uint8_t* p, int64_t n) {
-    uint8_t bad = 0;
-    for (int64_t i = 0; i < n; ++i) bad |= (uint8_t)(p[i] >= BP_ALPHABET);
-    return bad == 0;
+// Sets *bad when any residue code is >= 28 (16 bytes per thread per step).
+__global__ void check_residues(const uint8_t* __restrict__ res, int64_t n, uint32_t* bad) {
+    const int64_t n16 = n / 16;
+    uint32_t b = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n16; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint4 v = reinterpret_cast<const uint4*>(res)[i];
+        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            // a byte is >= 28 iff adding 100 sets its high bit or it already has it
+            const uint32_t x = w[k];
+            b |= (x | ((x & 0x7f7f7f7fu) + 0x64646464u)) & 0x80808080u;
+        }
+    }
+    if (blockIdx.x == 0)
+        for (int64_t i = n16 * 16 + threadIdx.x; i < n; i += blockDim.x) b |= res[i] >= BP_ALPHABET;
+    if (b) atomicOr(bad, 1u);
 }
 
 template <class T>
@@ -56,7 +70,36 @@ cudaError_t grow(T** p, size_t* cap_elems, size_t need) {
     return err;
 }
 
+constexpr int kPoolSlots = 1024;
+
 }  // namespace
+
+uint32_t* bp_pinned_get(bp_engine* e) {
+    {
+        std::lock_guard<std::mutex> lock(e->pool_mu);
+        if (e->h_pool && !e->pool_free.empty()) {
+            const int i = e->pool_free.back();
+            e->pool_free.pop_back();
+            return e->h_pool + 4 * i;
+        }
+    }
+    uint32_t* p = nullptr;
+    if (cudaMallocHost((void**)&p, 4 * sizeof(uint32_t)) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return p;
+}
+
+void bp_pinned_put(bp_engine* e, uint32_t* p) {
+    if (!p) return;
+    if (e->h_pool && p >= e->h_pool && p < e->h_pool + 4 * kPoolSlots) {
+        std::lock_guard<std::mutex> lock(e->pool_mu);
+        e->pool_free.push_back((int)((p - e->h_pool) / 4));
+    } else {
+        cudaFreeHost(p);
+    }
+}
 
 // Enqueues scan + ordering for r (subjects r->first.. of r->db against r->q)
 // on the engine stream.  Scratch is the engine's; outputs are r's.
@@ -64,7 +107,6 @@ bp_status bp_run_search(bp_engine* e, bp_result* r) {
     const bp_db* db = r->db;
     const bp_query* q = r->q;
     const int32_t n = r->n;
-    // scratch on the engine
     size_t cap = e->rec_cap;
     CK(grow(&e->d_recs, &cap, std::max<size_t>(r->cap, 65536)), "cudaMalloc(records)");
     e->rec_cap = (uint32_t)cap;
@@ -74,15 +116,14 @@ bp_status bp_run_search(bp_engine* e, bp_result* r) {
     size_t bcap = (size_t)e->blocksum_cap;
     CK(grow(&e->d_blocksums, &bcap, (size_t)bp_order_blocksums_needed(n)), "cudaMalloc(blocksums)");
     e->blocksum_cap = (int32_t)bcap;
-    // result buffers sized to the record buffer
     if (r->cap < e->rec_cap || !r->d_hsps) {
-        if (r->d_hsps) cudaFree(r->d_hsps);
-        if (r->d_keys) cudaFree(r->d_keys);
+        if (r->d_hsps) cudaFreeAsync(r->d_hsps, e->stream);
+        if (r->d_keys) cudaFreeAsync(r->d_keys, e->stream);
         r->d_hsps = nullptr;
         r->d_keys = nullptr;
         r->cap = e->rec_cap;
-        CK(cudaMalloc((void**)&r->d_hsps, (size_t)r->cap * sizeof(bp_hsp)), "cudaMalloc(hsps)");
-        CK(cudaMalloc((void**)&r->d_keys, (size_t)r->cap * sizeof(int32_t)), "cudaMalloc(keys)");
+        CK(cudaMallocAsync((void**)&r->d_hsps, (size_t)r->cap * sizeof(bp_hsp), e->stream), "cudaMallocAsync(hsps)");
+        CK(cudaMallocAsync((void**)&r->d_keys, (size_t)r->cap * sizeof(int32_t), e->stream), "cudaMallocAsync(keys)");
     }
     CK(cudaMemsetAsync(e->d_counts, 0, 4 * sizeof(uint32_t), e->stream), "memset(counts)");
 
@@ -93,9 +134,9 @@ bp_status bp_run_search(bp_engine* e, bp_result* r) {
     a.n = n;
     a.query = q->d_q;
     a.qlen = q->qlen;
-    a.cell_start = q->d_cell_start;
+    a.cells = q->d_cells;
     a.entries = q->d_entries;
-    a.pv = q->d_pv;
+    a.n_entries = (int32_t)q->n_entries;
     a.ctx = q->d_ctx;
     a.n_ctx = q->n_ctx;
     a.matrix = e->d_matrix;
@@ -106,13 +147,14 @@ bp_status bp_run_search(bp_engine* e, bp_result* r) {
     a.rec_cap = std::min(e->rec_cap, r->cap);
     a.rec_count = e->d_counts;
     a.cursor = e->d_counts + 1;
+    a.error = e->d_counts + 2;
     CK(cudaEventRecord(e->ev_scan0, e->stream), "cudaEventRecord");
     if (n > 0) CK(bp_launch_scan(e, a), "scan kernel launch");
     CK(cudaEventRecord(e->ev_scan1, e->stream), "cudaEventRecord");
-    CK(bp_launch_order(e, n, r->d_counters, r->d_hsp_off, e->d_recs, a.rec_cap, e->d_counts, e->d_fill,
-                       r->d_hsps, r->d_keys, e->d_blocksums),
+    CK(bp_launch_order(e, n, r->d_counters, r->d_hsp_off, e->d_recs, a.rec_cap, e->d_counts, e->d_fill, r->d_hsps,
+                       r->d_keys, e->d_blocksums),
        "order kernels launch");
-    CK(cudaMemcpyAsync(r->h_count, e->d_counts, sizeof(uint32_t), cudaMemcpyDeviceToHost, e->stream),
+    CK(cudaMemcpyAsync(r->h_count, e->d_counts, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, e->stream),
        "copy counts");
     r->n_hsps = -1;
     return BP_OK;
@@ -159,7 +201,9 @@ bp_status bp_engine_create(int device, bp_engine** out) {
     do {
         cudaError_t err;
         if ((err = cudaSetDevice(device)) != cudaSuccess) { st = bp_set_cuda_error(e, err, "cudaSetDevice"); break; }
-        if ((err = cudaDeviceGetAttribute(&e->sm_count, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess) {
+        if ((err = cudaDeviceGetAttribute(&e->sm_count, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess ||
+            (err = cudaDeviceGetAttribute(&e->smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device)) !=
+                cudaSuccess) {
             st = bp_set_cuda_error(e, err, "cudaDeviceGetAttribute"); break;
         }
         if ((err = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking)) != cudaSuccess) {
@@ -169,6 +213,13 @@ bp_status bp_engine_create(int device, bp_engine** out) {
             (err = cudaEventCreate(&e->ev_scan1)) != cudaSuccess) {
             st = bp_set_cuda_error(e, err, "cudaEventCreate"); break;
         }
+        // keep freed stream-ordered allocations cached in the pool
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        cudaGetLastError();
         int8_t m28[28 * 28], m32[28 * BP_MROW];
         bp_fill_matrix28(m28);
         for (int a = 0; a < 28; ++a)
@@ -178,9 +229,10 @@ bp_status bp_engine_create(int device, bp_engine** out) {
             st = bp_set_cuda_error(e, err, "matrix upload"); break;
         }
         if ((err = cudaMalloc((void**)&e->d_counts, 16 * sizeof(uint32_t))) != cudaSuccess ||
-            (err = cudaMallocHost((void**)&e->h_counts, 16 * sizeof(uint32_t))) != cudaSuccess) {
+            (err = cudaMallocHost((void**)&e->h_pool, kPoolSlots * 4 * sizeof(uint32_t))) != cudaSuccess) {
             st = bp_set_cuda_error(e, err, "counter alloc"); break;
         }
+        for (int i = kPoolSlots - 1; i >= 0; --i) e->pool_free.push_back(i);
     } while (0);
     if (st != BP_OK) {
         fprintf(stderr, "bp_engine_create: %s\n", e->err.c_str());
@@ -198,9 +250,9 @@ void bp_engine_destroy(bp_engine* e) {
     cudaFree(e->d_matrix);
     cudaFree(e->d_recs);
     cudaFree(e->d_counts);
-    cudaFreeHost(e->h_counts);
     cudaFree(e->d_fill);
     cudaFree(e->d_blocksums);
+    if (e->h_pool) cudaFreeHost(e->h_pool);
     if (e->ev_scan0) cudaEventDestroy(e->ev_scan0);
     if (e->ev_scan1) cudaEventDestroy(e->ev_scan1);
     if (e->stream) cudaStreamDestroy(e->stream);
@@ -223,13 +275,30 @@ static bp_status db_alloc(bp_engine* e, int64_t n_residues, int32_t n_subjects, 
     db->e = e;
     db->n = n_subjects;
     db->nres = n_residues;
-    cudaError_t err = cudaMalloc((void**)&db->d_res, (size_t)std::max<int64_t>(n_residues, 1) + 16);
+    cudaError_t err = cudaMalloc((void**)&db->d_res, (size_t)((n_residues + 15) & ~15LL) + 32);
     if (err == cudaSuccess) err = cudaMalloc((void**)&db->d_off, ((size_t)n_subjects + 1) * sizeof(int64_t));
     if (err != cudaSuccess) {
         bp_db_destroy(db);
         return bp_set_cuda_error(e, err, "cudaMalloc(database)");
     }
     *out = db;
+    return BP_OK;
+}
+
+// Zero padding after the residues, then the residue-code check on the device.
+static bp_status db_finish(bp_engine* e, bp_db* db) {
+    const size_t padded = (size_t)((db->nres + 15) & ~15LL) + 32;
+    CK(cudaMemsetAsync(db->d_res + db->nres, 0, padded - (size_t)db->nres, e->stream), "pad database");
+    CK(cudaMemsetAsync(e->d_counts + 3, 0, sizeof(uint32_t), e->stream), "memset(check)");
+    if (db->nres > 0) {
+        check_residues<<<e->sm_count * 4, 256, 0, e->stream>>>(db->d_res, db->nres, e->d_counts + 3);
+        e->launches += 1;
+        CK(cudaGetLastError(), "residue check launch");
+    }
+    uint32_t bad = 0;
+    CK(cudaMemcpyAsync(&bad, e->d_counts + 3, sizeof(uint32_t), cudaMemcpyDeviceToHost, e->stream), "read check");
+    CK(cudaStreamSynchronize(e->stream), "database upload");
+    if (bad) return bp_set_error(e, BP_ERR_INVALID, "database: residue code >= 28");
     return BP_OK;
 }
 
@@ -241,30 +310,31 @@ bp_status bp_db_create(bp_engine* e, const uint8_t* residues, int64_t n_residues
     if (offsets[0] != 0 || offsets[n_subjects] != n_residues)
         return bp_set_error(e, BP_ERR_INVALID, "bp_db_create: offsets must run from 0 to n_residues");
     for (int32_t i = 0; i < n_subjects; ++i)
-        if (offsets[i + 1] < offsets[i] || offsets[i + 1] - offsets[i] > INT32_MAX / 2)
-            return bp_set_error(e, BP_ERR_INVALID, "bp_db_create: offsets must be non-decreasing");
-    if (!residues_valid(residues, n_residues))
-        return bp_set_error(e, BP_ERR_INVALID, "bp_db_create: residue code >= 28");
+        if (offsets[i + 1] < offsets[i] || offsets[i + 1] - offsets[i] > (1 << 29))
+            return bp_set_error(e, BP_ERR_INVALID, "bp_db_create: offsets must be non-decreasing, subjects < 2^29");
     CK(cudaSetDevice(e->device), "cudaSetDevice");
     bp_db* db = nullptr;
     bp_status st = db_alloc(e, n_residues, n_subjects, &db);
     if (st != BP_OK) return st;
     cudaError_t err = cudaMemcpyAsync(db->d_res, residues, (size_t)n_residues, cudaMemcpyHostToDevice, e->stream);
-    if (err == cudaSuccess) err = cudaMemsetAsync(db->d_res + n_residues, 0, 16, e->stream);
     if (err == cudaSuccess)
-        err = cudaMemcpyAsync(db->d_off, offsets, ((size_t)n_subjects + 1) * sizeof(int64_t),
-                              cudaMemcpyHostToDevice, e->stream);
-    if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
+        err = cudaMemcpyAsync(db->d_off, offsets, ((size_t)n_subjects + 1) * sizeof(int64_t), cudaMemcpyHostToDevice,
+                              e->stream);
     if (err != cudaSuccess) {
         bp_db_destroy(db);
         return bp_set_cuda_error(e, err, "database upload");
+    }
+    st = db_finish(e, db);
+    if (st != BP_OK) {
+        bp_db_destroy(db);
+        return st;
     }
     *out = db;
     return BP_OK;
 }
 
-bp_status bp_db_create_device(bp_engine* e, const uint8_t* d_residues, int64_t n_residues,
-                              const int64_t* d_offsets, int32_t n_subjects, bp_db** out) {
+bp_status bp_db_create_device(bp_engine* e, const uint8_t* d_residues, int64_t n_residues, const int64_t* d_offsets,
+                              int32_t n_subjects, bp_db** out) {
     if (!e || !out || !d_offsets || n_subjects < 0 || n_residues < 0)
         return bp_set_error(e, BP_ERR_INVALID, "bp_db_create_device: bad argument");
     *out = nullptr;
@@ -273,17 +343,24 @@ bp_status bp_db_create_device(bp_engine* e, const uint8_t* d_residues, int64_t n
     CK(cudaMemcpy(off.data(), d_offsets, off.size() * sizeof(int64_t), cudaMemcpyDeviceToHost), "read offsets");
     if (off[0] != 0 || off[n_subjects] != n_residues)
         return bp_set_error(e, BP_ERR_INVALID, "bp_db_create_device: offsets must run from 0 to n_residues");
+    for (int32_t i = 0; i < n_subjects; ++i)
+        if (off[i + 1] < off[i] || off[i + 1] - off[i] > (1 << 29))
+            return bp_set_error(e, BP_ERR_INVALID, "bp_db_create_device: offsets must be non-decreasing");
     bp_db* db = nullptr;
     bp_status st = db_alloc(e, n_residues, n_subjects, &db);
     if (st != BP_OK) return st;
-    cudaError_t err = cudaMemcpyAsync(db->d_res, d_residues, (size_t)n_residues, cudaMemcpyDeviceToDevice, e->stream);
-    if (err == cudaSuccess) err = cudaMemsetAsync(db->d_res + n_residues, 0, 16, e->stream);
+    cudaError_t err =
+        cudaMemcpyAsync(db->d_res, d_residues, (size_t)n_residues, cudaMemcpyDeviceToDevice, e->stream);
     if (err == cudaSuccess)
         err = cudaMemcpyAsync(db->d_off, d_offsets, off.size() * sizeof(int64_t), cudaMemcpyDeviceToDevice, e->stream);
-    if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
     if (err != cudaSuccess) {
         bp_db_destroy(db);
         return bp_set_cuda_error(e, err, "database copy");
+    }
+    st = db_finish(e, db);
+    if (st != BP_OK) {
+        bp_db_destroy(db);
+        return st;
     }
     *out = db;
     return BP_OK;
@@ -299,8 +376,7 @@ void bp_db_destroy(bp_db* db) {
 int32_t bp_db_subjects(const bp_db* db) { return db ? db->n : 0; }
 int64_t bp_db_residues(const bp_db* db) { return db ? db->nres : 0; }
 
-bp_status bp_query_create(bp_engine* e, const uint8_t* residues, int32_t length, const bp_params* p,
-                          bp_query** out) {
+bp_status bp_query_create(bp_engine* e, const uint8_t* residues, int32_t length, const bp_params* p, bp_query** out) {
     if (!e || !out || !p || length < 0 || (length > 0 && !residues))
         return bp_set_error(e, BP_ERR_INVALID, "bp_query_create: bad argument");
     *out = nullptr;
@@ -323,10 +399,9 @@ bp_status bp_query_create(bp_engine* e, const uint8_t* residues, int32_t length,
     do {
         cudaError_t err;
         if ((err = cudaMalloc((void**)&q->d_q, (size_t)((length + 15) & ~15) + 16)) != cudaSuccess ||
-            (err = cudaMalloc((void**)&q->d_cell_start, (BP_NCELL + 1) * sizeof(uint32_t))) != cudaSuccess ||
-            (err = cudaMalloc((void**)&q->d_pv, (BP_NCELL / 32) * sizeof(uint32_t))) != cudaSuccess ||
+            (err = cudaMalloc((void**)&q->d_cells, (BP_NC + 1) * sizeof(uint32_t))) != cudaSuccess ||
             (err = cudaMalloc((void**)&q->d_ctx, 3 * sizeof(int32_t))) != cudaSuccess ||
-            (err = cudaMalloc((void**)&d_tmp, BP_NCELL * sizeof(uint32_t))) != cudaSuccess) {
+            (err = cudaMalloc((void**)&d_tmp, BP_NC * sizeof(uint32_t))) != cudaSuccess) {
             st = bp_set_cuda_error(e, err, "cudaMalloc(query)"); break;
         }
         if (length > 0 &&
@@ -335,21 +410,22 @@ bp_status bp_query_create(bp_engine* e, const uint8_t* residues, int32_t length,
         }
         int32_t ctx[3] = {0, p->x_dropoff, p->cutoff_score};
         if ((err = cudaMemcpyAsync(q->d_ctx, ctx, sizeof(ctx), cudaMemcpyHostToDevice, e->stream)) != cudaSuccess ||
-            (err = bp_launch_table_build(e, q->d_q, length, p->threshold, q->d_cell_start, nullptr, q->d_pv, d_tmp, 0, 0)) !=
-                cudaSuccess) {
+            (err = bp_launch_table_build(e, q->d_q, length, p->threshold, q->d_cells, nullptr, d_tmp, 0)) != cudaSuccess) {
             st = bp_set_cuda_error(e, err, "table count"); break;
         }
-        uint32_t total = 0;
-        if ((err = cudaMemcpyAsync(&total, q->d_cell_start + BP_NCELL, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+        std::vector<uint32_t> cells(BP_NC + 1);
+        if ((err = cudaMemcpyAsync(cells.data(), q->d_cells, cells.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost,
                                    e->stream)) != cudaSuccess ||
             (err = cudaStreamSynchronize(e->stream)) != cudaSuccess) {
             st = bp_set_cuda_error(e, err, "table size"); break;
         }
+        const uint32_t total = cells[BP_NC];
         q->n_entries = total;
+        q->hits_per_residue = bp_expected_hits_per_residue(cells.data());
         if ((err = cudaMalloc((void**)&q->d_entries, (size_t)std::max<uint32_t>(total, 1) * sizeof(uint16_t))) !=
                 cudaSuccess ||
-            (err = bp_launch_table_build(e, q->d_q, length, p->threshold, q->d_cell_start, q->d_entries, q->d_pv,
-                                         d_tmp, total, 1)) != cudaSuccess ||
+            (err = bp_launch_table_build(e, q->d_q, length, p->threshold, q->d_cells, q->d_entries, d_tmp, 1)) !=
+                cudaSuccess ||
             (err = cudaStreamSynchronize(e->stream)) != cudaSuccess) {
             st = bp_set_cuda_error(e, err, "table fill"); break;
         }
@@ -366,9 +442,8 @@ bp_status bp_query_create(bp_engine* e, const uint8_t* residues, int32_t length,
 void bp_query_destroy(bp_query* q) {
     if (!q) return;
     cudaFree(q->d_q);
-    cudaFree(q->d_cell_start);
+    cudaFree(q->d_cells);
     cudaFree(q->d_entries);
-    cudaFree(q->d_pv);
     cudaFree(q->d_ctx);
     delete q;
 }
@@ -379,9 +454,19 @@ bp_status bp_query_table(bp_query* q, uint32_t* cell_start, uint16_t* entries, i
     CK(cudaSetDevice(e->device), "cudaSetDevice");
     CK(cudaStreamSynchronize(e->stream), "sync");
     if (n_entries) *n_entries = q->n_entries;
-    if (cell_start)
-        CK(cudaMemcpy(cell_start, q->d_cell_start, (BP_NCELL + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost),
-           "copy table");
+    if (cell_start) {
+        // expand the compact starts to the reference's 15-bit index (same entry order)
+        std::vector<uint32_t> cells(BP_NC + 1);
+        CK(cudaMemcpy(cells.data(), q->d_cells, cells.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost), "copy table");
+        std::vector<uint32_t> cnt(BP_NCELL, 0);
+        for (int c = 0; c < BP_NC; ++c) cnt[bp_cell_to_code15(c)] = cells[c + 1] - cells[c];
+        uint32_t acc = 0;
+        for (int c = 0; c < BP_NCELL; ++c) {
+            cell_start[c] = acc;
+            acc += cnt[c];
+        }
+        cell_start[BP_NCELL] = acc;
+    }
     if (entries && q->n_entries > 0)
         CK(cudaMemcpy(entries, q->d_entries, (size_t)std::min<int64_t>(cap, q->n_entries) * sizeof(uint16_t),
                       cudaMemcpyDeviceToHost),
@@ -389,14 +474,12 @@ bp_status bp_query_table(bp_query* q, uint32_t* cell_start, uint16_t* entries, i
     return BP_OK;
 }
 
-bp_status bp_search(bp_engine* e, const bp_db* db, const bp_query* q, int32_t first, int32_t count,
-                    bp_result** out) {
+bp_status bp_search(bp_engine* e, const bp_db* db, const bp_query* q, int32_t first, int32_t count, bp_result** out) {
     if (!e || !db || !q || !out || first < 0 || first > db->n)
         return bp_set_error(e, BP_ERR_INVALID, "bp_search: bad argument");
     *out = nullptr;
     if (count < 0 || count > db->n - first) count = db->n - first;
-    const int L = q->diag_mask + 1;
-    if ((size_t)L * 4 + 1024 + 4096 + 65552 > 227 * 1024)
+    if (!bp_scan_fits(q->qlen, q->diag_mask, q->n_entries, e->smem_optin))
         return bp_set_error(e, BP_ERR_TOO_LARGE, "bp_search: query too long for the shared-memory diagonal array");
     CK(cudaSetDevice(e->device), "cudaSetDevice");
     bp_result* r = new bp_result();
@@ -406,12 +489,12 @@ bp_status bp_search(bp_engine* e, const bp_db* db, const bp_query* q, int32_t fi
     r->q = q;
     r->first = first;
     r->cap = 0;
-    cudaError_t err = cudaMalloc((void**)&r->d_counters, (size_t)std::max(count, 1) * 3 * sizeof(int32_t));
-    if (err == cudaSuccess) err = cudaMalloc((void**)&r->d_hsp_off, ((size_t)count + 1) * sizeof(int64_t));
-    if (err == cudaSuccess) err = cudaMallocHost((void**)&r->h_count, sizeof(uint32_t));
+    cudaError_t err = cudaMallocAsync((void**)&r->d_counters, (size_t)std::max(count, 1) * 3 * sizeof(int32_t), e->stream);
+    if (err == cudaSuccess) err = cudaMallocAsync((void**)&r->d_hsp_off, ((size_t)count + 1) * sizeof(int64_t), e->stream);
+    if (err == cudaSuccess && !(r->h_count = bp_pinned_get(e))) err = cudaErrorMemoryAllocation;
     if (err != cudaSuccess) {
         bp_result_destroy(r);
-        return bp_set_cuda_error(e, err, "cudaMalloc(result)");
+        return bp_set_cuda_error(e, err, "allocate result");
     }
     bp_status st = bp_run_search(e, r);
     if (st != BP_OK) {
@@ -432,7 +515,8 @@ bp_status bp_result_wait(bp_result* r) {
         float ms = 0.f;
         if (cudaEventElapsedTime(&ms, e->ev_scan0, e->ev_scan1) == cudaSuccess) e->last_scan_ms = ms;
         cudaGetLastError();
-        const uint32_t count = *r->h_count;
+        if (r->h_count[2]) return bp_set_error(e, BP_ERR_TIMEOUT, "scan kernel: a bounded wait ran out");
+        const uint32_t count = r->h_count[0];
         if (count <= r->cap) {
             r->n_hsps = count;
             return BP_OK;
@@ -442,8 +526,8 @@ bp_status bp_result_wait(bp_result* r) {
         size_t cap = e->rec_cap;
         CK(grow(&e->d_recs, &cap, r->cap), "cudaMalloc(records)");
         e->rec_cap = (uint32_t)cap;
-        cudaFree(r->d_hsps);
-        cudaFree(r->d_keys);
+        cudaFreeAsync(r->d_hsps, e->stream);
+        cudaFreeAsync(r->d_keys, e->stream);
         r->d_hsps = nullptr;
         r->d_keys = nullptr;
         bp_status st = bp_run_search(e, r);
@@ -461,23 +545,28 @@ bp_status bp_result_copy(bp_result* r, int32_t* counters, int64_t* hsp_off, bp_h
     if (st != BP_OK) return st;
     bp_engine* e = r->e;
     if (counters && r->n > 0)
-        CK(cudaMemcpy(counters, r->d_counters, (size_t)r->n * 3 * sizeof(int32_t), cudaMemcpyDeviceToHost),
+        CK(cudaMemcpyAsync(counters, r->d_counters, (size_t)r->n * 3 * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                           e->stream),
            "copy counters");
     if (hsp_off)
-        CK(cudaMemcpy(hsp_off, r->d_hsp_off, ((size_t)r->n + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost),
+        CK(cudaMemcpyAsync(hsp_off, r->d_hsp_off, ((size_t)r->n + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost,
+                           e->stream),
            "copy offsets");
     if (hsps && r->n_hsps > 0)
-        CK(cudaMemcpy(hsps, r->d_hsps, (size_t)r->n_hsps * sizeof(bp_hsp), cudaMemcpyDeviceToHost), "copy hsps");
+        CK(cudaMemcpyAsync(hsps, r->d_hsps, (size_t)r->n_hsps * sizeof(bp_hsp), cudaMemcpyDeviceToHost, e->stream),
+           "copy hsps");
+    CK(cudaStreamSynchronize(e->stream), "copy results");
     return BP_OK;
 }
 
 void bp_result_destroy(bp_result* r) {
     if (!r) return;
-    cudaFree(r->d_counters);
-    cudaFree(r->d_hsp_off);
-    cudaFree(r->d_hsps);
-    cudaFree(r->d_keys);
-    cudaFreeHost(r->h_count);
+    bp_engine* e = r->e;
+    if (r->d_counters) cudaFreeAsync(r->d_counters, e->stream);
+    if (r->d_hsp_off) cudaFreeAsync(r->d_hsp_off, e->stream);
+    if (r->d_hsps) cudaFreeAsync(r->d_hsps, e->stream);
+    if (r->d_keys) cudaFreeAsync(r->d_keys, e->stream);
+    bp_pinned_put(e, r->h_count);
     delete r;
 }
 

@@ -152,8 +152,14 @@ Boolean GPU_BLASTP_check_memory(const LookupTableWrap* lookup_wrap, const Blast_
     if (num_queries > NUM_QUERIES_MAX_B200 || query_length > QUERY_LENGTH_MAX_B200) return FALSE;
     const BlastAaLookupTable* lookup = (const BlastAaLookupTable*)lookup_wrap->lut;
     if (lookup->word_length != 3 || lookup->charsize != 5) return FALSE;
-    const int L = ewp->diag_table->diag_array_length;
-    if ((size_t)L * 4 + 1024 + 4096 + (size_t)query_length + 16 > 227 * 1024) return FALSE;
+    int dev = 0, optin = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return FALSE;
+    }
+    // any table size fits when it stays in global memory; the diagonal array must fit shared memory
+    if (!bp_scan_fits(query_length, ewp->diag_table->diag_mask, 1 << 30, optin)) return FALSE;
     const size_t n = (size_t)gpu_options->num_sequences_to;
     size_t need = 2 * (size_t)h_Database2Dpadded_bytes + 8 * (n + 1) + (size_t)h_Hits_bytes +
                   3 * (size_t)h_GPUBlastInitHitList_bytes + (BP_NCELL + 1) * 4 +
@@ -218,33 +224,36 @@ void GPU_BLASTP(const BLAST_SequenceBlk* query, const BlastQueryInfo* query_info
         if (why) break;
         gbase[n_groups] = vol;
         if (vol > h_Database2Dpadded_bytes) { why = "database smaller than its group lengths"; break; }
-        const int L = ewp->diag_table->diag_mask + 1;
-        if ((size_t)L * 4 + 1024 + 4096 + (size_t)Q + 16 > 227 * 1024) { why = "query too long for the diagonal array"; break; }
-
-        // 1. NCBI table -> CSR.  A cell counts only when its presence bit is set,
-        // as the reference tests the bit first (gpu_blastp_kernel.cu:182-192).
+        // 1. NCBI table -> compact CSR over the 27^3 words of letters 1..27 (a
+        // word holding the gap letter or a code >= 28 can never be scanned:
+        // such words have no cell).  A cell counts only when its presence bit
+        // is set, as the reference tests the bit first
+        // (gpu_blastp_kernel.cu:182-192).
         const AaLookupSmallboneCell* cells = (const AaLookupSmallboneCell*)lookup->thick_backbone;
         const Uint2* ovf = (const Uint2*)lookup->overflow;
         const PV_ARRAY_TYPE* pv = lookup->pv;
         const int ncell = lookup->backbone_size < BP_NCELL ? lookup->backbone_size : BP_NCELL;
-        std::vector<uint32_t> cell_start(BP_NCELL + 1);
+        std::vector<uint32_t> cell_start(BP_NC + 1);
         std::vector<uint16_t> entries;
-        std::vector<uint32_t> pv_out(BP_NCELL / 32, 0);
-        for (int c = 0; c < BP_NCELL; ++c) {
-            cell_start[c] = (uint32_t)entries.size();
+        for (int cc = 0; cc < BP_NC; ++cc) {
+            cell_start[cc] = (uint32_t)entries.size();
+            const int c = bp_cell_to_code15(cc);
             if (c >= ncell || !(pv[c >> 5] & (1u << (c & 31)))) continue;
             const int used = cells[c].num_used;
             if (used <= 0) continue;
-            pv_out[c >> 5] |= 1u << (c & 31);
             const Uint2* src = used <= AA_HITS_PER_CELL ? cells[c].payload.entries
                                                         : ovf + cells[c].payload.overflow_cursor;
             entries.insert(entries.end(), src, src + used);
         }
-        cell_start[BP_NCELL] = (uint32_t)entries.size();
+        cell_start[BP_NC] = (uint32_t)entries.size();
         // every listed offset must start a whole word of the query
         for (uint16_t x : entries)
             if ((int32_t)x + 3 > Q) { why = "lookup table lists an offset beyond the query"; break; }
         if (why) break;
+        if (!bp_scan_fits(Q, ewp->diag_table->diag_mask, (int64_t)cell_start[BP_NC], e->smem_optin)) {
+            why = "query too long for the shared-memory diagonal array";
+            break;
+        }
         if (entries.empty()) entries.push_back(0);
 
         if (nq < 1) { why = "no query context"; break; }
@@ -279,7 +288,7 @@ void GPU_BLASTP(const BLAST_SequenceBlk* query, const BlastQueryInfo* query_info
         up((void**)d_Database2Dpadded, h_Database2Dpadded, (size_t)h_Database2Dpadded_bytes);
         up((void**)d_RepeatedSubstitutionMatrix, m32, sizeof(m32));
         up((void**)d_RepeatedSequence_length_vector, Sequence_length_vector, (size_t)n_groups * 4);
-        up((void**)d_RepeatedPV, pv_out.data(), pv_out.size() * 4);
+        *d_RepeatedPV = nullptr;   // the compact table needs no presence vector
         up((void**)d_ThickBackbone, cell_start.data(), cell_start.size() * 4);
         up((void**)d_overflow, entries.data(), entries.size() * 2);
         // arena: flat volume | offsets | group bases | query | contexts
@@ -323,15 +332,15 @@ void GPU_BLASTP(const BLAST_SequenceBlk* query, const BlastQueryInfo* query_info
         job->q.e = e;
         job->q.d_q = d_q;
         job->q.qlen = Q;
-        job->q.d_cell_start = (uint32_t*)*d_ThickBackbone;
+        job->q.d_cells = (uint32_t*)*d_ThickBackbone;
         job->q.d_entries = *d_overflow;
-        job->q.d_pv = *d_RepeatedPV;
-        job->q.n_entries = cell_start[BP_NCELL];
+        job->q.n_entries = cell_start[BP_NC];
         job->q.n_ctx = nq;
         job->q.d_ctx = d_ctx;
         job->q.p.word_length = 3;
         job->q.p.window = ewp->diag_table->window;
         job->q.diag_mask = ewp->diag_table->diag_mask;
+        job->q.hits_per_residue = bp_expected_hits_per_residue(cell_start.data());
         job->r.e = e;
         job->r.n = n;
         job->r.db = &job->db;
@@ -339,7 +348,7 @@ void GPU_BLASTP(const BLAST_SequenceBlk* query, const BlastQueryInfo* query_info
         job->r.first = 0;
         job->r.d_counters = *d_Hits;
         if ((err = cudaMalloc((void**)&job->r.d_hsp_off, ((size_t)n + 1) * 8)) != cudaSuccess ||
-            (err = cudaMallocHost((void**)&job->r.h_count, 4)) != cudaSuccess) {
+            !(job->r.h_count = bp_pinned_get(e))) {
             why = "result allocation";
             break;
         }
@@ -398,9 +407,12 @@ void GPU_BLASTP_free_memory(Int4** d_Hits, GPUBlastInitHitList** d_GPUBlastInitH
         LegacyJob* job = it->second;
         if (job->e) cudaStreamSynchronize(job->e->stream);
         cudaFree(job->r.d_hsp_off);
-        cudaFree(job->r.d_hsps);
-        cudaFree(job->r.d_keys);
-        cudaFreeHost(job->r.h_count);
+        if (job->e) {
+            if (job->r.d_hsps) cudaFreeAsync(job->r.d_hsps, job->e->stream);
+            if (job->r.d_keys) cudaFreeAsync(job->r.d_keys, job->e->stream);
+            cudaStreamSynchronize(job->e->stream);
+        }
+        if (job->e) bp_pinned_put(job->e, job->r.h_count);
         delete job;
         g_jobs.erase(it);
     }

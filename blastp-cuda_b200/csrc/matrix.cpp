@@ -50,6 +50,29 @@ int code_of(char c) { return (int)(strchr(kNcbiStdaa, c) - kNcbiStdaa); }
 
 }  // namespace
 
+// Robinson & Robinson (1991) background, per 1000, in NCBIstdaa code order
+// (0 for non-standard letters).
+static const float kBackground[28] = {0,     78.05, 0,     19.25, 53.64, 62.95, 38.56, 73.77, 21.99, 51.42,
+                                      57.44, 90.19, 22.43, 44.87, 52.03, 42.64, 51.29, 71.20, 58.41, 64.41,
+                                      13.30, 0,     32.16, 0,     0,     0,     0,     0};
+
+float bp_expected_hits_per_residue(const uint32_t* cells) {
+    double h = 0.0;
+    for (int a = 1; a < 28; ++a) {
+        if (kBackground[a] == 0.f) continue;
+        for (int b = 1; b < 28; ++b) {
+            if (kBackground[b] == 0.f) continue;
+            const double pab = (double)kBackground[a] * kBackground[b] * 1e-6;
+            for (int c = 1; c < 28; ++c) {
+                if (kBackground[c] == 0.f) continue;
+                const int cell = (a - 1) * 729 + (b - 1) * 27 + (c - 1);
+                h += pab * kBackground[c] * 1e-3 * (double)(cells[cell + 1] - cells[cell]);
+            }
+        }
+    }
+    return (float)h;
+}
+
 void bp_fill_matrix28(int8_t out[28 * 28]) {
     const int star = code_of('*');
     for (int a = 0; a < 28; ++a)

@@ -3,28 +3,57 @@
 // Semantics follow the reference kernel GPU_BLASTP_kernelTwoHit
 // (gpu_blastp_kernel.cu:42-320) and its extenders (:341-549); the mapping to
 // the hardware does not:
-//  * a warp owns one subject at a time (subjects handed out by an atomic
-//    cursor, so length skew does not idle a CTA) instead of a thread per
-//    subject;
-//  * the warp reads 32 consecutive word positions, looks them up in the
-//    presence bitmap (shared memory) and the CSR table, and flattens the
-//    resulting word hits into chunks of 32 -- one hit per lane, whatever the
-//    per-position hit counts are;
+//  * one persistent CTA per SM with up to 32 warps; the query, the scoring
+//    matrix and (when they fit) the compact neighbour-word table are loaded
+//    into shared memory once and shared by every warp for the whole launch;
+//  * a warp owns one subject at a time, taken from a global cursor.  Each
+//    warp runs a three-stage software pipeline over its subjects: cursor grab
+//    (i+3), offsets load (i+2), cp.async.bulk L2 prefetch of the residues
+//    (i+1), scan (i) -- so the database is streamed from HBM into L2 ahead of
+//    the warp that reads it;
+//  * the warp reads 128 consecutive word positions (4 per lane, contiguous),
+//    loading the next window's residues while it works on the current one,
+//    looks the words up in the table and flattens the resulting word hits
+//    into chunks of 32 -- one hit per lane, whatever the per-position hit
+//    counts are;
 //  * the per-diagonal two-hit state lives in shared memory, one array per
 //    warp (the reference keeps it in global memory, one per thread);
-//  * hits of one chunk that fall on the same diagonal are ordered with
-//    __match_any_sync: they are applied in word-position order, which is the
-//    only order the state machine depends on (distinct diagonals are
-//    independent);
+//  * hits of one chunk on the same diagonal are applied in word-position
+//    order (__match_any_sync), the only order the state machine depends on;
+//    distinct diagonals are independent;
+//  * each X-drop extension is walked by the whole warp, 32 letters per step:
+//    prefix sums give the running scores, prefix maxima the best score so
+//    far, and a ballot the first letter where the drop reaches x_drop (or,
+//    walking right, where the score falls to 0) -- the same stop and the same
+//    best offset as the reference's letter-by-letter loops;
 //  * surviving HSPs are compacted with a warp ballot into one global append
 //    buffer, tagged with the subject and the hit's index in the subject's hit
-//    stream so a later pass can restore the reference's discovery order.
+//    stream, from which the ordering pass restores the discovery order.
 #include "bp_internal.h"
+
+extern __shared__ __align__(128) uint8_t bp_smem[];
 
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr uint32_t kFlag = 0x80000000u;
+constexpr int kP = 4;                       // word positions per lane per window
+constexpr int kMaxWarps = 32;
+
+}  // namespace
+
+// Shared-memory layout of one launch (host computes, kernel reads).
+struct ScanLayout {
+    int warps;
+    int cells_mode;        // 0: u16 starts in smem, 1: u32 starts in smem, 2: u32 starts in global
+    int entries_smem;
+    int L;
+    int off_cells, off_entries, off_query, off_warps;
+    int warp_bytes;        // diagonal array + per-lane position table
+    int total;
+};
+
+namespace {
 
 struct ExtOut {
     int hsp_q, hsp_s, len, score, s_last, right_ext;
@@ -32,12 +61,68 @@ struct ExtOut {
 
 __device__ __forceinline__ int msc(const int8_t* m, int a, int b) { return m[a * BP_MROW + b]; }
 
+__device__ __forceinline__ int warp_incl_sum(int x, int lane) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(kFull, x, o);
+        if (lane >= o) x += y;
+    }
+    return x;
+}
+
+__device__ __forceinline__ int warp_incl_max(int x, int lane) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(kFull, x, o);
+        if (lane >= o) x = max(x, y);
+    }
+    return x;
+}
+
+// One X-drop walk, 32 letters per iteration.  Letter i (i = 0..n-1) scores
+// m[q(i)][s(i)] with q(i) = qry[q0 + dir*i], s(i) = subj[s0 + dir*i].  The
+// running score starts at `start`, the best at `start`; the walk stops after
+// the first letter where best - run >= xdrop (or, when walking right,
+// run <= 0).  Returns the best score, the index of the letter that first
+// reached it (-1 if none), and the index of the stopping letter (n if the
+// walk ran out of letters).  All lanes return the same values.
+template <bool kRight>
+__device__ __forceinline__ void warp_xdrop(const int8_t* m, const uint8_t* __restrict__ subj, const uint8_t* qry,
+                                           int s0, int q0, int n, int start, int xdrop, int lane, int& best,
+                                           int& best_i, int& stop_i) {
+    int carry = start;
+    best = start;
+    best_i = -1;
+    stop_i = n;
+    for (int i0 = 0; i0 < n; i0 += 32) {
+        const int i = i0 + lane;
+        const bool valid = i < n;
+        int v = 0;
+        if (valid) v = kRight ? msc(m, qry[q0 + i], __ldg(subj + s0 + i)) : msc(m, qry[q0 - i], __ldg(subj + s0 - i));
+        const int run = carry + warp_incl_sum(v, lane);
+        const int pm = max(best, warp_incl_max(run, lane));
+        const bool stop = valid && ((pm - run >= xdrop) || (kRight && run <= 0));
+        const unsigned sb = __ballot_sync(kFull, stop);
+        const int last = sb ? (__ffs(sb) - 1) : min(31, n - 1 - i0);
+        const int nb = __shfl_sync(kFull, pm, last);
+        if (nb > best) {
+            const unsigned at = __ballot_sync(kFull, valid && lane <= last && run == nb);
+            best_i = i0 + __ffs(at) - 1;
+            best = nb;
+        }
+        carry = __shfl_sync(kFull, run, last);
+        if (sb) {
+            stop_i = i0 + last;
+            break;
+        }
+    }
+}
+
 // s_BlastAaExtendTwoHit (gpu_blastp_kernel.cu:341-415) with the left
-// (:435-481) and right (:503-549) X-drop walks inlined.  Subject read through
-// the read-only path, query and matrix from shared memory.
-__device__ ExtOut extend_two_hit(const int8_t* m, const uint8_t* __restrict__ subj, int slen,
-                                 const uint8_t* qry, int qlen, int s_left, int s_right,
-                                 int q_right, int xdrop) {
+// (:435-481) and right (:503-549) walks done by the whole warp.  Every lane
+// passes the same arguments and gets the same result.
+__device__ ExtOut warp_extend_two_hit(const int8_t* m, const uint8_t* __restrict__ subj, int slen, const uint8_t* qry,
+                                      int qlen, int s_left, int s_right, int q_right, int xdrop, int lane) {
     int score = 0, left_score = 0, shift = 0;
 #pragma unroll
     for (int i = 0; i < BP_WORD; ++i) {
@@ -50,19 +135,11 @@ __device__ ExtOut extend_two_hit(const int8_t* m, const uint8_t* __restrict__ su
     q_right += shift;
     s_right += shift;
 
-    int s_off = s_right - 1, q_off = q_right - 1;
-    int n = min(s_off, q_off);
-    int run = 0, best = 0, best_k = -1;
-    for (int k = 0; k <= n; ++k) {
-        run += msc(m, qry[q_off - k], __ldg(subj + s_off - k));
-        if (run > best) {
-            best = run;
-            best_k = k;
-        }
-        if (best - run >= xdrop) break;
-    }
-    int left_d = best_k + 1;
-    left_score = best;
+    int lbest, lbest_k, lstop;
+    const int nl = min(s_right - 1, q_right - 1) + 1;
+    warp_xdrop<false>(m, subj, qry, s_right - 1, q_right - 1, nl, 0, xdrop, lane, lbest, lbest_k, lstop);
+    const int left_d = lbest_k + 1;
+    left_score = lbest;
 
     ExtOut o;
     o.right_ext = 0;
@@ -70,19 +147,12 @@ __device__ ExtOut extend_two_hit(const int8_t* m, const uint8_t* __restrict__ su
     int right_d = 0, right_score = 0;
     if (left_d >= s_right - s_left) {
         o.right_ext = 1;
-        int n2 = min(slen - s_right, qlen - q_right);
-        int rrun = left_score, rbest = left_score, rbest_i = -1, i = 0;
-        for (; i < n2; ++i) {
-            rrun += msc(m, qry[q_right + i], __ldg(subj + s_right + i));
-            if (rrun > rbest) {
-                rbest = rrun;
-                rbest_i = i;
-            }
-            if (rrun <= 0 || rbest - rrun >= xdrop) break;
-        }
+        const int nr = min(slen - s_right, qlen - q_right);
+        int rbest, rbest_i, rstop;
+        warp_xdrop<true>(m, subj, qry, s_right, q_right, nr, left_score, xdrop, lane, rbest, rbest_i, rstop);
         right_d = rbest_i + 1;
         right_score = rbest;
-        o.s_last = s_right + i;
+        o.s_last = s_right + rstop;
     }
     o.hsp_q = q_right - left_d;
     o.hsp_s = s_right - left_d;
@@ -95,182 +165,318 @@ __device__ ExtOut extend_two_hit(const int8_t* m, const uint8_t* __restrict__ su
 __device__ __forceinline__ int context_of(const int32_t* __restrict__ ctx, int n_ctx, int q) {
     int lo = 0, hi = n_ctx - 1;
     while (lo < hi) {
-        int mid = (lo + hi + 1) >> 1;
-        if (__ldg(ctx + 3 * mid) <= q) lo = mid; else hi = mid - 1;
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(ctx + 3 * mid) <= q) lo = mid;
+        else hi = mid - 1;
     }
     return lo;
 }
 
-template <int WARPS>
-__global__ void __launch_bounds__(WARPS * 32)
-scan_plain(ScanArgs a) {
-    extern __shared__ __align__(16) uint8_t sm[];
-    int8_t* m = reinterpret_cast<int8_t*>(sm);                 // 28 x 32, padded to 1 KB
-    uint32_t* pv = reinterpret_cast<uint32_t*>(sm + 1024);     // 1024 words
-    uint8_t* qs = sm + 1024 + 4096;
-    const int qpad = (a.qlen + 15) & ~15;
-    uint32_t* diag_all = reinterpret_cast<uint32_t*>(qs + qpad);
-    const int L = a.diag_mask + 1;
+__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// Residues r..r+kP+1 of the window starting at `sl` (code-1, or -1 past the end).
+__device__ __forceinline__ void load_window(const uint8_t* __restrict__ sub, int slen, int sl, int (&r)[kP + 2]) {
+#pragma unroll
+    for (int i = 0; i < kP + 2; ++i) r[i] = (sl + i < slen) ? (int)__ldg(sub + sl + i) - 1 : -1;
+}
+
+template <typename CellT>
+__device__ void scan_subject(const ScanArgs& a, const int8_t* m, const uint8_t* qs, const CellT* cells,
+                             const uint16_t* entries, uint32_t* diag, uint32_t* lane_pos, int oid,
+                             const uint8_t* __restrict__ sub, int slen, int& base, int lane) {
+    const unsigned lt = (1u << lane) - 1u;
+    if (base + slen + a.window > (1 << 30)) {
+        for (int i = lane; i <= a.diag_mask; i += 32) diag[i] = 0;
+        __syncwarp();
+        base = a.window;
+    }
+    int hits = 0, ext = 0, succ = 0, key_base = 0;
+    const int last_pos = slen - BP_WORD;
+    const uint32_t* my_row = lane_pos - lane * kP * 2;
+    int r[kP + 2];
+    load_window(sub, slen, lane * kP, r);
+    for (int s0 = 0; s0 <= last_pos; s0 += 32 * kP) {
+        int rn[kP + 2];
+        load_window(sub, slen, s0 + 32 * kP + lane * kP, rn);    // next window, in flight meanwhile
+        const int sl = s0 + lane * kP;
+        uint32_t lane_cnt = 0;
+#pragma unroll
+        for (int p = 0; p < kP; ++p) {
+            uint32_t start = 0, cnt = 0;
+            if (sl + p <= last_pos && (unsigned)r[p] < 27u && (unsigned)r[p + 1] < 27u && (unsigned)r[p + 2] < 27u) {
+                const int c = r[p] * 729 + r[p + 1] * 27 + r[p + 2];
+                start = cells[c];
+                cnt = (uint32_t)cells[c + 1] - start;
+            }
+            lane_pos[p] = lane_cnt;        // hits of this lane before position p
+            lane_pos[kP + p] = start;
+            lane_cnt += cnt;
+        }
+        hits += (int)lane_cnt;
+        const uint32_t incl = (uint32_t)warp_incl_sum((int)lane_cnt, lane);
+        const uint32_t total = __shfl_sync(kFull, incl, 31);
+        __syncwarp();
+        for (uint32_t hb = 0; hb < total; hb += 32) {
+            const uint32_t j = hb + lane;
+            const bool hv = j < total;
+            // owner lane: first lane whose inclusive prefix exceeds j
+            int lo = 0;
+#pragma unroll
+            for (int step = 16; step >= 1; step >>= 1) {
+                const uint32_t v = __shfl_sync(kFull, incl, lo + step - 1);
+                if (v <= j) lo += step;
+            }
+            const uint32_t o_incl = __shfl_sync(kFull, incl, lo);
+            const uint32_t o_cnt = __shfl_sync(kFull, lane_cnt, lo);
+            int hs = 0, hq = 0, d = 0;
+            if (hv) {
+                const uint32_t local = j - (o_incl - o_cnt);
+                const uint32_t* op = my_row + lo * kP * 2;
+                int p = 0;
+#pragma unroll
+                for (int t = 1; t < kP; ++t)
+                    if (op[t] <= local) p = t;
+                hs = s0 + lo * kP + p;
+                hq = entries[op[kP + p] + (local - op[p])];
+                d = (hq - hs) & a.diag_mask;
+            }
+            const unsigned vmask = __ballot_sync(kFull, hv);
+            unsigned peers = 0;
+            if (hv) peers = __match_any_sync(vmask, d);
+            bool pending = hv, found = false;
+            ExtOut res;
+            res.hsp_q = res.hsp_s = res.len = res.score = res.s_last = res.right_ext = 0;
+            for (;;) {
+                const unsigned pend = __ballot_sync(kFull, pending);
+                if (!pend) break;
+                bool need = false;
+                int prev = 0;
+                if (pending && (peers & pend & lt) == 0) {
+                    pending = false;
+                    const uint32_t v = diag[d];
+                    const int stamp = hs + base;
+                    if (v & kFlag) {
+                        // an extension already covered this hit; the first hit past it restarts the diagonal
+                        if (stamp >= (int)(v & ~kFlag)) diag[d] = (uint32_t)stamp;
+                    } else {
+                        prev = (int)v - base;
+                        const int diff = hs - prev;
+                        if (diff >= a.window) diag[d] = (uint32_t)stamp;
+                        else if (diff >= BP_WORD) need = true;
+                    }
+                }
+                // extensions of this round, one after the other, each by the whole warp
+                unsigned E = __ballot_sync(kFull, need);
+                while (E) {
+                    const int leader = __ffs(E) - 1;
+                    E &= E - 1;
+                    const int e_s = __shfl_sync(kFull, hs, leader);
+                    const int e_q = __shfl_sync(kFull, hq, leader);
+                    const int e_prev = __shfl_sync(kFull, prev, leader);
+                    const int k = a.n_ctx == 1 ? 0 : context_of(a.ctx, a.n_ctx, e_q);
+                    const ExtOut x = warp_extend_two_hit(m, sub, slen, qs, a.qlen, e_prev + BP_WORD, e_s, e_q,
+                                                         __ldg(a.ctx + 3 * k + 1), lane);
+                    if (lane == leader) {
+                        res = x;
+                        ++ext;
+                        found = x.score >= __ldg(a.ctx + 3 * k + 2);
+                        diag[d] = x.right_ext ? ((uint32_t)(x.s_last - (BP_WORD - 1) + base) | kFlag)
+                                              : (uint32_t)(hs + base);
+                    }
+                }
+                __syncwarp();
+            }
+            const unsigned fm = __ballot_sync(kFull, found);
+            if (fm) {
+                uint32_t pos0 = 0;
+                if (lane == 0) pos0 = atomicAdd(a.rec_count, (uint32_t)__popc(fm));
+                pos0 = __shfl_sync(kFull, pos0, 0);
+                if (found) {
+                    const uint32_t pos = pos0 + (uint32_t)__popc(fm & lt);
+                    if (pos < a.rec_cap) {
+                        HspRec rec;
+                        rec.oid = oid;
+                        rec.key = key_base + (int)j;
+                        rec.h.hsp_q = res.hsp_q;
+                        rec.h.hsp_s = res.hsp_s;
+                        rec.h.query_offset = hq;
+                        rec.h.subject_offset = hs;
+                        rec.h.hsp_len = res.len;
+                        rec.h.score = res.score;
+                        a.recs[pos] = rec;
+                    }
+                }
+                succ += __popc(fm);
+            }
+        }
+        key_base += (int)total;
+        __syncwarp();
+#pragma unroll
+        for (int i = 0; i < kP + 2; ++i) r[i] = rn[i];
+    }
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) {
+        hits += __shfl_xor_sync(kFull, hits, o);
+        ext += __shfl_xor_sync(kFull, ext, o);
+    }
+    if (lane == 0) {
+        a.counters[3 * (int64_t)oid + 0] = hits;
+        a.counters[3 * (int64_t)oid + 1] = succ;
+        a.counters[3 * (int64_t)oid + 2] = ext;
+    }
+    base += slen + a.window;
+}
+
+template <typename CellT, bool kCellsSmem>
+__global__ void __launch_bounds__(kMaxWarps * 32, 1)
+scan_kernel(ScanArgs a, ScanLayout lay) {
+    uint8_t* sm = bp_smem;
+    int8_t* m = reinterpret_cast<int8_t*>(sm);
+    uint8_t* qs = sm + lay.off_query;
+    const CellT* cells = kCellsSmem ? reinterpret_cast<const CellT*>(sm + lay.off_cells)
+                                    : reinterpret_cast<const CellT*>(a.cells);
+    const uint16_t* entries = lay.entries_smem ? reinterpret_cast<const uint16_t*>(sm + lay.off_entries) : a.entries;
 
     for (int i = threadIdx.x; i < 28 * BP_MROW; i += blockDim.x) m[i] = a.matrix[i];
-    for (int i = threadIdx.x; i < BP_NCELL / 32; i += blockDim.x) pv[i] = a.pv[i];
+    if (kCellsSmem) {
+        CellT* c = reinterpret_cast<CellT*>(sm + lay.off_cells);
+        for (int i = threadIdx.x; i <= BP_NC; i += blockDim.x) c[i] = (CellT)a.cells[i];
+    }
+    if (lay.entries_smem) {
+        uint16_t* e = reinterpret_cast<uint16_t*>(sm + lay.off_entries);
+        for (int i = threadIdx.x; i < a.n_entries; i += blockDim.x) e[i] = a.entries[i];
+    }
     for (int i = threadIdx.x; i < a.qlen; i += blockDim.x) qs[i] = a.query[i];
-    for (int i = threadIdx.x; i < WARPS * L; i += blockDim.x) diag_all[i] = 0;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint8_t* wr = sm + lay.off_warps + (size_t)warp * lay.warp_bytes;
+    uint32_t* diag = reinterpret_cast<uint32_t*>(wr);
+    uint32_t* lane_pos = reinterpret_cast<uint32_t*>(wr + (size_t)lay.L * 4) + lane * kP * 2;
+    for (int i = lane; i < lay.L; i += 32) diag[i] = 0;
     __syncthreads();
 
-    const int lane = threadIdx.x & 31;
-    const unsigned lt = (1u << lane) - 1u;
-    uint32_t* diag = diag_all + (threadIdx.x >> 5) * L;
+    // Subject pipeline, kept by lane 0.  At the top of iteration i:
+    //   cur (+ cs, ce)   subject i, offsets known: scan it now
+    //   oid1 (+ s1, e1)  subject i+1, offsets known: prefetch its residues now
+    //   oid2             subject i+2, id known: load its offsets now
+    // and the id of subject i+3 is taken from the cursor.
+    int cur = 0, oid1 = 0, oid2 = 0;
+    long long cs = 0, ce = 0, s1 = 0, e1 = 0;
+    if (lane == 0) {
+        cur = (int)atomicAdd(a.cursor, 1u);
+        oid1 = (int)atomicAdd(a.cursor, 1u);
+        oid2 = (int)atomicAdd(a.cursor, 1u);
+        if (cur < a.n) {
+            cs = a.db_off[a.first + cur];
+            ce = a.db_off[a.first + cur + 1];
+        }
+        if (oid1 < a.n) {
+            s1 = a.db_off[a.first + oid1];
+            e1 = a.db_off[a.first + oid1 + 1];
+        }
+    }
+    cur = __shfl_sync(kFull, cur, 0);
+    cs = __shfl_sync(kFull, cs, 0);
+    ce = __shfl_sync(kFull, ce, 0);
     int base = a.window;   // diagonal stamp offset (gpu_blastp_kernel.cu:308)
-
-    for (;;) {
-        int oid = 0;
-        if (lane == 0) oid = (int)atomicAdd(a.cursor, 1u);
-        oid = __shfl_sync(kFull, oid, 0);
-        if (oid >= a.n) break;
-        const int64_t so = a.db_off[a.first + oid];
-        const int slen = (int)(a.db_off[a.first + oid + 1] - so);
-        const uint8_t* __restrict__ sub = a.db + so;
-        if (base + slen + a.window > (1 << 30)) {
-            for (int i = lane; i < L; i += 32) diag[i] = 0;
-            __syncwarp();
-            base = a.window;
-        }
-        int hits = 0, ext = 0, succ = 0, key_base = 0;
-        for (int s0 = 0; s0 <= slen - BP_WORD; s0 += 32) {
-            const int s = s0 + lane;
-            uint32_t start = 0, cnt = 0;
-            if (s <= slen - BP_WORD) {
-                uint32_t c = ((uint32_t)__ldg(sub + s) << 10) | ((uint32_t)__ldg(sub + s + 1) << 5) |
-                             (uint32_t)__ldg(sub + s + 2);
-                if (pv[c >> 5] & (1u << (c & 31))) {
-                    start = __ldg(a.cell_start + c);
-                    cnt = __ldg(a.cell_start + c + 1) - start;
-                }
-            }
-            hits += (int)cnt;
-            uint32_t incl = cnt;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                uint32_t v = __shfl_up_sync(kFull, incl, o);
-                if (lane >= o) incl += v;
-            }
-            const uint32_t total = __shfl_sync(kFull, incl, 31);
-            for (uint32_t hb = 0; hb < total; hb += 32) {
-                const uint32_t j = hb + lane;
-                const bool hv = j < total;
-                int lo = 0;
-#pragma unroll
-                for (int step = 16; step >= 1; step >>= 1) {
-                    uint32_t v = __shfl_sync(kFull, incl, lo + step - 1);
-                    if (v <= j) lo += step;
-                }
-                const uint32_t o_incl = __shfl_sync(kFull, incl, lo);
-                const uint32_t o_cnt = __shfl_sync(kFull, cnt, lo);
-                const uint32_t o_start = __shfl_sync(kFull, start, lo);
-                const int hs = s0 + lo;
-                int hq = 0, d = 0;
-                if (hv) {
-                    hq = __ldg(a.entries + o_start + (j - (o_incl - o_cnt)));
-                    d = (hq - hs) & a.diag_mask;
-                }
-                const unsigned vmask = __ballot_sync(kFull, hv);
-                unsigned peers = 0;
-                if (hv) peers = __match_any_sync(vmask, d);
-                bool pending = hv, found = false;
-                ExtOut r;
-                for (;;) {
-                    const unsigned pend = __ballot_sync(kFull, pending);
-                    if (!pend) break;
-                    if (pending && (peers & pend & lt) == 0) {
-                        pending = false;
-                        const uint32_t v = diag[d];
-                        const int stamp = hs + base;
-                        if (v & kFlag) {
-                            if (stamp >= (int)(v & ~kFlag)) diag[d] = (uint32_t)stamp;
-                        } else {
-                            const int prev = (int)v - base;
-                            const int diff = hs - prev;
-                            if (diff >= a.window) {
-                                diag[d] = (uint32_t)stamp;
-                            } else if (diff >= BP_WORD) {
-                                const int k = a.n_ctx == 1 ? 0 : context_of(a.ctx, a.n_ctx, hq);
-                                r = extend_two_hit(m, sub, slen, qs, a.qlen, prev + BP_WORD, hs, hq,
-                                                   __ldg(a.ctx + 3 * k + 1));
-                                ++ext;
-                                found = r.score >= __ldg(a.ctx + 3 * k + 2);
-                                diag[d] = r.right_ext
-                                              ? ((uint32_t)(r.s_last - (BP_WORD - 1) + base) | kFlag)
-                                              : (uint32_t)stamp;
-                            }
-                        }
-                    }
-                    __syncwarp();
-                }
-                const unsigned fm = __ballot_sync(kFull, found);
-                if (fm) {
-                    uint32_t pos0 = 0;
-                    if (lane == 0) pos0 = atomicAdd(a.rec_count, (uint32_t)__popc(fm));
-                    pos0 = __shfl_sync(kFull, pos0, 0);
-                    if (found) {
-                        const uint32_t pos = pos0 + (uint32_t)__popc(fm & lt);
-                        if (pos < a.rec_cap) {
-                            HspRec rec;
-                            rec.oid = oid;
-                            rec.key = key_base + (int)j;
-                            rec.h.hsp_q = r.hsp_q;
-                            rec.h.hsp_s = r.hsp_s;
-                            rec.h.query_offset = hq;
-                            rec.h.subject_offset = hs;
-                            rec.h.hsp_len = r.len;
-                            rec.h.score = r.score;
-                            a.recs[pos] = rec;
-                        }
-                    }
-                    succ += __popc(fm);
-                }
-            }
-            key_base += (int)total;
-        }
-#pragma unroll
-        for (int o = 16; o >= 1; o >>= 1) {
-            hits += __shfl_xor_sync(kFull, hits, o);
-            ext += __shfl_xor_sync(kFull, ext, o);
-        }
+    while (cur < a.n) {
+        long long s2 = 0, e2 = 0;
+        int oid3 = 0;
         if (lane == 0) {
-            a.counters[3 * (int64_t)oid + 0] = hits;
-            a.counters[3 * (int64_t)oid + 1] = succ;
-            a.counters[3 * (int64_t)oid + 2] = ext;
+            if (oid1 < a.n && e1 > s1) prefetch_l2(a.db + (s1 & ~15LL), (uint32_t)(((e1 + 15) & ~15LL) - (s1 & ~15LL)));
+            if (oid2 < a.n) {
+                s2 = a.db_off[a.first + oid2];
+                e2 = a.db_off[a.first + oid2 + 1];
+            }
+            oid3 = (int)atomicAdd(a.cursor, 1u);
         }
-        base += slen + a.window;
+        scan_subject<CellT>(a, m, qs, cells, entries, diag, lane_pos, cur, a.db + cs, (int)(ce - cs), base, lane);
+        int nxt = 0;
+        long long ns = 0, ne = 0;
+        if (lane == 0) {
+            nxt = oid1;
+            ns = s1;
+            ne = e1;
+            oid1 = oid2;
+            s1 = s2;
+            e1 = e2;
+            oid2 = oid3;
+        }
+        cur = __shfl_sync(kFull, nxt, 0);
+        cs = __shfl_sync(kFull, ns, 0);
+        ce = __shfl_sync(kFull, ne, 0);
     }
 }
 
-template <int WARPS>
-cudaError_t launch_scan_t(bp_engine* e, const ScanArgs& a) {
-    const int L = a.diag_mask + 1;
-    size_t smem = 1024 + 4096 + (size_t)((a.qlen + 15) & ~15) + (size_t)WARPS * L * 4;
-    cudaError_t err = cudaFuncSetAttribute(scan_plain<WARPS>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+ScanLayout make_layout(int qlen, int L, int64_t n_entries, int warps, int cells_mode, int entries_smem) {
+    ScanLayout l{};
+    l.warps = warps;
+    l.cells_mode = cells_mode;
+    l.entries_smem = entries_smem;
+    l.L = L;
+    auto al = [](long long x, long long a) { return (x + a - 1) / a * a; };
+    long long off = 1024;                             // matrix 28 x 32
+    l.off_cells = (int)off;
+    if (cells_mode == 0) off = al(off + (BP_NC + 1) * 2LL, 16);
+    else if (cells_mode == 1) off = al(off + (BP_NC + 1) * 4LL, 16);
+    l.off_entries = (int)off;
+    if (entries_smem) off = al(off + n_entries * 2, 16);
+    const long long big = 1LL << 30;                  // anything this large cannot fit
+    if (off > big) off = big;
+    l.off_query = (int)off;
+    off = al(off + qlen, 16);
+    l.off_warps = (int)off;
+    const long long wb = al((long long)L * 4 + 32 * kP * 2 * 4, 16);
+    l.warp_bytes = (int)(wb > big ? big : wb);
+    off += (long long)warps * wb;
+    l.total = (int)(off > big ? big : off);
+    return l;
+}
+
+// Picks the layout with the most warps, preferring the whole table in shared
+// memory as long as that still leaves at least 16 warps.
+bool choose_layout(int qlen, int L, int64_t n_entries, int smem_optin, ScanLayout* out) {
+    const int cell_modes[2] = {n_entries < 65536 ? 0 : 1, 2};
+    for (int min_w : {16, 8, 1})
+        for (int cm : cell_modes)
+            for (int es = 1; es >= 0; --es) {
+                if (es && cm == 2) continue;
+                for (int w = kMaxWarps; w >= min_w; --w) {
+                    const ScanLayout l = make_layout(qlen, L, n_entries, w, cm, es);
+                    if (l.total <= smem_optin) {
+                        *out = l;
+                        return true;
+                    }
+                }
+            }
+    return false;
+}
+
+template <typename CellT, bool kCellsSmem>
+cudaError_t launch(bp_engine* e, const ScanArgs& a, const ScanLayout& lay) {
+    auto kern = scan_kernel<CellT, kCellsSmem>;
+    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, lay.total);
     if (err != cudaSuccess) return err;
-    int per_sm = 0;
-    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, scan_plain<WARPS>, WARPS * 32, smem);
-    if (err != cudaSuccess) return err;
-    if (per_sm < 1) return cudaErrorInvalidConfiguration;
-    int grid = e->sm_count * per_sm;
-    int need = (a.n + WARPS - 1) / WARPS;
+    int grid = e->sm_count;
+    const int need = (a.n + lay.warps - 1) / lay.warps;   // no more CTAs than subjects to feed them
     if (grid > need) grid = need > 0 ? need : 1;
-    scan_plain<WARPS><<<grid, WARPS * 32, smem, e->stream>>>(a);
+    kern<<<grid, lay.warps * 32, lay.total, e->stream>>>(a, lay);
     e->launches += 1;
     return cudaGetLastError();
 }
 
 }  // namespace
 
+bool bp_scan_fits(int32_t qlen, int32_t diag_mask, int64_t n_entries, int smem_optin) {
+    ScanLayout l;
+    return choose_layout(qlen, diag_mask + 1, n_entries, smem_optin, &l);
+}
+
 cudaError_t bp_launch_scan(bp_engine* e, const ScanArgs& a) {
-    const int L = a.diag_mask + 1;
-    // Keep the per-CTA diagonal arrays within ~96 KB so two CTAs fit an SM.
-    if (L <= 2048) return launch_scan_t<8>(e, a);
-    if (L <= 8192) return launch_scan_t<2>(e, a);
-    return launch_scan_t<1>(e, a);
+    ScanLayout lay;
+    if (!choose_layout(a.qlen, a.diag_mask + 1, a.n_entries, e->smem_optin, &lay)) return cudaErrorInvalidValue;
+    if (lay.cells_mode == 0) return launch<uint16_t, true>(e, a, lay);
+    if (lay.cells_mode == 1) return launch<uint32_t, true>(e, a, lay);
+    return launch<uint32_t, false>(e, a, lay);
 }
