@@ -88,7 +88,7 @@ class Engine:
     def search(self, db: "Database", q: "Query", first: int = 0, count: int = -1) -> "PendingResult":
         h = ctypes.c_void_p()
         check(lib().bp_search(self.h, db.h, q.h, first, count, ctypes.byref(h)), self.h)
-        return PendingResult(self, h)
+        return PendingResult(self, h, keep=(db, q))
 
     def blastp_host(self, query, params, residues, offsets, hsp_cap=None):
         """End-to-end: host buffers in, host buffers out (one C call)."""
@@ -165,9 +165,10 @@ class Query:
 
 
 class PendingResult:
-    def __init__(self, engine: Engine, h):
+    def __init__(self, engine: Engine, h, keep=()):
         self.engine = engine
         self.h = h
+        self._keep = keep      # the database and query must outlive the search
 
     def wait(self):
         check(lib().bp_result_wait(self.h), self.engine.h)
