@@ -58,6 +58,7 @@ SIGNATURES = {
     "bp_result_copy": (ctypes.c_int, [P, P, P, P]),
     "bp_result_destroy": (None, [P]),
     "bp_blastp_host": (ctypes.c_int, [P, P, i32, P, P, i64, P, i32, P, P, P, i64, P]),
+    "bp_search_noalloc": (ctypes.c_int, [P, i32, P, P, i64, P, i32, P, P, P, i64, P, P]),
     # reference-compatible entry points
     "GPU_BLASTP": (None, [P] * 7 + [ctypes.c_int, P, P, i32, P, i32] + [P] * 7),
     "GPU_BLASTP_get_data": (None, [P, P, i32, P, P, i32, i32]),

@@ -129,6 +129,30 @@ bp_status bp_blastp_host(bp_engine* e, const uint8_t* query, int32_t qlen, const
                          int32_t n_subjects, int32_t* counters, int64_t* hsp_off,
                          bp_hsp* hsps, int64_t hsp_cap, int64_t* n_hsps);
 
+/* The plain search for callers that cannot allocate device memory: a process
+ * that hands out a fixed device-memory budget at start-up, a latency-critical
+ * path where cudaMalloc/cudaFree would synchronise the device, or code whose
+ * buffers come from an outside allocator.  No counterpart in the reference.
+ *
+ * The caller passes device buffers for everything: the query (d_query,
+ * residues 1..27), the database (d_residues, d_offsets with n_subjects+1
+ * entries running from 0 to n_residues), and the outputs d_counters
+ * (3*n_subjects int32), d_hsp_off (n_subjects+1 int64) and d_hsps (hsp_cap
+ * records).  Scratch -- neighbour table, unordered HSP records, ordering
+ * cursors -- is one static 16 MiB device array in the library; the call makes
+ * no cudaMalloc or cudaFree.  Limits: n_subjects <= 1,048,576, qlen <= 4096,
+ * neighbour-table entries <= 1,048,576, HSPs per call <= min(hsp_cap, 262,144);
+ * beyond them it returns BP_ERR_TOO_LARGE (for too many HSPs *n_hsps holds the
+ * true count and the counters and offsets are complete).  The call runs on
+ * `stream` (NULL: the legacy default stream) and returns when the results are
+ * in place.  The first call on a device sets the array up (looks up its
+ * device address and copies the scoring matrix, synchronously), so make it
+ * before any stream capture.  Every call reuses the same array: calls that
+ * overlap on the GPU race and must be serialised by the caller. */
+bp_status bp_search_noalloc(const uint8_t* d_query, int32_t qlen, const bp_params* p, const uint8_t* d_residues,
+                            int64_t n_residues, const int64_t* d_offsets, int32_t n_subjects, int32_t* d_counters,
+                            int64_t* d_hsp_off, bp_hsp* d_hsps, int64_t hsp_cap, int64_t* n_hsps, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
