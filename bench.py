@@ -128,8 +128,8 @@ def measured_peak_hbm():
 
 def profiled_traffic_per_residue():
     """dram bytes per database residue of the scan kernel, from the committed
-    ncu summary (profiles/scan_plain_q500_vs_1M.md), or None."""
-    path = os.path.join(ROOT, "profiles", "scan_plain_q500_vs_1M.md")
+    ncu summary (profiles/scan_kernel_q500_vs_1M.md), or None."""
+    path = os.path.join(ROOT, "profiles", "scan_kernel_q500_vs_1M.md")
     try:
         for line in open(path):
             if line.startswith("traffic_bytes_per_residue:"):
@@ -311,7 +311,7 @@ def run_ours(args):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
                      "traffic": (tpr * w.db.n_residues) if tpr else None,
-                     "kernel": "scan_plain", "kernel_ms": scan_avg_ms,
+                     "kernel": "scan_kernel", "kernel_ms": scan_avg_ms,
                      "algorithmic_bytes": alg_bytes},
         "hsps": int(len(ref_hsps.hsps)),
     }
