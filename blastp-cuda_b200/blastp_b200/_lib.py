@@ -25,6 +25,14 @@ class BpParams(ctypes.Structure):
                 ("x_dropoff", i32), ("cutoff_score", i32)]
 
 
+class BpBatchOptions(ctypes.Structure):
+    _fields_ = [("chunk_residues", i32), ("schedule", i32), ("ctas", i32), ("max_warps", i32),
+                ("use_graph", i32), ("item_costs", P)]
+
+
+SCHED_DYNAMIC, SCHED_STATIC, SCHED_COSTS = 0, 1, 2
+
+
 class BpError(RuntimeError):
     def __init__(self, status, msg=""):
         self.status = status
@@ -59,6 +67,17 @@ SIGNATURES = {
     "bp_result_destroy": (None, [P]),
     "bp_blastp_host": (ctypes.c_int, [P, P, i32, P, P, i64, P, i32, P, P, P, i64, P]),
     "bp_search_noalloc": (ctypes.c_int, [P, i32, P, P, i64, P, i32, P, P, P, i64, P, P]),
+    "bp_batch_options_default": (None, [P]),
+    "bp_batch_plan": (ctypes.c_int, [P, i32, P, P]),
+    "bp_search_batch": (ctypes.c_int, [P, P, P, i32, P, P]),
+    "bp_batch_run": (ctypes.c_int, [P]),
+    "bp_batch_wait": (ctypes.c_int, [P]),
+    "bp_batch_hsps": (i64, [P]),
+    "bp_batch_items": (i32, [P]),
+    "bp_batch_last_scan_ms": (ctypes.c_float, [P]),
+    "bp_batch_copy_query": (ctypes.c_int, [P, i32, P, P, P, P]),
+    "bp_batch_queue_costs": (ctypes.c_int, [P, P, P]),
+    "bp_batch_destroy": (None, [P]),
     # reference-compatible entry points
     "GPU_BLASTP": (None, [P] * 7 + [ctypes.c_int, P, P, i32, P, i32] + [P] * 7),
     "GPU_BLASTP_get_data": (None, [P, P, i32, P, P, i32, i32]),

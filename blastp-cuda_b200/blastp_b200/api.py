@@ -9,7 +9,7 @@ import ctypes
 import numpy as np
 
 from . import _lib
-from ._lib import BpParams, check, lib
+from ._lib import BpBatchOptions, BpParams, check, lib
 
 HSP_DTYPE = np.dtype([("hsp_q", "<i4"), ("hsp_s", "<i4"), ("query_offset", "<i4"),
                       ("subject_offset", "<i4"), ("hsp_len", "<i4"), ("score", "<i4")])
@@ -89,6 +89,35 @@ class Engine:
         h = ctypes.c_void_p()
         check(lib().bp_search(self.h, db.h, q.h, first, count, ctypes.byref(h)), self.h)
         return PendingResult(self, h, keep=(db, q))
+
+    def plan_chunks(self, db: "Database", chunk_residues: int) -> np.ndarray:
+        """Chunk boundaries of a batched search: chunk c holds subjects
+        [first[c], first[c+1])."""
+        n = ctypes.c_int32(0)
+        check(lib().bp_batch_plan(db.h, chunk_residues, None, ctypes.byref(n)), self.h)
+        first = np.zeros(n.value + 1, dtype=np.int32)
+        check(lib().bp_batch_plan(db.h, chunk_residues, _p(first), ctypes.byref(n)), self.h)
+        return first
+
+    def search_batch(self, db: "Database", queries, chunk_residues: int = 1 << 18, schedule: int = 0,
+                     ctas: int = 0, max_warps: int = 0, use_graph: bool = True, item_costs=None) -> "Batch":
+        """Many queries against db in one persistent launch; each query's
+        result equals its single-query search."""
+        o = BpBatchOptions()
+        lib().bp_batch_options_default(ctypes.byref(o))
+        o.chunk_residues = chunk_residues
+        o.schedule = schedule
+        o.ctas = ctas
+        o.max_warps = max_warps
+        o.use_graph = int(bool(use_graph))
+        costs = None
+        if item_costs is not None:
+            costs = np.ascontiguousarray(item_costs, dtype=np.float32)
+            o.item_costs = costs.ctypes.data
+        arr = (ctypes.c_void_p * max(1, len(queries)))(*[q.h.value for q in queries])
+        h = ctypes.c_void_p()
+        check(lib().bp_search_batch(self.h, db.h, arr, len(queries), ctypes.byref(o), ctypes.byref(h)), self.h)
+        return Batch(self, h, db, list(queries))
 
     def blastp_host(self, query, params, residues, offsets, hsp_cap=None):
         """End-to-end: host buffers in, host buffers out (one C call)."""
@@ -187,6 +216,67 @@ class PendingResult:
     def close(self):
         if self.h:
             lib().bp_result_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """A batched search that can be re-run (a CUDA graph replay by default)."""
+
+    def __init__(self, engine: Engine, h, db, queries):
+        self.engine = engine
+        self.h = h
+        self._keep = (db, queries)     # must outlive the batch
+        self.n_subjects = db.n_subjects
+        self.n_queries = len(queries)
+
+    def run(self):
+        check(lib().bp_batch_run(self.h), self.engine.h)
+        return self
+
+    def wait(self):
+        check(lib().bp_batch_wait(self.h), self.engine.h)
+        return self
+
+    @property
+    def n_hsps(self) -> int:
+        return int(lib().bp_batch_hsps(self.h))
+
+    @property
+    def n_items(self) -> int:
+        return int(lib().bp_batch_items(self.h))
+
+    @property
+    def last_scan_ms(self) -> float:
+        return float(lib().bp_batch_last_scan_ms(self.h))
+
+    def queue_costs(self) -> np.ndarray:
+        n = ctypes.c_int32(0)
+        check(lib().bp_batch_queue_costs(self.h, None, ctypes.byref(n)), self.engine.h)
+        out = np.zeros(n.value, dtype=np.float64)
+        check(lib().bp_batch_queue_costs(self.h, _p(out), ctypes.byref(n)), self.engine.h)
+        return out
+
+    def fetch(self, qi: int) -> Result:
+        self.wait()
+        n = self.n_subjects
+        nh = ctypes.c_int64(0)
+        check(lib().bp_batch_copy_query(self.h, qi, None, None, None, ctypes.byref(nh)), self.engine.h)
+        counters = np.zeros((n, 3), dtype=np.int32)
+        hoff = np.zeros(n + 1, dtype=np.int64)
+        hsps = np.zeros(max(nh.value, 1), dtype=HSP_DTYPE)
+        check(lib().bp_batch_copy_query(self.h, qi, _p(counters), _p(hoff), _p(hsps), ctypes.byref(nh)),
+              self.engine.h)
+        return Result(counters, hoff, hsps[:nh.value])
+
+    def close(self):
+        if self.h:
+            lib().bp_batch_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -1,0 +1,498 @@
+// Batched search: many queries against one HBM-resident database in one
+// persistent launch (scan_batch_kernel), optionally captured in a CUDA graph
+// and replayed.
+//
+// The reference searches one query per kernel launch (gpu_blastp.cu:197-210,
+// the query in constant memory, contexts capped at 4096).  Here a batch of
+// queries, each with its own device table, is cut into work items
+// (query, subject chunk); the items are handed to the CTAs either through a
+// global cursor, or through per-CTA queues filled statically (round robin) or
+// from predicted costs (longest-processing-time-first into the least loaded
+// queue).  Queries are grouped into classes by diagonal-array size, so a
+// short query does not run with the shared-memory layout (and the lower warp
+// count) of the longest one; each class is one persistent launch, the
+// classes on parallel streams (parallel graph branches) so one class's tail
+// overlaps the next class's start.  Every (query, subject) pair is scanned
+// exactly as in the single-query kernel, so each query's result equals its
+// single-query result.
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <numeric>
+#include <queue>
+#include <vector>
+
+#include "bp_internal.h"
+
+#define CKB(call, what)                                                   \
+    do {                                                                  \
+        cudaError_t _err = (call);                                        \
+        if (_err != cudaSuccess) return bp_set_cuda_error(e, _err, what); \
+    } while (0)
+
+struct bp_batch {
+    bp_engine* e = nullptr;
+    const bp_db* db = nullptr;
+    int32_t nq = 0, n = 0;
+    int64_t nseg = 0;
+    std::vector<const bp_query*> queries;
+    bp_batch_options opt{};
+    std::vector<int32_t> chunk_first;        // n_chunks + 1 subject boundaries
+    // device
+    BatchQuery* d_queries = nullptr;
+    WorkItem* d_items = nullptr;
+    int32_t* d_queue_off = nullptr;
+    int32_t* d_queue_items = nullptr;
+    int32_t* d_counters = nullptr;
+    int64_t* d_hsp_off = nullptr;
+    bp_hsp* d_hsps = nullptr;
+    int32_t* d_keys = nullptr;
+    uint32_t cap = 0;                        // capacity of d_hsps / d_keys / d_recs
+    uint32_t alloc_cap = 0;
+    HspRec* d_recs = nullptr;                // batch-owned scratch, so a captured graph
+    int32_t* d_fill = nullptr;               // never points at engine buffers that a
+    int64_t* d_blocksums = nullptr;          // later search may regrow
+    uint32_t* d_counts = nullptr;            // [0] records, [1] item cursor
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    uint64_t launches_per_run = 0;
+    float last_ms = 0.f;
+    uint32_t* h_count = nullptr;
+    int64_t n_hsps = -1;
+    int32_t n_items = 0;
+    struct Class {
+        int32_t max_qlen = 0, max_mask = 0;
+        int64_t max_entries = 0;
+        int32_t item_lo = 0, item_hi = 0;      // its items in d_items
+        int32_t queue_lo = 0;                  // its queue offsets start at d_queue_off[queue_lo]
+        int32_t grid = 0;
+        double est = 0;                        // expected word hits, to order the launches
+    };
+    std::vector<Class> classes;
+    std::vector<cudaStream_t> side;          // one per class after the first
+    std::vector<cudaEvent_t> ev_join;
+    cudaEvent_t ev_fork = nullptr;
+    bool capturing = false;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<double> queue_cost;         // predicted cost per CTA queue (cost schedules)
+};
+
+namespace {
+
+void plan_chunks(const bp_db* db, int32_t chunk_residues, std::vector<int32_t>& first) {
+    first.clear();
+    first.push_back(0);
+    const int64_t* off = db->h_off.data();
+    int32_t s = 0;
+    while (s < db->n) {
+        const int64_t limit = off[s] + std::max<int64_t>(chunk_residues, 1);
+        // at least one subject per chunk, then as many as fit under the limit
+        int32_t t = (int32_t)(std::upper_bound(off + s + 1, off + db->n + 1, limit) - off) - 1;
+        if (t <= s) t = s + 1;
+        if (t > db->n) t = db->n;
+        first.push_back(t);
+        s = t;
+    }
+}
+
+// Enqueues the batch's device work on the engine stream: one persistent
+// launch per class (forked onto side streams), then the ordering pass.
+bp_status enqueue(bp_batch* b) {
+    bp_engine* e = b->e;
+    const uint64_t l0 = e->launches;
+    CKB(cudaMemsetAsync(b->d_counts, 0, (4 + b->classes.size()) * sizeof(uint32_t), e->stream), "memset(counts)");
+    // inside a capture a timing event must be an external record node
+    const unsigned rec_flags = b->capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
+    CKB(cudaEventRecordWithFlags(b->ev0, e->stream, rec_flags), "cudaEventRecord");
+    CKB(cudaEventRecord(b->ev_fork, e->stream), "cudaEventRecord");
+    for (size_t c = 0; c < b->classes.size(); ++c) {
+        const bp_batch::Class& k = b->classes[c];
+        cudaStream_t st = c == 0 ? e->stream : b->side[c - 1];
+        if (c > 0) CKB(cudaStreamWaitEvent(st, b->ev_fork, 0), "cudaStreamWaitEvent");
+        BatchArgs a;
+        a.db = b->db->d_res;
+        a.db_off = b->db->d_off;
+        a.n_subjects = b->n;
+        a.queries = b->d_queries;
+        a.n_queries = b->nq;
+        a.items = b->d_items + k.item_lo;
+        a.n_items = k.item_hi - k.item_lo;
+        a.queue_off = b->opt.schedule == BP_SCHED_DYNAMIC ? nullptr : b->d_queue_off + k.queue_lo;
+        a.queue_items = b->d_queue_items;
+        a.item_cursor = b->d_counts + 4 + c;
+        a.matrix = e->d_matrix;
+        a.window = b->queries[0]->p.window;
+        a.counters = b->d_counters;
+        a.recs = b->d_recs;
+        a.rec_cap = b->cap;
+        a.rec_count = b->d_counts;
+        if (a.n_items > 0)
+            CKB(bp_launch_scan_batch(e, st, a, k.max_qlen, k.max_mask, k.max_entries, k.grid, b->opt.max_warps),
+                "batched scan launch");
+        if (c > 0) {
+            CKB(cudaEventRecord(b->ev_join[c - 1], st), "cudaEventRecord");
+            CKB(cudaStreamWaitEvent(e->stream, b->ev_join[c - 1], 0), "cudaStreamWaitEvent");
+        }
+    }
+    CKB(cudaEventRecordWithFlags(b->ev1, e->stream, rec_flags), "cudaEventRecord");
+    CKB(bp_launch_order(e, (int32_t)b->nseg, b->d_counters, b->d_hsp_off, b->d_recs, b->cap, b->d_counts,
+                        b->d_fill, b->d_hsps, b->d_keys, b->d_blocksums),
+        "order kernels launch");
+    CKB(cudaMemcpyAsync(b->h_count, b->d_counts, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, e->stream),
+        "copy counts");
+    b->launches_per_run = e->launches - l0;
+    return BP_OK;
+}
+
+// Sizes the batch's scratch and outputs for the current record capacity.
+bp_status prepare(bp_batch* b) {
+    bp_engine* e = b->e;
+    if (!b->d_counts) {
+        CKB(cudaMalloc((void**)&b->d_counts, (4 + b->classes.size()) * sizeof(uint32_t)), "cudaMalloc(counts)");
+        CKB(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming), "cudaEventCreate");
+        for (size_t c = 1; c < b->classes.size(); ++c) {
+            cudaStream_t st = nullptr;
+            cudaEvent_t ev = nullptr;
+            CKB(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate");
+            b->side.push_back(st);
+            CKB(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreate");
+            b->ev_join.push_back(ev);
+        }
+        CKB(cudaMalloc((void**)&b->d_fill, (size_t)std::max<int64_t>(b->nseg, 1) * sizeof(int32_t)), "cudaMalloc(fill)");
+        CKB(cudaMalloc((void**)&b->d_blocksums,
+                       (size_t)std::max(bp_order_blocksums_needed((int32_t)b->nseg), 1) * sizeof(int64_t)),
+            "cudaMalloc(sums)");
+        CKB(cudaEventCreate(&b->ev0), "cudaEventCreate");
+        CKB(cudaEventCreate(&b->ev1), "cudaEventCreate");
+    }
+    if (b->alloc_cap < b->cap || !b->d_hsps) {
+        cudaFree(b->d_recs);
+        cudaFree(b->d_hsps);
+        cudaFree(b->d_keys);
+        b->d_recs = nullptr;
+        b->d_hsps = nullptr;
+        b->d_keys = nullptr;
+        b->alloc_cap = 0;
+        const size_t n = std::max<uint32_t>(b->cap, 1);
+        CKB(cudaMalloc((void**)&b->d_recs, n * sizeof(HspRec)), "cudaMalloc(records)");
+        CKB(cudaMalloc((void**)&b->d_hsps, n * sizeof(bp_hsp)), "cudaMalloc(hsps)");
+        CKB(cudaMalloc((void**)&b->d_keys, n * sizeof(int32_t)), "cudaMalloc(keys)");
+        b->alloc_cap = b->cap;
+    }
+    return BP_OK;
+}
+
+bp_status capture(bp_batch* b) {
+    bp_engine* e = b->e;
+    if (b->exec) {
+        cudaGraphExecDestroy(b->exec);
+        b->exec = nullptr;
+    }
+    if (b->graph) {
+        cudaGraphDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    CKB(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeRelaxed), "begin capture");
+    const uint64_t l0 = e->launches;
+    b->capturing = true;
+    bp_status st = enqueue(b);
+    b->capturing = false;
+    e->launches = l0;   // captured, not run
+    cudaGraph_t g = nullptr;
+    cudaError_t err = cudaStreamEndCapture(e->stream, &g);
+    if (st != BP_OK) {
+        if (g) cudaGraphDestroy(g);
+        return st;
+    }
+    CKB(err, "end capture");
+    b->graph = g;
+    CKB(cudaGraphInstantiate(&b->exec, g, 0), "instantiate graph");
+    return BP_OK;
+}
+
+bp_status launch_batch(bp_batch* b) {
+    bp_engine* e = b->e;
+    b->n_hsps = -1;
+    if (b->opt.use_graph) {
+        if (!b->exec) {
+            bp_status st = capture(b);
+            if (st != BP_OK) return st;
+        }
+        CKB(cudaGraphLaunch(b->exec, e->stream), "graph launch");
+        e->launches += b->launches_per_run;   // the kernels captured in the graph
+        return BP_OK;
+    }
+    return enqueue(b);
+}
+
+}  // namespace
+
+extern "C" {
+
+void bp_batch_options_default(bp_batch_options* o) {
+    memset(o, 0, sizeof(*o));
+    o->chunk_residues = 1 << 18;
+    o->schedule = BP_SCHED_DYNAMIC;
+    o->use_graph = 1;
+}
+
+bp_status bp_batch_plan(const bp_db* db, int32_t chunk_residues, int32_t* chunk_first, int32_t* n_chunks) {
+    if (!db || !n_chunks) return BP_ERR_INVALID;
+    std::vector<int32_t> first;
+    plan_chunks(db, chunk_residues, first);
+    *n_chunks = (int32_t)first.size() - 1;
+    if (chunk_first) memcpy(chunk_first, first.data(), first.size() * sizeof(int32_t));
+    return BP_OK;
+}
+
+bp_status bp_search_batch(bp_engine* e, const bp_db* db, const bp_query* const* queries, int32_t n_queries,
+                          const bp_batch_options* opt, bp_batch** out) {
+    if (!e || !db || !queries || n_queries < 0 || !out) return bp_set_error(e, BP_ERR_INVALID, "bp_search_batch: bad argument");
+    *out = nullptr;
+    bp_batch_options o;
+    if (opt) o = *opt;
+    else bp_batch_options_default(&o);
+    if (o.schedule == BP_SCHED_COSTS && !o.item_costs)
+        return bp_set_error(e, BP_ERR_INVALID, "bp_search_batch: cost schedule without item costs");
+    if ((int64_t)n_queries * db->n >= (1LL << 31) - 1)
+        return bp_set_error(e, BP_ERR_TOO_LARGE, "bp_search_batch: queries x subjects must stay below 2^31");
+    CKB(cudaSetDevice(e->device), "cudaSetDevice");
+    bp_batch* b = new bp_batch();
+    b->e = e;
+    b->db = db;
+    b->nq = n_queries;
+    b->n = db->n;
+    b->nseg = (int64_t)n_queries * db->n;
+    b->opt = o;
+    b->queries.assign(queries, queries + n_queries);
+    plan_chunks(db, o.chunk_residues, b->chunk_first);
+    const int32_t n_chunks = (int32_t)b->chunk_first.size() - 1;
+
+    std::vector<BatchQuery> hq(n_queries);
+    double hits_sum = 0;
+    int window = -1;
+    for (int32_t i = 0; i < n_queries; ++i) {
+        const bp_query* q = queries[i];
+        if (window >= 0 && q->p.window != window) {
+            delete b;
+            return bp_set_error(e, BP_ERR_INVALID, "bp_search_batch: all queries must share one window");
+        }
+        window = q->p.window;
+        hq[i].query = q->d_q;
+        hq[i].cells = q->d_cells;
+        hq[i].entries = q->d_entries;
+        hq[i].ctx = q->d_ctx;
+        hq[i].qlen = q->qlen;
+        hq[i].n_entries = (int32_t)q->n_entries;
+        hq[i].n_ctx = q->n_ctx;
+        hq[i].diag_mask = q->diag_mask;
+        if (!bp_scan_fits(q->qlen, q->diag_mask, q->n_entries, e->smem_optin)) {
+            delete b;
+            return bp_set_error(e, BP_ERR_TOO_LARGE, "bp_search_batch: a query is too long for the diagonal array");
+        }
+        hits_sum += q->hits_per_residue;
+    }
+    // classes: one per distinct diagonal-array size, longest first
+    std::vector<int32_t> order(n_queries);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int32_t x, int32_t y) { return hq[x].diag_mask > hq[y].diag_mask; });
+    std::vector<WorkItem> items;
+    items.reserve((size_t)n_queries * n_chunks);
+    std::vector<int32_t> item_pos((size_t)n_queries * n_chunks);   // caller's item index -> position
+    for (size_t i = 0; i < order.size();) {
+        bp_batch::Class k;
+        k.max_mask = hq[order[i]].diag_mask;
+        k.item_lo = (int32_t)items.size();
+        for (; i < order.size() && hq[order[i]].diag_mask == k.max_mask; ++i) {
+            const int32_t qi = order[i];
+            k.max_qlen = std::max(k.max_qlen, hq[qi].qlen);
+            k.max_entries = std::max<int64_t>(k.max_entries, hq[qi].n_entries);
+            k.est += queries[qi]->hits_per_residue;
+            for (int32_t c = 0; c < n_chunks; ++c) {
+                item_pos[(size_t)qi * n_chunks + c] = (int32_t)items.size();
+                WorkItem w;
+                w.qid = qi;
+                w.first = b->chunk_first[c];
+                w.count = b->chunk_first[c + 1] - b->chunk_first[c];
+                w.pad = 0;
+                items.push_back(w);
+            }
+        }
+        k.item_hi = (int32_t)items.size();
+        b->classes.push_back(k);
+    }
+    b->n_items = (int32_t)items.size();
+    // per-CTA queues of each class (indices local to the class)
+    const int grid_max = o.ctas > 0 ? o.ctas : e->sm_count;
+    std::vector<int32_t> qoff(1, 0), qitems;
+    b->queue_cost.clear();
+    for (bp_batch::Class& k : b->classes) {
+        const int32_t nk = k.item_hi - k.item_lo;
+        k.grid = std::max(1, std::min(grid_max, nk));
+        k.queue_lo = (int32_t)qoff.size() - 1;
+        std::vector<std::vector<int32_t>> qs(k.grid);
+        std::vector<double> load(k.grid, 0.0);
+        if (o.schedule == BP_SCHED_COSTS) {
+            // longest predicted item first, into the least loaded queue; each
+            // queue then runs its items in order, query by query, so a CTA
+            // reloads a query's table only when the query changes
+            std::vector<int32_t> loc(nk);
+            std::iota(loc.begin(), loc.end(), 0);
+            std::vector<float> cost(nk);
+            for (int32_t qi = 0; qi < n_queries; ++qi)
+                for (int32_t c = 0; c < n_chunks; ++c) {
+                    const int32_t pos = item_pos[(size_t)qi * n_chunks + c];
+                    if (pos >= k.item_lo && pos < k.item_hi) cost[pos - k.item_lo] = std::max(0.f, o.item_costs[(size_t)qi * n_chunks + c]);
+                }
+            std::stable_sort(loc.begin(), loc.end(), [&](int32_t x, int32_t y) { return cost[x] > cost[y]; });
+            typedef std::pair<double, int> Load;
+            std::priority_queue<Load, std::vector<Load>, std::greater<Load>> heap;
+            for (int c = 0; c < k.grid; ++c) heap.push(Load(0.0, c));
+            for (int32_t i : loc) {
+                Load l = heap.top();
+                heap.pop();
+                qs[l.second].push_back(i);
+                l.first += cost[i];
+                load[l.second] = l.first;
+                heap.push(l);
+            }
+            for (auto& q : qs) std::sort(q.begin(), q.end());
+        } else {
+            for (int32_t i = 0; i < nk; ++i) qs[i % k.grid].push_back(i);
+        }
+        for (int c = 0; c < k.grid; ++c) {
+            qoff.push_back(qoff.back() + (int32_t)qs[c].size());
+            qitems.insert(qitems.end(), qs[c].begin(), qs[c].end());
+            b->queue_cost.push_back(load[c]);
+        }
+    }
+    // record capacity: 1 % of the expected word hits (extensions run on ~5 %
+    // of hits on background composition, fewer succeed); grown and re-run on
+    // overflow, then kept for later runs
+    b->cap = (uint32_t)std::min<double>(1 << 26, std::max(65536.0, 0.01 * hits_sum * (double)db->nres));
+    cudaError_t err = cudaMalloc((void**)&b->d_queries, std::max<size_t>(1, hq.size()) * sizeof(BatchQuery));
+    if (err == cudaSuccess) err = cudaMalloc((void**)&b->d_items, std::max<size_t>(1, items.size()) * sizeof(WorkItem));
+    if (err == cudaSuccess) err = cudaMalloc((void**)&b->d_queue_off, qoff.size() * sizeof(int32_t));
+    if (err == cudaSuccess) err = cudaMalloc((void**)&b->d_queue_items, std::max<size_t>(1, qitems.size()) * sizeof(int32_t));
+    if (err == cudaSuccess) err = cudaMalloc((void**)&b->d_counters, (size_t)std::max<int64_t>(b->nseg, 1) * 3 * sizeof(int32_t));
+    if (err == cudaSuccess) err = cudaMalloc((void**)&b->d_hsp_off, ((size_t)b->nseg + 1) * sizeof(int64_t));
+    if (err == cudaSuccess && !(b->h_count = bp_pinned_get(e))) err = cudaErrorMemoryAllocation;
+    if (err == cudaSuccess && !hq.empty())
+        err = cudaMemcpy(b->d_queries, hq.data(), hq.size() * sizeof(BatchQuery), cudaMemcpyHostToDevice);
+    if (err == cudaSuccess && !items.empty())
+        err = cudaMemcpy(b->d_items, items.data(), items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice);
+    if (err == cudaSuccess) err = cudaMemcpy(b->d_queue_off, qoff.data(), qoff.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+    if (err == cudaSuccess && !qitems.empty())
+        err = cudaMemcpy(b->d_queue_items, qitems.data(), qitems.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+    if (err != cudaSuccess) {
+        bp_batch_destroy(b);
+        return bp_set_cuda_error(e, err, "bp_search_batch: allocate");
+    }
+    bp_status st = prepare(b);
+    if (st == BP_OK) st = launch_batch(b);
+    if (st != BP_OK) {
+        bp_batch_destroy(b);
+        return st;
+    }
+    *out = b;
+    return BP_OK;
+}
+
+bp_status bp_batch_run(bp_batch* b) {
+    if (!b) return BP_ERR_INVALID;
+    bp_engine* e = b->e;
+    CKB(cudaSetDevice(e->device), "cudaSetDevice");
+    return launch_batch(b);
+}
+
+bp_status bp_batch_wait(bp_batch* b) {
+    if (!b) return BP_ERR_INVALID;
+    bp_engine* e = b->e;
+    if (b->n_hsps >= 0) return BP_OK;
+    CKB(cudaSetDevice(e->device), "cudaSetDevice");
+    for (int attempt = 0; attempt < 4; ++attempt) {
+        CKB(cudaStreamSynchronize(e->stream), "batched search");
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, b->ev0, b->ev1) == cudaSuccess) {
+            b->last_ms = ms;
+            e->last_scan_ms = ms;
+        }
+        cudaGetLastError();
+        const uint32_t count = b->h_count[0];
+        if (count <= b->cap) {
+            b->n_hsps = count;
+            return BP_OK;
+        }
+        b->cap = count + count / 4 + 1024;
+        bp_status st = prepare(b);
+        if (st == BP_OK && b->opt.use_graph) st = capture(b);   // buffers moved: capture again
+        if (st == BP_OK) st = launch_batch(b);
+        if (st != BP_OK) return st;
+    }
+    return bp_set_error(e, BP_ERR_CUDA, "bp_batch_wait: record buffer kept overflowing");
+}
+
+int64_t bp_batch_hsps(const bp_batch* b) { return b ? b->n_hsps : -1; }
+float bp_batch_last_scan_ms(const bp_batch* b) { return b ? b->last_ms : 0.f; }
+int32_t bp_batch_items(const bp_batch* b) { return b ? b->n_items : 0; }
+
+bp_status bp_batch_copy_query(bp_batch* b, int32_t qi, int32_t* counters, int64_t* hsp_off, bp_hsp* hsps,
+                              int64_t* n_hsps) {
+    if (!b || qi < 0 || qi >= b->nq) return BP_ERR_INVALID;
+    bp_status st = bp_batch_wait(b);
+    if (st != BP_OK) return st;
+    bp_engine* e = b->e;
+    const size_t s0 = (size_t)qi * b->n;
+    int64_t lo = 0, hi = 0;
+    CKB(cudaMemcpy(&lo, b->d_hsp_off + s0, sizeof(int64_t), cudaMemcpyDeviceToHost), "copy offsets");
+    CKB(cudaMemcpy(&hi, b->d_hsp_off + s0 + b->n, sizeof(int64_t), cudaMemcpyDeviceToHost), "copy offsets");
+    if (n_hsps) *n_hsps = hi - lo;
+    if (counters && b->n > 0)
+        CKB(cudaMemcpy(counters, b->d_counters + 3 * s0, (size_t)b->n * 3 * sizeof(int32_t), cudaMemcpyDeviceToHost),
+            "copy counters");
+    if (hsp_off) {
+        CKB(cudaMemcpy(hsp_off, b->d_hsp_off + s0, ((size_t)b->n + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost),
+            "copy offsets");
+        for (int32_t i = 0; i <= b->n; ++i) hsp_off[i] -= lo;
+    }
+    if (hsps && hi > lo)
+        CKB(cudaMemcpy(hsps, b->d_hsps + lo, (size_t)(hi - lo) * sizeof(bp_hsp), cudaMemcpyDeviceToHost), "copy hsps");
+    return BP_OK;
+}
+
+bp_status bp_batch_queue_costs(const bp_batch* b, double* costs, int32_t* n_queues) {
+    if (!b || !n_queues) return BP_ERR_INVALID;
+    *n_queues = (int32_t)b->queue_cost.size();
+    if (costs) memcpy(costs, b->queue_cost.data(), b->queue_cost.size() * sizeof(double));
+    return BP_OK;
+}
+
+void bp_batch_destroy(bp_batch* b) {
+    if (!b) return;
+    if (b->e) cudaStreamSynchronize(b->e->stream);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    cudaFree(b->d_queries);
+    cudaFree(b->d_items);
+    cudaFree(b->d_queue_off);
+    cudaFree(b->d_queue_items);
+    cudaFree(b->d_counters);
+    cudaFree(b->d_hsp_off);
+    cudaFree(b->d_hsps);
+    cudaFree(b->d_keys);
+    cudaFree(b->d_recs);
+    cudaFree(b->d_fill);
+    cudaFree(b->d_blocksums);
+    cudaFree(b->d_counts);
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+    for (cudaEvent_t ev : b->ev_join) cudaEventDestroy(ev);
+    for (cudaStream_t st : b->side) cudaStreamDestroy(st);
+    if (b->e) bp_pinned_put(b->e, b->h_count);
+    delete b;
+}
+
+}  // extern "C"

@@ -59,6 +59,7 @@ struct bp_db {
     int64_t* d_off = nullptr;
     int32_t n = 0;
     int64_t nres = 0;
+    std::vector<int64_t> h_off;          // host copy of the offsets (chunk planning)
 };
 
 struct bp_query {
@@ -115,6 +116,39 @@ struct ScanArgs {
     uint32_t* error;            // set when a bounded wait runs out
 };
 
+// Batched form: one query of a batch, one work item, and the launch arguments.
+struct BatchQuery {
+    const uint8_t* query;
+    const uint32_t* cells;
+    const uint16_t* entries;
+    const int32_t* ctx;
+    int32_t qlen, n_entries, n_ctx, diag_mask;
+};
+struct WorkItem {
+    int32_t qid;            // query of the batch
+    int32_t first, count;   // subjects [first, first+count)
+    int32_t pad;
+};
+struct BatchArgs {
+    const uint8_t* db;
+    const int64_t* db_off;
+    int32_t n_subjects;     // segment stride: segment = query * n_subjects + subject
+    const BatchQuery* queries;
+    int32_t n_queries;
+    const WorkItem* items;
+    int32_t n_items;
+    const int32_t* queue_off;     // per-CTA queues: items queue_items[queue_off[c] .. queue_off[c+1]) (or null);
+                                  // item indices are relative to `items`
+    const int32_t* queue_items;
+    uint32_t* item_cursor;        // global cursor when queue_off is null
+    const int8_t* matrix;
+    int32_t window;
+    int32_t* counters;            // 3 per segment
+    HspRec* recs;
+    uint32_t rec_cap;
+    uint32_t* rec_count;
+};
+
 // ---- host helpers ---------------------------------------------------------
 bp_status bp_set_cuda_error(bp_engine* e, cudaError_t err, const char* what);
 bp_status bp_set_error(bp_engine* e, bp_status s, const std::string& msg);
@@ -131,6 +165,8 @@ bool bp_scan_fits(int32_t qlen, int32_t diag_mask, int64_t n_entries, int smem_o
 cudaError_t bp_launch_table_build(bp_engine* e, const uint8_t* d_q, int32_t qlen, int32_t threshold,
                                   uint32_t* d_cells, uint16_t* d_entries, uint32_t* d_counts_tmp, int pass);
 cudaError_t bp_launch_scan(bp_engine* e, const ScanArgs& a);
+cudaError_t bp_launch_scan_batch(bp_engine* e, cudaStream_t stream, const BatchArgs& b, int32_t max_qlen,
+                                 int32_t max_diag_mask, int64_t max_entries, int grid, int max_warps);
 cudaError_t bp_launch_order(bp_engine* e, int32_t n, const int32_t* d_counters, int64_t* d_hsp_off,
                             const HspRec* d_recs, uint32_t rec_cap, const uint32_t* d_rec_count,
                             int32_t* d_fill, bp_hsp* d_out, int32_t* d_keys, int64_t* d_blocksums);

@@ -329,6 +329,7 @@ bp_status bp_db_create(bp_engine* e, const uint8_t* residues, int64_t n_residues
         bp_db_destroy(db);
         return st;
     }
+    db->h_off.assign(offsets, offsets + (size_t)n_subjects + 1);
     *out = db;
     return BP_OK;
 }
@@ -362,6 +363,7 @@ bp_status bp_db_create_device(bp_engine* e, const uint8_t* d_residues, int64_t n
         bp_db_destroy(db);
         return st;
     }
+    db->h_off.swap(off);
     *out = db;
     return BP_OK;
 }

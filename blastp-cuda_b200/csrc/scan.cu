@@ -48,7 +48,7 @@ struct ScanLayout {
     int cells_mode;        // 0: u16 starts in smem, 1: u32 starts in smem, 2: u32 starts in global
     int entries_smem;
     int L;
-    int off_cells, off_entries, off_query, off_warps;
+    int off_cells, off_entries, off_query, off_warps, off_ctl;
     int warp_bytes;        // diagonal array + per-lane position table
     int total;
 };
@@ -409,6 +409,124 @@ scan_kernel(ScanArgs a, ScanLayout lay) {
     }
 }
 
+// Per-CTA control block of the batched kernel (shared memory).
+struct BatchCtl {
+    ScanArgs args;         // the current query's view, read by scan_subject
+    int item;              // work item in hand (-1: none left)
+    unsigned sub_ctr;      // next subject of the item
+};
+
+// Batched form: many queries against one resident database in one launch.
+// Work items are (query, subject chunk) pairs; a CTA takes items from its own
+// queue (per-CTA schedule) or from a global cursor, loads a query's table
+// into shared memory only when the query changes, prefetches the chunk's
+// residues into L2, and its warps share the chunk's subjects.  Each
+// (query, subject) pair is scanned by scan_subject exactly as in the
+// single-query kernel, so every query's result is the single-query result;
+// counters and records are indexed by segment = query * n_subjects + subject.
+template <typename CellT, bool kCellsSmem>
+__global__ void __launch_bounds__(kMaxWarps * 32, 1)
+scan_batch_kernel(BatchArgs b, ScanLayout lay) {
+    uint8_t* sm = bp_smem;
+    int8_t* m = reinterpret_cast<int8_t*>(sm);
+    uint8_t* qs = sm + lay.off_query;
+    BatchCtl* ctl = reinterpret_cast<BatchCtl*>(sm + lay.off_ctl);
+    for (int i = threadIdx.x; i < 28 * BP_MROW; i += blockDim.x) m[i] = b.matrix[i];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint8_t* wr = sm + lay.off_warps + (size_t)warp * lay.warp_bytes;
+    uint32_t* diag = reinterpret_cast<uint32_t*>(wr);
+    uint32_t* lane_pos = reinterpret_cast<uint32_t*>(wr + (size_t)lay.L * 4) + lane * kP * 2;
+    for (int i = lane; i < lay.L; i += 32) diag[i] = 0;
+    int base = b.window;   // diagonal stamp offset, carried across queries (stale stamps stay stale)
+    int cur_q = -1;
+    const CellT* cells = nullptr;
+    const uint16_t* entries = nullptr;
+    int qpos = 0, qend = 0;
+    if (b.queue_off) {
+        qpos = b.queue_off[blockIdx.x];
+        qend = b.queue_off[blockIdx.x + 1];
+    }
+    for (;;) {
+        if (threadIdx.x == 0) {
+            int it = -1;
+            if (b.queue_off) {
+                if (qpos < qend) it = b.queue_items[qpos++];
+            } else {
+                const int k = (int)atomicAdd(b.item_cursor, 1u);
+                if (k < b.n_items) it = k;
+            }
+            ctl->item = it;
+            ctl->sub_ctr = 0;
+        }
+        __syncthreads();
+        const int it = ctl->item;
+        if (it < 0) break;
+        const WorkItem wi = b.items[it];
+        if (wi.qid != cur_q) {
+            const BatchQuery bq = b.queries[wi.qid];
+            for (int i = threadIdx.x; i < bq.qlen; i += blockDim.x) qs[i] = bq.query[i];
+            if (kCellsSmem) {
+                CellT* c = reinterpret_cast<CellT*>(sm + lay.off_cells);
+                for (int i = threadIdx.x; i <= BP_NC; i += blockDim.x) c[i] = (CellT)bq.cells[i];
+                cells = c;
+            } else {
+                cells = reinterpret_cast<const CellT*>(bq.cells);
+            }
+            if (lay.entries_smem) {
+                uint16_t* e = reinterpret_cast<uint16_t*>(sm + lay.off_entries);
+                for (int i = threadIdx.x; i < bq.n_entries; i += blockDim.x) e[i] = bq.entries[i];
+                entries = e;
+            } else {
+                entries = bq.entries;
+            }
+            if (threadIdx.x == 0) {
+                ScanArgs& a = ctl->args;
+                a.query = bq.query;
+                a.qlen = bq.qlen;
+                a.ctx = bq.ctx;
+                a.n_ctx = bq.n_ctx;
+                a.window = b.window;
+                a.diag_mask = bq.diag_mask;
+                a.counters = b.counters;
+                a.recs = b.recs;
+                a.rec_cap = b.rec_cap;
+                a.rec_count = b.rec_count;
+            }
+            cur_q = wi.qid;
+            __syncthreads();
+        }
+        if (threadIdx.x == 0 && wi.count > 0) {
+            // stream the chunk's residues into L2 ahead of the warps
+            long long lo = b.db_off[wi.first] & ~15LL;
+            const long long hi = (b.db_off[wi.first + wi.count] + 15) & ~15LL;
+            while (lo < hi) {
+                const long long n = min(hi - lo, (long long)(1 << 20));
+                prefetch_l2(b.db + lo, (uint32_t)n);
+                lo += n;
+            }
+        }
+        const long long seg0 = (long long)wi.qid * b.n_subjects;
+        for (;;) {
+            unsigned s = 0;
+            if (lane == 0) s = atomicAdd(&ctl->sub_ctr, 1u);
+            s = __shfl_sync(kFull, s, 0);
+            if (s >= (unsigned)wi.count) break;
+            const int oid = wi.first + (int)s;
+            const long long so = b.db_off[oid], eo = b.db_off[oid + 1];
+            if (base + (int)(eo - so) + b.window > (1 << 30)) {
+                // the stamp offset is about to wrap: clear the whole array, since
+                // queries with a wider mask than this one read past its mask
+                for (int i = lane; i < lay.L; i += 32) diag[i] = 0;
+                __syncwarp();
+                base = b.window;
+            }
+            scan_subject<CellT>(ctl->args, m, qs, cells, entries, diag, lane_pos, (int)(seg0 + oid), b.db + so,
+                                (int)(eo - so), base, lane);
+        }
+        __syncthreads();
+    }
+}
+
 ScanLayout make_layout(int qlen, int L, int64_t n_entries, int warps, int cells_mode, int entries_smem) {
     ScanLayout l{};
     l.warps = warps;
@@ -430,6 +548,9 @@ ScanLayout make_layout(int qlen, int L, int64_t n_entries, int warps, int cells_
     const long long wb = al((long long)L * 4 + 32 * kP * 2 * 4, 16);
     l.warp_bytes = (int)(wb > big ? big : wb);
     off += (long long)warps * wb;
+    off = al(off, 16);
+    l.off_ctl = (int)(off > big ? big : off);
+    off += 512;                                       // batched kernel's control block
     l.total = (int)(off > big ? big : off);
     return l;
 }
@@ -466,7 +587,31 @@ cudaError_t launch(bp_engine* e, const ScanArgs& a, const ScanLayout& lay) {
     return cudaGetLastError();
 }
 
+template <typename CellT, bool kCellsSmem>
+cudaError_t launch_batch(bp_engine* e, cudaStream_t stream, const BatchArgs& b, const ScanLayout& lay, int grid) {
+    auto kern = scan_batch_kernel<CellT, kCellsSmem>;
+    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, lay.total);
+    if (err != cudaSuccess) return err;
+    kern<<<grid, lay.warps * 32, lay.total, stream>>>(b, lay);
+    e->launches += 1;
+    return cudaGetLastError();
+}
+
 }  // namespace
+
+static_assert(sizeof(BatchCtl) <= 512, "batched control block must fit its shared-memory slot");
+
+cudaError_t bp_launch_scan_batch(bp_engine* e, cudaStream_t stream, const BatchArgs& b, int32_t max_qlen,
+                                 int32_t max_diag_mask, int64_t max_entries, int grid, int max_warps) {
+    ScanLayout lay;
+    if (!choose_layout(max_qlen, max_diag_mask + 1, max_entries, e->smem_optin, &lay)) return cudaErrorInvalidValue;
+    if (max_warps > 0 && lay.warps > max_warps) {
+        lay = make_layout(max_qlen, max_diag_mask + 1, max_entries, max_warps, lay.cells_mode, lay.entries_smem);
+    }
+    if (lay.cells_mode == 0) return launch_batch<uint16_t, true>(e, stream, b, lay, grid);
+    if (lay.cells_mode == 1) return launch_batch<uint32_t, true>(e, stream, b, lay, grid);
+    return launch_batch<uint32_t, false>(e, stream, b, lay, grid);
+}
 
 bool bp_scan_fits(int32_t qlen, int32_t diag_mask, int64_t n_entries, int smem_optin) {
     ScanLayout l;

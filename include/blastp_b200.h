@@ -129,6 +129,50 @@ bp_status bp_blastp_host(bp_engine* e, const uint8_t* query, int32_t qlen, const
                          int32_t n_subjects, int32_t* counters, int64_t* hsp_off,
                          bp_hsp* hsps, int64_t hsp_cap, int64_t* n_hsps);
 
+/* ---- batched search ------------------------------------------------------
+ * Many queries against one resident database in one persistent launch.  The
+ * reference runs one launch per query (gpu_blastp.cu:197-210); here the
+ * subjects are cut into chunks of about chunk_residues residues and every
+ * (query, chunk) pair is a work item.  Each query's results are identical to
+ * its bp_search results. */
+typedef struct bp_batch bp_batch;
+
+typedef enum {
+    BP_SCHED_DYNAMIC = 0,   /* CTAs take items from one global cursor */
+    BP_SCHED_STATIC = 1,    /* item i goes to CTA i mod ctas */
+    BP_SCHED_COSTS = 2      /* longest predicted item first into the least loaded CTA */
+} bp_schedule;
+
+typedef struct {
+    int32_t chunk_residues;     /* residues per chunk (a chunk holds at least one subject) */
+    int32_t schedule;           /* bp_schedule */
+    int32_t ctas;               /* persistent CTAs (0: one per SM) */
+    int32_t max_warps;          /* warps per CTA cap (0: as many as shared memory allows) */
+    int32_t use_graph;          /* capture the launch sequence once, replay it on bp_batch_run */
+    const float* item_costs;    /* BP_SCHED_COSTS: predicted cost of item q*n_chunks + c */
+} bp_batch_options;
+
+void bp_batch_options_default(bp_batch_options* o);
+/* Chunk boundaries the batch would use: chunk c holds subjects
+ * [chunk_first[c], chunk_first[c+1]).  chunk_first may be NULL to only count. */
+bp_status bp_batch_plan(const bp_db* db, int32_t chunk_residues, int32_t* chunk_first, int32_t* n_chunks);
+/* Creates the batch and enqueues its first run.  The engine, database and
+ * queries must outlive the batch.  All queries share one window. */
+bp_status bp_search_batch(bp_engine* e, const bp_db* db, const bp_query* const* queries, int32_t n_queries,
+                          const bp_batch_options* opt, bp_batch** out);
+/* Enqueues the same search again (a graph replay when use_graph is set). */
+bp_status bp_batch_run(bp_batch* b);
+bp_status bp_batch_wait(bp_batch* b);
+int64_t bp_batch_hsps(const bp_batch* b);            /* all queries, after bp_batch_wait */
+int32_t bp_batch_items(const bp_batch* b);
+float bp_batch_last_scan_ms(const bp_batch* b);      /* device time of the last run's scan launch */
+/* Query qi's results in the bp_result_copy layout (offsets start at 0). */
+bp_status bp_batch_copy_query(bp_batch* b, int32_t qi, int32_t* counters, int64_t* hsp_off, bp_hsp* hsps,
+                              int64_t* n_hsps);
+/* Predicted load of each CTA queue (BP_SCHED_COSTS), for reporting. */
+bp_status bp_batch_queue_costs(const bp_batch* b, double* costs, int32_t* n_queues);
+void bp_batch_destroy(bp_batch* b);
+
 /* The plain search for callers that cannot allocate device memory: a process
  * that hands out a fixed device-memory budget at start-up, a latency-critical
  * path where cudaMalloc/cudaFree would synchronise the device, or code whose
