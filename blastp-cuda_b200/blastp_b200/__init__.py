@@ -6,4 +6,5 @@ synthetic-data generators used by the benchmark and the tests.
 """
 from . import synth  # noqa: F401
 from ._lib import BpError, BpParams, lib  # noqa: F401
-from .api import HSP_DTYPE, Database, Engine, PendingResult, Query, Result, blosum62, default_params  # noqa: F401
+from .api import HSP_DTYPE, Batch, Database, Engine, Mlp, PendingResult, Query, Result, blosum62, default_params  # noqa: F401
+from . import costmodel  # noqa: F401,E402

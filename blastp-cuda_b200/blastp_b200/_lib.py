@@ -31,6 +31,7 @@ class BpBatchOptions(ctypes.Structure):
 
 
 SCHED_DYNAMIC, SCHED_STATIC, SCHED_COSTS = 0, 1, 2
+COST_FEATURES = 24
 
 
 class BpError(RuntimeError):
@@ -77,7 +78,18 @@ SIGNATURES = {
     "bp_batch_last_scan_ms": (ctypes.c_float, [P]),
     "bp_batch_copy_query": (ctypes.c_int, [P, i32, P, P, P, P]),
     "bp_batch_queue_costs": (ctypes.c_int, [P, P, P]),
+    "bp_batch_item_queues": (ctypes.c_int, [P, P]),
     "bp_batch_destroy": (None, [P]),
+    "bp_db_chunk_histograms": (ctypes.c_int, [P, P, P, i32, P]),
+    "bp_batch_features": (ctypes.c_int, [P, P, P, i32, P, i32, ctypes.c_float, P]),
+    "bp_mlp_create": (ctypes.c_int, [P, i32, i32, i32, u64, P]),
+    "bp_mlp_destroy": (None, [P]),
+    "bp_mlp_num_params": (i32, [P]),
+    "bp_mlp_get_params": (ctypes.c_int, [P, P, P]),
+    "bp_mlp_set_params": (ctypes.c_int, [P, P, P]),
+    "bp_mlp_loss_grad": (ctypes.c_int, [P, P, P, i32, P, P]),
+    "bp_mlp_fit": (ctypes.c_int, [P, P, P, i32, i32, i32, ctypes.c_float, u64, P]),
+    "bp_mlp_predict": (ctypes.c_int, [P, P, i32, P]),
     # reference-compatible entry points
     "GPU_BLASTP": (None, [P] * 7 + [ctypes.c_int, P, P, i32, P, i32] + [P] * 7),
     "GPU_BLASTP_get_data": (None, [P, P, i32, P, P, i32, i32]),

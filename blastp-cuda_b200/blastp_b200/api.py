@@ -9,7 +9,7 @@ import ctypes
 import numpy as np
 
 from . import _lib
-from ._lib import BpBatchOptions, BpParams, check, lib
+from ._lib import COST_FEATURES, BpBatchOptions, BpParams, check, lib
 
 HSP_DTYPE = np.dtype([("hsp_q", "<i4"), ("hsp_s", "<i4"), ("query_offset", "<i4"),
                       ("subject_offset", "<i4"), ("hsp_len", "<i4"), ("score", "<i4")])
@@ -117,7 +117,27 @@ class Engine:
         arr = (ctypes.c_void_p * max(1, len(queries)))(*[q.h.value for q in queries])
         h = ctypes.c_void_p()
         check(lib().bp_search_batch(self.h, db.h, arr, len(queries), ctypes.byref(o), ctypes.byref(h)), self.h)
-        return Batch(self, h, db, list(queries))
+        b = Batch(self, h, db, list(queries))
+        b.n_chunks = len(self.plan_chunks(db, chunk_residues)) - 1
+        return b
+
+    def chunk_histograms(self, db: "Database", chunk_first) -> np.ndarray:
+        """Residue counts (28 NCBIstdaa bins) of every chunk, on the device."""
+        first = np.ascontiguousarray(chunk_first, dtype=np.int32)
+        n = len(first) - 1
+        out = np.zeros((max(n, 0), 28), dtype=np.uint32)
+        check(lib().bp_db_chunk_histograms(self.h, db.h, _p(first), n, _p(out)), self.h)
+        return out
+
+    def batch_features(self, db: "Database", queries, chunk_first, planted_density: float = 0.0) -> np.ndarray:
+        """Cost-model features of every (query, chunk) item, row q*n_chunks + c."""
+        first = np.ascontiguousarray(chunk_first, dtype=np.int32)
+        n = len(first) - 1
+        X = np.zeros((len(queries) * n, COST_FEATURES), dtype=np.float32)
+        arr = (ctypes.c_void_p * max(1, len(queries)))(*[q.h.value for q in queries])
+        check(lib().bp_batch_features(self.h, db.h, arr, len(queries), _p(first), n, planted_density, _p(X)),
+              self.h)
+        return X
 
     def blastp_host(self, query, params, residues, offsets, hsp_cap=None):
         """End-to-end: host buffers in, host buffers out (one C call)."""
@@ -262,6 +282,12 @@ class Batch:
         check(lib().bp_batch_queue_costs(self.h, _p(out), ctypes.byref(n)), self.engine.h)
         return out
 
+    def item_queues(self) -> np.ndarray:
+        n = self.n_queries * self.n_chunks
+        out = np.zeros(max(n, 1), dtype=np.int32)
+        check(lib().bp_batch_item_queues(self.h, _p(out)), self.engine.h)
+        return out[:n]
+
     def fetch(self, qi: int) -> Result:
         self.wait()
         n = self.n_subjects
@@ -277,6 +303,66 @@ class Batch:
     def close(self):
         if self.h:
             lib().bp_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Mlp:
+    """Two-layer MLP (ReLU hidden layer, fp32) trained and evaluated on the
+    device by the library's kernels (bp_mlp_*)."""
+
+    def __init__(self, engine: Engine, n_in: int = COST_FEATURES, n_hidden: int = 64, n_out: int = 2,
+                 seed: int = 0):
+        h = ctypes.c_void_p()
+        check(lib().bp_mlp_create(engine.h, n_in, n_hidden, n_out, seed, ctypes.byref(h)), engine.h)
+        self.h = h
+        self.engine = engine
+        self.shape = (n_in, n_hidden, n_out)
+
+    @property
+    def n_params(self) -> int:
+        return int(lib().bp_mlp_num_params(self.h))
+
+    def get_params(self):
+        p = np.zeros(self.n_params, dtype=np.float32)
+        norm = np.zeros(2 * self.shape[0] + 2 * self.shape[2], dtype=np.float32)
+        check(lib().bp_mlp_get_params(self.h, _p(p), _p(norm)), self.engine.h)
+        return p, norm
+
+    def set_params(self, params=None, norm=None):
+        p = None if params is None else np.ascontiguousarray(params, dtype=np.float32)
+        n = None if norm is None else np.ascontiguousarray(norm, dtype=np.float32)
+        check(lib().bp_mlp_set_params(self.h, _p(p), _p(n)), self.engine.h)
+
+    def loss_grad(self, X, T):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        T = np.ascontiguousarray(T, dtype=np.float32)
+        loss = ctypes.c_float(0)
+        g = np.zeros(self.n_params, dtype=np.float32)
+        check(lib().bp_mlp_loss_grad(self.h, _p(X), _p(T), len(X), ctypes.byref(loss), _p(g)), self.engine.h)
+        return float(loss.value), g
+
+    def fit(self, X, T, epochs=200, batch=1024, lr=3e-3, seed=0):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        T = np.ascontiguousarray(T, dtype=np.float32)
+        curve = np.zeros(max(epochs, 1), dtype=np.float32)
+        check(lib().bp_mlp_fit(self.h, _p(X), _p(T), len(X), epochs, batch, lr, seed, _p(curve)), self.engine.h)
+        return curve[:epochs]
+
+    def predict(self, X) -> np.ndarray:
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        Y = np.zeros((len(X), self.shape[2]), dtype=np.float32)
+        check(lib().bp_mlp_predict(self.h, _p(X), len(X), _p(Y)), self.engine.h)
+        return Y
+
+    def close(self):
+        if self.h:
+            lib().bp_mlp_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -63,14 +63,21 @@ def _inverse_cdf_table(probs: np.ndarray, symbols: np.ndarray) -> np.ndarray:
 _BACKGROUND_TABLE = _inverse_cdf_table(STANDARD_PROBS, STANDARD_CODES)
 
 
-def residues(rng: np.random.Generator, n: int, chunk: int = 1 << 26) -> np.ndarray:
-    """n i.i.d. background residues (uint8 NCBIstdaa)."""
+def residues(rng: np.random.Generator, n: int, chunk: int = 1 << 26, probs=None) -> np.ndarray:
+    """n i.i.d. residues (uint8 NCBIstdaa): background composition, or
+    `probs` over the 20 standard residues (STANDARD_CODES order)."""
+    table = _BACKGROUND_TABLE if probs is None else _inverse_cdf_table(np.asarray(probs, np.float64), STANDARD_CODES)
     out = np.empty(n, dtype=np.uint8)
     for lo in range(0, n, chunk):
         hi = min(n, lo + chunk)
         u = rng.integers(0, 65536, size=hi - lo, dtype=np.uint16)
-        np.take(_BACKGROUND_TABLE, u, out=out[lo:hi])
+        np.take(table, u, out=out[lo:hi])
     return out
+
+
+def skewed_composition(rng, strength: float) -> np.ndarray:
+    """Background composition mixed with a random Dirichlet(1) draw."""
+    return (1.0 - strength) * STANDARD_PROBS + strength * rng.dirichlet(np.ones(20))
 
 
 def lognormal_lengths(rng, n, median, sigma, lo, hi) -> np.ndarray:
@@ -121,14 +128,21 @@ class Database:
 
 
 def make_database(rng, n_subjects, queries, plant_rate, seg_range, identity_range,
-                  matrix28, median=300, sigma=0.6, lo=30, hi=5000) -> Database:
+                  matrix28, median=300, sigma=0.6, lo=30, hi=5000, compositions=None) -> Database:
     """Subjects with log-normal lengths; for every query, a `plant_rate`
     fraction of subjects receive a mutated copy of a random query segment of
-    length in seg_range (inclusive) at an identity drawn from identity_range."""
+    length in seg_range (inclusive) at an identity drawn from identity_range.
+    `compositions` (optional): residue compositions of equal contiguous blocks
+    of subjects (default: the background everywhere)."""
     lengths = lognormal_lengths(rng, n_subjects, median, sigma, lo, hi)
     offsets = np.zeros(n_subjects + 1, dtype=np.int64)
     np.cumsum(lengths, out=offsets[1:])
-    res = residues(rng, int(offsets[-1]))
+    if compositions is None:
+        res = residues(rng, int(offsets[-1]))
+    else:
+        k = len(compositions)
+        cut = [int(offsets[(n_subjects * i) // k]) for i in range(k + 1)]
+        res = np.concatenate([residues(rng, cut[i + 1] - cut[i], probs=compositions[i]) for i in range(k)])
     sub_tabs = substitution_tables(np.asarray(matrix28))
     plants = []
     for qi, q in enumerate(queries):

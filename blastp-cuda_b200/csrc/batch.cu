@@ -76,6 +76,7 @@ struct bp_batch {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     std::vector<double> queue_cost;         // predicted cost per CTA queue (cost schedules)
+    std::vector<int32_t> item_queue;        // caller's item index -> queue (-1: dynamic)
 };
 
 namespace {
@@ -326,6 +327,7 @@ bp_status bp_search_batch(bp_engine* e, const bp_db* db, const bp_query* const* 
     b->n_items = (int32_t)items.size();
     // per-CTA queues of each class (indices local to the class)
     const int grid_max = o.ctas > 0 ? o.ctas : e->sm_count;
+    std::vector<int32_t> local_queue(items.size(), -1);
     std::vector<int32_t> qoff(1, 0), qitems;
     b->queue_cost.clear();
     for (bp_batch::Class& k : b->classes) {
@@ -366,8 +368,12 @@ bp_status bp_search_batch(bp_engine* e, const bp_db* db, const bp_query* const* 
             qoff.push_back(qoff.back() + (int32_t)qs[c].size());
             qitems.insert(qitems.end(), qs[c].begin(), qs[c].end());
             b->queue_cost.push_back(load[c]);
+            if (o.schedule != BP_SCHED_DYNAMIC)
+                for (int32_t li : qs[c]) local_queue[(size_t)(k.item_lo + li)] = k.queue_lo + c;
         }
     }
+    b->item_queue.resize(item_pos.size());
+    for (size_t i = 0; i < item_pos.size(); ++i) b->item_queue[i] = local_queue[(size_t)item_pos[i]];
     // record capacity: 1 % of the expected word hits (extensions run on ~5 %
     // of hits on background composition, fewer succeed); grown and re-run on
     // overflow, then kept for later runs
@@ -466,6 +472,12 @@ bp_status bp_batch_queue_costs(const bp_batch* b, double* costs, int32_t* n_queu
     if (!b || !n_queues) return BP_ERR_INVALID;
     *n_queues = (int32_t)b->queue_cost.size();
     if (costs) memcpy(costs, b->queue_cost.data(), b->queue_cost.size() * sizeof(double));
+    return BP_OK;
+}
+
+bp_status bp_batch_item_queues(const bp_batch* b, int32_t* queue_of_item) {
+    if (!b || !queue_of_item) return BP_ERR_INVALID;
+    memcpy(queue_of_item, b->item_queue.data(), b->item_queue.size() * sizeof(int32_t));
     return BP_OK;
 }
 

@@ -171,7 +171,42 @@ bp_status bp_batch_copy_query(bp_batch* b, int32_t qi, int32_t* counters, int64_
                               int64_t* n_hsps);
 /* Predicted load of each CTA queue (BP_SCHED_COSTS), for reporting. */
 bp_status bp_batch_queue_costs(const bp_batch* b, double* costs, int32_t* n_queues);
+/* Queue (index into bp_batch_queue_costs' list) of every item q*n_chunks + c;
+ * -1 under BP_SCHED_DYNAMIC. */
+bp_status bp_batch_item_queues(const bp_batch* b, int32_t* queue_of_item);
 void bp_batch_destroy(bp_batch* b);
+
+/* ---- learned cost model ---------------------------------------------------
+ * A two-layer MLP (ReLU hidden layer, fp32) that predicts each work item's
+ * word-hit and extension counts, trained and evaluated on the device with
+ * the library's own kernels.  No counterpart in the reference. */
+typedef struct bp_mlp bp_mlp;
+#define BP_COST_FEATURES 24
+
+/* Residue counts per chunk (28 bins, NCBIstdaa codes), on the device. */
+bp_status bp_db_chunk_histograms(bp_engine* e, const bp_db* db, const int32_t* chunk_first, int32_t n_chunks,
+                                 uint32_t* counts);
+/* Features of item q*n_chunks + c, BP_COST_FEATURES floats each:
+ * log(1+query length), log(1+neighbour-word entries), log(1+chunk residues),
+ * the chunk's composition over the 20 standard residues (fractions), and the
+ * caller's planted-homolog density (0 when unknown). */
+bp_status bp_batch_features(bp_engine* e, const bp_db* db, const bp_query* const* queries, int32_t n_queries,
+                            const int32_t* chunk_first, int32_t n_chunks, float planted_density, float* X);
+bp_status bp_mlp_create(bp_engine* e, int32_t n_in, int32_t n_hidden, int32_t n_out, uint64_t seed, bp_mlp** out);
+void bp_mlp_destroy(bp_mlp* m);
+int32_t bp_mlp_num_params(const bp_mlp* m);
+/* Parameters W1[in][hidden], b1[hidden], W2[hidden][out], b2[out]; norm =
+ * x_mean[in], x_std[in], y_mean[out], y_std[out].  Either may be NULL. */
+bp_status bp_mlp_get_params(bp_mlp* m, float* params, float* norm);
+bp_status bp_mlp_set_params(bp_mlp* m, const float* params, const float* norm);
+/* Mean squared error over rows and outputs, and its gradient with respect to
+ * the parameters, on raw inputs (no standardisation). */
+bp_status bp_mlp_loss_grad(bp_mlp* m, const float* X, const float* T, int32_t n, float* loss, float* grad);
+/* Standardises X and T per column (kept in the model), then trains with Adam
+ * on shuffled minibatches.  loss_curve: optional, one value per epoch. */
+bp_status bp_mlp_fit(bp_mlp* m, const float* X, const float* T, int32_t n, int32_t epochs, int32_t batch, float lr,
+                     uint64_t seed, float* loss_curve);
+bp_status bp_mlp_predict(bp_mlp* m, const float* X, int32_t n, float* Y);
 
 /* The plain search for callers that cannot allocate device memory: a process
  * that hands out a fixed device-memory budget at start-up, a latency-critical
