@@ -44,6 +44,10 @@ def parse():
     ap.add_argument("--qlen", type=int, default=500)
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--cpu-seconds", type=float, default=3.0, help="wall-clock budget of the CPU baseline sample")
+    ap.add_argument("--batched", type=int, default=1, help="also measure the batched workload (1 GPU runs only)")
+    ap.add_argument("--batch-subjects", type=int, default=2_000_000)
+    ap.add_argument("--batch-queries", type=int, default=256)
+    ap.add_argument("--batch-reps", type=int, default=1)
     return ap.parse_args()
 
 
@@ -159,6 +163,113 @@ def cpu_baseline(matrix, w, budget_s, threads):
     return {"value": done_res * len(q) / dt, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": "first %d subjects (%d residues) x %d reps, query %d aa, all host threads; %.1f s wall"
                       % (n, int(off[-1]), reps, len(q), dt)}
+
+
+def run_batched(eng, matrix, args, torch):
+    """256 queries (50-2000 aa) vs 2,000,000 subjects: the plain form (one
+    search per query, back to back on the stream) against the batched
+    persistent launch under each schedule, the autotuned configuration, and
+    the learned schedule; device time with CUDA events on the engine stream."""
+    from blastp_b200 import costmodel, synth
+    from blastp_b200._lib import SCHED_COSTS, SCHED_DYNAMIC, SCHED_NAMES, SCHED_STATIC
+    w = synth.shape3(matrix, n_subjects=args.batch_subjects, n_queries=args.batch_queries)
+    db = eng.database(w.db.residues, w.db.offsets)
+    qs = [eng.query(q) for q in w.queries]
+    qres = int(sum(len(q) for q in w.queries))
+    work = float(w.db.n_residues) * qres
+    stream = torch.cuda.ExternalStream(eng.stream)
+
+    def timed(fn):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), out
+
+    def plain_all():
+        return [eng.search(db, q) for q in qs]
+
+    for r in plain_all():                 # warm-up
+        r.close()
+    plain_ms, rs = timed(plain_all)
+    plain_counts = []
+    from blastp_b200._lib import lib
+    for r in rs:
+        r.wait()
+        plain_counts.append(int(lib().bp_result_hsps(r.h)))
+    check_q = [0, len(qs) // 2, len(qs) - 1]
+    plain_check = {i: eng.search(db, qs[i]).fetch() for i in check_q}
+    for r in rs:
+        r.close()
+    out = {"workload": w.name, "queries": len(qs), "query_residues": qres, "subjects": w.db.n_subjects,
+           "residues": w.db.n_residues, "plain": {"ms": plain_ms, "value": work / (plain_ms / 1e3)}}
+    model = costmodel.CostModel.load(eng)
+    planted = 0.002
+    t0 = time.perf_counter()
+    best, trials = eng.autotune(db, qs, model=model, planted_density=planted,
+                                sample_subjects=max(1, w.db.n_subjects // 16), reps=1)
+    out["autotune"] = {"sample_subjects": max(1, w.db.n_subjects // 16), "seconds": time.perf_counter() - t0,
+                       "best": dict(best, schedule=SCHED_NAMES[best["schedule"]]),
+                       "trials": [[t["chunk_residues"], SCHED_NAMES[t["schedule"]], t["max_warps"], round(t["ms"], 3)]
+                                  for t in trials]}
+    variants = {"static": dict(chunk_residues=1 << 20, schedule=SCHED_STATIC),
+                "dynamic": dict(chunk_residues=1 << 20, schedule=SCHED_DYNAMIC),
+                "learned": dict(chunk_residues=1 << 20, schedule=SCHED_COSTS),
+                "autotuned": dict(best)}
+    identical = True
+    res = {}
+    for name, kw in variants.items():
+        if kw["schedule"] == SCHED_COSTS:
+            first = eng.plan_chunks(db, kw["chunk_residues"])
+            kw["item_costs"] = eng.predict_costs(model, db, qs, first, planted)
+        b = eng.search_batch(db, qs, **kw)
+        b.wait()
+        launches0 = eng.launches
+        ms_runs = []
+        for _ in range(max(1, args.batch_reps)):
+            ms, _ = timed(lambda: b.run())
+            b.wait()
+            ms_runs.append(ms)
+        ms = float(min(ms_runs))
+        res[name] = {"ms": ms, "value": work / (ms / 1e3), "speedup_vs_plain": plain_ms / ms,
+                     "chunk_residues": kw["chunk_residues"], "schedule": SCHED_NAMES[kw["schedule"]],
+                     "max_warps": kw.get("max_warps", 0), "items": b.n_items,
+                     "launches_per_run": (eng.launches - launches0) // max(1, args.batch_reps)}
+        if b.n_hsps != sum(plain_counts):
+            identical = False
+        for i in check_q:
+            r = b.fetch(i)
+            p = plain_check[i]
+            if not (np.array_equal(r.counters, p.counters) and np.array_equal(r.hsp_off, p.hsp_off) and
+                    np.array_equal(r.hsps_as_array(), p.hsps_as_array())):
+                identical = False
+        if name == "learned":
+            # count error of the model on this workload: items of the checked queries
+            first = eng.plan_chunks(db, kw["chunk_residues"])
+            nc = len(first) - 1
+            X = eng.batch_features(db, [qs[i] for i in check_q], first, planted)
+            pred = model.predict_counts(X)
+            true = np.concatenate([costmodel.chunk_sums(plain_check[i].counters, first)[:, [0, 2]]
+                                   for i in check_q])
+            res[name]["mlp_error"] = {"hits": costmodel.relative_error(pred[:, 0], true[:, 0]),
+                                      "extensions": costmodel.relative_error(pred[:, 1], true[:, 1]),
+                                      "items": int(len(true)), "queries": len(check_q), "chunks": nc}
+        b.close()
+    out["batched"] = res
+    out["identical_to_plain"] = identical
+    out["hsps"] = int(sum(plain_counts))
+    try:
+        with open(os.path.join(os.path.dirname(costmodel.MODEL_PATH), "costmodel_b200_report.json")) as f:
+            out["mlp_training"] = json.load(f)
+    except OSError:
+        pass
+    for q in qs:
+        q.close()
+    db.close()
+    return out
 
 
 def run_reference(args):
@@ -316,6 +427,8 @@ def run_ours(args):
         "hsps": int(len(ref_hsps.hsps)),
     }
     line["clocks"] = clk.summary()
+    if world == 1 and args.batched:
+        line["batched"] = run_batched(eng, matrix, args, torch)
     if rank == 0:
         sys.path.insert(0, ROOT)
         line["cpu_baseline"] = cpu_baseline(matrix, w, args.cpu_seconds, os.cpu_count() or 1)

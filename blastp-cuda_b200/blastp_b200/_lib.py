@@ -27,10 +27,21 @@ class BpParams(ctypes.Structure):
 
 class BpBatchOptions(ctypes.Structure):
     _fields_ = [("chunk_residues", i32), ("schedule", i32), ("ctas", i32), ("max_warps", i32),
-                ("use_graph", i32), ("item_costs", P)]
+                ("use_graph", i32), ("item_costs", P), ("subject_first", i32), ("subject_count", i32)]
+
+
+class BpAutotuneTrial(ctypes.Structure):
+    _fields_ = [("chunk_residues", i32), ("schedule", i32), ("max_warps", i32), ("ms", ctypes.c_float)]
+
+
+class BpAutotuneOptions(ctypes.Structure):
+    _fields_ = [("chunk_sizes", P), ("n_chunk_sizes", i32), ("warp_caps", P), ("n_warp_caps", i32),
+                ("schedules_mask", i32), ("model", P), ("cost_weights", ctypes.c_float * 3),
+                ("planted_density", ctypes.c_float), ("sample_subjects", i32), ("reps", i32)]
 
 
 SCHED_DYNAMIC, SCHED_STATIC, SCHED_COSTS = 0, 1, 2
+SCHED_NAMES = {0: "dynamic", 1: "static", 2: "learned"}
 COST_FEATURES = 24
 
 
@@ -69,7 +80,7 @@ SIGNATURES = {
     "bp_blastp_host": (ctypes.c_int, [P, P, i32, P, P, i64, P, i32, P, P, P, i64, P]),
     "bp_search_noalloc": (ctypes.c_int, [P, i32, P, P, i64, P, i32, P, P, P, i64, P, P]),
     "bp_batch_options_default": (None, [P]),
-    "bp_batch_plan": (ctypes.c_int, [P, i32, P, P]),
+    "bp_batch_plan": (ctypes.c_int, [P, i32, i32, i32, P, P]),
     "bp_search_batch": (ctypes.c_int, [P, P, P, i32, P, P]),
     "bp_batch_run": (ctypes.c_int, [P]),
     "bp_batch_wait": (ctypes.c_int, [P]),
@@ -90,6 +101,9 @@ SIGNATURES = {
     "bp_mlp_loss_grad": (ctypes.c_int, [P, P, P, i32, P, P]),
     "bp_mlp_fit": (ctypes.c_int, [P, P, P, i32, i32, i32, ctypes.c_float, u64, P]),
     "bp_mlp_predict": (ctypes.c_int, [P, P, i32, P]),
+    "bp_batch_predict_costs": (ctypes.c_int, [P, P, P, P, P, i32, P, i32, ctypes.c_float, P]),
+    "bp_autotune_options_default": (None, [P]),
+    "bp_batch_autotune": (ctypes.c_int, [P, P, P, i32, P, P, P, i32, P]),
     # reference-compatible entry points
     "GPU_BLASTP": (None, [P] * 7 + [ctypes.c_int, P, P, i32, P, i32] + [P] * 7),
     "GPU_BLASTP_get_data": (None, [P, P, i32, P, P, i32, i32]),

@@ -9,7 +9,7 @@ import ctypes
 import numpy as np
 
 from . import _lib
-from ._lib import COST_FEATURES, BpBatchOptions, BpParams, check, lib
+from ._lib import COST_FEATURES, BpAutotuneOptions, BpAutotuneTrial, BpBatchOptions, BpParams, check, lib
 
 HSP_DTYPE = np.dtype([("hsp_q", "<i4"), ("hsp_s", "<i4"), ("query_offset", "<i4"),
                       ("subject_offset", "<i4"), ("hsp_len", "<i4"), ("score", "<i4")])
@@ -90,17 +90,18 @@ class Engine:
         check(lib().bp_search(self.h, db.h, q.h, first, count, ctypes.byref(h)), self.h)
         return PendingResult(self, h, keep=(db, q))
 
-    def plan_chunks(self, db: "Database", chunk_residues: int) -> np.ndarray:
-        """Chunk boundaries of a batched search: chunk c holds subjects
-        [first[c], first[c+1])."""
+    def plan_chunks(self, db: "Database", chunk_residues: int, first: int = 0, count: int = -1) -> np.ndarray:
+        """Chunk boundaries of a batched search over subjects [first,
+        first+count): chunk c holds subjects [b[c], b[c+1])."""
         n = ctypes.c_int32(0)
-        check(lib().bp_batch_plan(db.h, chunk_residues, None, ctypes.byref(n)), self.h)
-        first = np.zeros(n.value + 1, dtype=np.int32)
-        check(lib().bp_batch_plan(db.h, chunk_residues, _p(first), ctypes.byref(n)), self.h)
-        return first
+        check(lib().bp_batch_plan(db.h, first, count, chunk_residues, None, ctypes.byref(n)), self.h)
+        out = np.zeros(n.value + 1, dtype=np.int32)
+        check(lib().bp_batch_plan(db.h, first, count, chunk_residues, _p(out), ctypes.byref(n)), self.h)
+        return out
 
     def search_batch(self, db: "Database", queries, chunk_residues: int = 1 << 18, schedule: int = 0,
-                     ctas: int = 0, max_warps: int = 0, use_graph: bool = True, item_costs=None) -> "Batch":
+                     ctas: int = 0, max_warps: int = 0, use_graph: bool = True, item_costs=None,
+                     first: int = 0, count: int = -1) -> "Batch":
         """Many queries against db in one persistent launch; each query's
         result equals its single-query search."""
         o = BpBatchOptions()
@@ -110,6 +111,8 @@ class Engine:
         o.ctas = ctas
         o.max_warps = max_warps
         o.use_graph = int(bool(use_graph))
+        o.subject_first = first
+        o.subject_count = count
         costs = None
         if item_costs is not None:
             costs = np.ascontiguousarray(item_costs, dtype=np.float32)
@@ -118,7 +121,8 @@ class Engine:
         h = ctypes.c_void_p()
         check(lib().bp_search_batch(self.h, db.h, arr, len(queries), ctypes.byref(o), ctypes.byref(h)), self.h)
         b = Batch(self, h, db, list(queries))
-        b.n_chunks = len(self.plan_chunks(db, chunk_residues)) - 1
+        b.n_chunks = len(self.plan_chunks(db, chunk_residues, first, count)) - 1
+        b.n_subjects = (db.n_subjects - first) if count < 0 else count
         return b
 
     def chunk_histograms(self, db: "Database", chunk_first) -> np.ndarray:
@@ -138,6 +142,54 @@ class Engine:
         check(lib().bp_batch_features(self.h, db.h, arr, len(queries), _p(first), n, planted_density, _p(X)),
               self.h)
         return X
+
+    def predict_costs(self, model, db: "Database", queries, chunk_first, planted_density: float = 0.0):
+        """Item costs of the cost schedule (bp_batch_predict_costs) from a
+        costmodel.CostModel."""
+        first = np.ascontiguousarray(chunk_first, dtype=np.int32)
+        n = len(first) - 1
+        out = np.zeros(len(queries) * n, dtype=np.float32)
+        w = np.ascontiguousarray(model.weights, dtype=np.float32)
+        arr = (ctypes.c_void_p * max(1, len(queries)))(*[q.h.value for q in queries])
+        check(lib().bp_batch_predict_costs(self.h, model.mlp.h, _p(w), db.h, arr, len(queries), _p(first), n,
+                                           planted_density, _p(out)), self.h)
+        return out
+
+    def autotune(self, db: "Database", queries, model=None, planted_density: float = 0.0, sample_subjects: int = 0,
+                 chunk_sizes=None, warp_caps=None, schedules=(0, 1, 2), reps: int = 2):
+        """Times candidate batch configurations on a sample of the subjects
+        (bp_batch_autotune); returns (best options dict, list of trials)."""
+        o = BpAutotuneOptions()
+        lib().bp_autotune_options_default(ctypes.byref(o))
+        keep = []
+        if chunk_sizes is not None:
+            cs = np.ascontiguousarray(chunk_sizes, dtype=np.int32)
+            keep.append(cs)
+            o.chunk_sizes = cs.ctypes.data
+            o.n_chunk_sizes = len(cs)
+        if warp_caps is not None:
+            wc = np.ascontiguousarray(warp_caps, dtype=np.int32)
+            keep.append(wc)
+            o.warp_caps = wc.ctypes.data
+            o.n_warp_caps = len(wc)
+        o.schedules_mask = sum(1 << s for s in schedules)
+        if model is not None:
+            o.model = model.mlp.h.value
+            for i in range(3):
+                o.cost_weights[i] = float(model.weights[i])
+        o.planted_density = planted_density
+        o.sample_subjects = sample_subjects
+        o.reps = reps
+        best = BpBatchOptions()
+        trials = (BpAutotuneTrial * 256)()
+        nt = ctypes.c_int32(0)
+        arr = (ctypes.c_void_p * max(1, len(queries)))(*[q.h.value for q in queries])
+        check(lib().bp_batch_autotune(self.h, db.h, arr, len(queries), ctypes.byref(o), ctypes.byref(best), trials,
+                                      256, ctypes.byref(nt)), self.h)
+        out = [{"chunk_residues": t.chunk_residues, "schedule": t.schedule, "max_warps": t.max_warps,
+                "ms": float(t.ms)} for t in trials[:min(nt.value, 256)]]
+        return ({"chunk_residues": best.chunk_residues, "schedule": best.schedule, "max_warps": best.max_warps},
+                out)
 
     def blastp_host(self, query, params, residues, offsets, hsp_cap=None):
         """End-to-end: host buffers in, host buffers out (one C call)."""

@@ -34,7 +34,7 @@
 struct bp_batch {
     bp_engine* e = nullptr;
     const bp_db* db = nullptr;
-    int32_t nq = 0, n = 0;
+    int32_t nq = 0, n = 0, first = 0;    // n subjects from `first`
     int64_t nseg = 0;
     std::vector<const bp_query*> queries;
     bp_batch_options opt{};
@@ -81,20 +81,30 @@ struct bp_batch {
 
 namespace {
 
-void plan_chunks(const bp_db* db, int32_t chunk_residues, std::vector<int32_t>& first) {
+// Chunk boundaries over subjects [s0, s1): each chunk holds at least one
+// subject, then as many more as keep it within chunk_residues residues.
+void plan_chunks(const bp_db* db, int32_t s0, int32_t s1, int32_t chunk_residues, std::vector<int32_t>& first) {
     first.clear();
-    first.push_back(0);
+    first.push_back(s0);
     const int64_t* off = db->h_off.data();
-    int32_t s = 0;
-    while (s < db->n) {
+    int32_t s = s0;
+    while (s < s1) {
         const int64_t limit = off[s] + std::max<int64_t>(chunk_residues, 1);
-        // at least one subject per chunk, then as many as fit under the limit
-        int32_t t = (int32_t)(std::upper_bound(off + s + 1, off + db->n + 1, limit) - off) - 1;
+        int32_t t = (int32_t)(std::upper_bound(off + s + 1, off + s1 + 1, limit) - off) - 1;
         if (t <= s) t = s + 1;
-        if (t > db->n) t = db->n;
+        if (t > s1) t = s1;
         first.push_back(t);
         s = t;
     }
+}
+
+bool resolve_range(const bp_db* db, int32_t first, int32_t count, int32_t* s0, int32_t* s1) {
+    if (first < 0 || first > db->n) return false;
+    if (count < 0) count = db->n - first;
+    if ((int64_t)first + count > db->n) return false;
+    *s0 = first;
+    *s1 = first + count;
+    return true;
 }
 
 // Enqueues the batch's device work on the engine stream: one persistent
@@ -115,6 +125,7 @@ bp_status enqueue(bp_batch* b) {
         a.db = b->db->d_res;
         a.db_off = b->db->d_off;
         a.n_subjects = b->n;
+        a.subject_first = b->first;
         a.queries = b->d_queries;
         a.n_queries = b->nq;
         a.items = b->d_items + k.item_lo;
@@ -236,12 +247,16 @@ void bp_batch_options_default(bp_batch_options* o) {
     o->chunk_residues = 1 << 18;
     o->schedule = BP_SCHED_DYNAMIC;
     o->use_graph = 1;
+    o->subject_first = 0;
+    o->subject_count = -1;
 }
 
-bp_status bp_batch_plan(const bp_db* db, int32_t chunk_residues, int32_t* chunk_first, int32_t* n_chunks) {
-    if (!db || !n_chunks) return BP_ERR_INVALID;
+bp_status bp_batch_plan(const bp_db* db, int32_t subject_first, int32_t subject_count, int32_t chunk_residues,
+                        int32_t* chunk_first, int32_t* n_chunks) {
+    int32_t s0 = 0, s1 = 0;
+    if (!db || !n_chunks || !resolve_range(db, subject_first, subject_count, &s0, &s1)) return BP_ERR_INVALID;
     std::vector<int32_t> first;
-    plan_chunks(db, chunk_residues, first);
+    plan_chunks(db, s0, s1, chunk_residues, first);
     *n_chunks = (int32_t)first.size() - 1;
     if (chunk_first) memcpy(chunk_first, first.data(), first.size() * sizeof(int32_t));
     return BP_OK;
@@ -256,18 +271,22 @@ bp_status bp_search_batch(bp_engine* e, const bp_db* db, const bp_query* const* 
     else bp_batch_options_default(&o);
     if (o.schedule == BP_SCHED_COSTS && !o.item_costs)
         return bp_set_error(e, BP_ERR_INVALID, "bp_search_batch: cost schedule without item costs");
-    if ((int64_t)n_queries * db->n >= (1LL << 31) - 1)
+    int32_t s0 = 0, s1 = 0;
+    if (!resolve_range(db, o.subject_first, o.subject_count, &s0, &s1))
+        return bp_set_error(e, BP_ERR_INVALID, "bp_search_batch: subject range outside the database");
+    if ((int64_t)n_queries * (s1 - s0) >= (1LL << 31) - 1)
         return bp_set_error(e, BP_ERR_TOO_LARGE, "bp_search_batch: queries x subjects must stay below 2^31");
     CKB(cudaSetDevice(e->device), "cudaSetDevice");
     bp_batch* b = new bp_batch();
     b->e = e;
     b->db = db;
     b->nq = n_queries;
-    b->n = db->n;
-    b->nseg = (int64_t)n_queries * db->n;
+    b->first = s0;
+    b->n = s1 - s0;
+    b->nseg = (int64_t)n_queries * b->n;
     b->opt = o;
     b->queries.assign(queries, queries + n_queries);
-    plan_chunks(db, o.chunk_residues, b->chunk_first);
+    plan_chunks(db, s0, s1, o.chunk_residues, b->chunk_first);
     const int32_t n_chunks = (int32_t)b->chunk_first.size() - 1;
 
     std::vector<BatchQuery> hq(n_queries);
@@ -505,6 +524,117 @@ void bp_batch_destroy(bp_batch* b) {
     for (cudaStream_t st : b->side) cudaStreamDestroy(st);
     if (b->e) bp_pinned_put(b->e, b->h_count);
     delete b;
+}
+
+}  // extern "C"
+
+// ---- cost prediction and autotuning ---------------------------------------
+
+extern "C" {
+
+bp_status bp_batch_predict_costs(bp_engine* e, bp_mlp* model, const float* weights, const bp_db* db,
+                                 const bp_query* const* queries, int32_t n_queries, const int32_t* chunk_first,
+                                 int32_t n_chunks, float planted_density, float* costs) {
+    if (!e || !model || !weights || !db || !chunk_first || !costs || n_queries < 0 || n_chunks < 0)
+        return BP_ERR_INVALID;
+    const size_t n = (size_t)n_queries * n_chunks;
+    if (n == 0) return BP_OK;
+    std::vector<float> X(n * BP_COST_FEATURES), Y(n * 2);
+    bp_status st = bp_batch_features(e, db, queries, n_queries, chunk_first, n_chunks, planted_density, X.data());
+    if (st == BP_OK) st = bp_mlp_predict(model, X.data(), (int32_t)n, Y.data());
+    if (st != BP_OK) return st;
+    for (size_t i = 0; i < n; ++i) {
+        const double res = expm1((double)X[i * BP_COST_FEATURES + 2]);
+        const double hits = expm1(std::max(0.0, (double)Y[2 * i]));
+        const double ext = expm1(std::max(0.0, (double)Y[2 * i + 1]));
+        costs[i] = (float)(weights[0] * res + weights[1] * hits + weights[2] * ext);
+    }
+    return BP_OK;
+}
+
+void bp_autotune_options_default(bp_autotune_options* o) {
+    memset(o, 0, sizeof(*o));
+    o->schedules_mask = (1 << BP_SCHED_DYNAMIC) | (1 << BP_SCHED_STATIC) | (1 << BP_SCHED_COSTS);
+    o->reps = 2;
+}
+
+// Times every candidate (chunk size x warp cap x schedule) on a sample of the
+// subjects with the whole query set, and returns the fastest as *best.  The
+// cost schedule is tried only with a model; its costs for the full run come
+// from bp_batch_predict_costs with the chosen chunk size.
+bp_status bp_batch_autotune(bp_engine* e, const bp_db* db, const bp_query* const* queries, int32_t n_queries,
+                            const bp_autotune_options* opt, bp_batch_options* best, bp_autotune_trial* trials,
+                            int32_t trials_cap, int32_t* n_trials) {
+    if (!e || !db || !queries || n_queries < 1 || !best) return bp_set_error(e, BP_ERR_INVALID, "bp_batch_autotune");
+    bp_autotune_options o;
+    if (opt) o = *opt;
+    else bp_autotune_options_default(&o);
+    static const int32_t kChunks[] = {1 << 16, 1 << 18, 1 << 20, 1 << 22};
+    static const int32_t kWarps[] = {0, 16};
+    const int32_t* chunks = o.chunk_sizes ? o.chunk_sizes : kChunks;
+    const int n_chunk_sizes = o.chunk_sizes ? o.n_chunk_sizes : 4;
+    const int32_t* warps = o.warp_caps ? o.warp_caps : kWarps;
+    const int n_warp_caps = o.warp_caps ? o.n_warp_caps : 2;
+    const int32_t sample = o.sample_subjects > 0 ? std::min(o.sample_subjects, db->n) : std::max(1, db->n / 16);
+    const int reps = std::max(1, o.reps);
+    bp_batch_options_default(best);
+    float best_ms = 1e30f;
+    int32_t nt = 0;
+    for (int ci = 0; ci < n_chunk_sizes; ++ci) {
+        std::vector<float> costs;
+        for (int sched = 0; sched < 3; ++sched) {
+            if (!(o.schedules_mask & (1 << sched))) continue;
+            if (sched == BP_SCHED_COSTS) {
+                if (!o.model) continue;
+                if (costs.empty()) {
+                    std::vector<int32_t> first;
+                    plan_chunks(db, 0, sample, chunks[ci], first);
+                    costs.resize((size_t)n_queries * (first.size() - 1));
+                    bp_status st = bp_batch_predict_costs(e, o.model, o.cost_weights, db, queries, n_queries,
+                                                          first.data(), (int32_t)first.size() - 1,
+                                                          o.planted_density, costs.data());
+                    if (st != BP_OK) return st;
+                }
+            }
+            for (int wi = 0; wi < n_warp_caps; ++wi) {
+                bp_batch_options bo;
+                bp_batch_options_default(&bo);
+                bo.chunk_residues = chunks[ci];
+                bo.schedule = sched;
+                bo.max_warps = warps[wi];
+                bo.item_costs = sched == BP_SCHED_COSTS ? costs.data() : nullptr;
+                bo.subject_first = 0;
+                bo.subject_count = sample;
+                bp_batch* b = nullptr;
+                bp_status st = bp_search_batch(e, db, queries, n_queries, &bo, &b);
+                if (st == BP_OK) st = bp_batch_wait(b);
+                float ms = 1e30f;
+                for (int r = 0; r < reps && st == BP_OK; ++r) {
+                    st = bp_batch_run(b);
+                    if (st == BP_OK) st = bp_batch_wait(b);
+                    if (st == BP_OK) ms = std::min(ms, b->last_ms);
+                }
+                bp_batch_destroy(b);
+                if (st != BP_OK) return st;
+                if (trials && nt < trials_cap) {
+                    trials[nt].chunk_residues = bo.chunk_residues;
+                    trials[nt].schedule = bo.schedule;
+                    trials[nt].max_warps = bo.max_warps;
+                    trials[nt].ms = ms;
+                }
+                ++nt;
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    *best = bo;
+                    best->item_costs = nullptr;
+                    best->subject_first = 0;
+                    best->subject_count = -1;
+                }
+            }
+        }
+    }
+    if (n_trials) *n_trials = nt;
+    return BP_OK;
 }
 
 }  // extern "C"

@@ -132,7 +132,8 @@ struct WorkItem {
 struct BatchArgs {
     const uint8_t* db;
     const int64_t* db_off;
-    int32_t n_subjects;     // segment stride: segment = query * n_subjects + subject
+    int32_t n_subjects;     // segment stride: segment = query * n_subjects + (subject - subject_first)
+    int32_t subject_first;
     const BatchQuery* queries;
     int32_t n_queries;
     const WorkItem* items;

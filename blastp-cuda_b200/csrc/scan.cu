@@ -520,8 +520,8 @@ scan_batch_kernel(BatchArgs b, ScanLayout lay) {
                 __syncwarp();
                 base = b.window;
             }
-            scan_subject<CellT>(ctl->args, m, qs, cells, entries, diag, lane_pos, (int)(seg0 + oid), b.db + so,
-                                (int)(eo - so), base, lane);
+            scan_subject<CellT>(ctl->args, m, qs, cells, entries, diag, lane_pos, (int)(seg0 + oid - b.subject_first),
+                                b.db + so, (int)(eo - so), base, lane);
         }
         __syncthreads();
     }

@@ -150,12 +150,17 @@ typedef struct {
     int32_t max_warps;          /* warps per CTA cap (0: as many as shared memory allows) */
     int32_t use_graph;          /* capture the launch sequence once, replay it on bp_batch_run */
     const float* item_costs;    /* BP_SCHED_COSTS: predicted cost of item q*n_chunks + c */
+    int32_t subject_first;      /* subjects [subject_first, subject_first + subject_count) */
+    int32_t subject_count;      /* (< 0: to the end of the database) */
 } bp_batch_options;
 
 void bp_batch_options_default(bp_batch_options* o);
-/* Chunk boundaries the batch would use: chunk c holds subjects
- * [chunk_first[c], chunk_first[c+1]).  chunk_first may be NULL to only count. */
-bp_status bp_batch_plan(const bp_db* db, int32_t chunk_residues, int32_t* chunk_first, int32_t* n_chunks);
+/* Chunk boundaries the batch would use over subjects [subject_first,
+ * subject_first + subject_count) (count < 0: to the end): chunk c holds
+ * subjects [chunk_first[c], chunk_first[c+1]).  chunk_first may be NULL to
+ * only count. */
+bp_status bp_batch_plan(const bp_db* db, int32_t subject_first, int32_t subject_count, int32_t chunk_residues,
+                        int32_t* chunk_first, int32_t* n_chunks);
 /* Creates the batch and enqueues its first run.  The engine, database and
  * queries must outlive the batch.  All queries share one window. */
 bp_status bp_search_batch(bp_engine* e, const bp_db* db, const bp_query* const* queries, int32_t n_queries,
@@ -166,7 +171,8 @@ bp_status bp_batch_wait(bp_batch* b);
 int64_t bp_batch_hsps(const bp_batch* b);            /* all queries, after bp_batch_wait */
 int32_t bp_batch_items(const bp_batch* b);
 float bp_batch_last_scan_ms(const bp_batch* b);      /* device time of the last run's scan launch */
-/* Query qi's results in the bp_result_copy layout (offsets start at 0). */
+/* Query qi's results in the bp_result_copy layout (offsets start at 0),
+ * for the batch's subjects (index 0 = subject_first). */
 bp_status bp_batch_copy_query(bp_batch* b, int32_t qi, int32_t* counters, int64_t* hsp_off, bp_hsp* hsps,
                               int64_t* n_hsps);
 /* Predicted load of each CTA queue (BP_SCHED_COSTS), for reporting. */
@@ -207,6 +213,39 @@ bp_status bp_mlp_loss_grad(bp_mlp* m, const float* X, const float* T, int32_t n,
 bp_status bp_mlp_fit(bp_mlp* m, const float* X, const float* T, int32_t n, int32_t epochs, int32_t batch, float lr,
                      uint64_t seed, float* loss_curve);
 bp_status bp_mlp_predict(bp_mlp* m, const float* X, int32_t n, float* Y);
+
+/* Item costs for BP_SCHED_COSTS from a model predicting log(1 + hits) and
+ * log(1 + extensions):  cost = w[0]*residues + w[1]*hits + w[2]*extensions. */
+bp_status bp_batch_predict_costs(bp_engine* e, bp_mlp* model, const float* weights, const bp_db* db,
+                                 const bp_query* const* queries, int32_t n_queries, const int32_t* chunk_first,
+                                 int32_t n_chunks, float planted_density, float* costs);
+
+/* ---- autotuner -------------------------------------------------------------
+ * Times candidate batch configurations (subject-chunk size, warps per CTA,
+ * schedule) on the first sample_subjects subjects with the whole query set
+ * and returns the fastest. */
+typedef struct {
+    int32_t chunk_residues, schedule, max_warps;
+    float ms;                   /* best scan time of the candidate on the sample */
+} bp_autotune_trial;
+
+typedef struct {
+    const int32_t* chunk_sizes; /* NULL: 64Ki, 256Ki, 1Mi, 4Mi residues */
+    int32_t n_chunk_sizes;
+    const int32_t* warp_caps;   /* NULL: {0 (as many as fit), 16} */
+    int32_t n_warp_caps;
+    int32_t schedules_mask;     /* bit s tries bp_schedule s; BP_SCHED_COSTS needs model */
+    bp_mlp* model;
+    float cost_weights[3];
+    float planted_density;
+    int32_t sample_subjects;    /* <= 0: 1/16 of the database */
+    int32_t reps;               /* timed runs per candidate, best kept */
+} bp_autotune_options;
+
+void bp_autotune_options_default(bp_autotune_options* o);
+bp_status bp_batch_autotune(bp_engine* e, const bp_db* db, const bp_query* const* queries, int32_t n_queries,
+                            const bp_autotune_options* opt, bp_batch_options* best, bp_autotune_trial* trials,
+                            int32_t trials_cap, int32_t* n_trials);
 
 /* The plain search for callers that cannot allocate device memory: a process
  * that hands out a fixed device-memory budget at start-up, a latency-critical

@@ -139,3 +139,39 @@ def test_batch_rejects_mixed_windows_and_missing_costs(engine):
         engine.search_batch(d, [a, c])
     with pytest.raises(BpError):
         engine.search_batch(d, [a], schedule=SCHED_COSTS)
+
+
+@pytest.mark.parametrize("first,count", [(0, 5000), (3333, 4000), (11_999, 1), (12_000, 0), (7000, -1)])
+def test_subject_range(engine, workload, first, count):
+    qs, db = workload
+    d = engine.database(db.residues, db.offsets)
+    hs = [engine.query(q) for q in qs[:4]]
+    b = engine.search_batch(d, hs, chunk_residues=1 << 16, first=first, count=count)
+    for i, h in enumerate(hs):
+        s = engine.search(d, h, first, count).fetch()
+        assert_same(b.fetch(i), (s.counters, s.hsp_off, s.hsps_as_array()), "range query %d" % i)
+    b.close()
+
+
+def test_bad_subject_range_rejected(engine, workload):
+    qs, db = workload
+    d = engine.database(db.residues, db.offsets)
+    h = engine.query(qs[0])
+    for first, count in ((-1, 5), (0, 12_001), (12_001, -1)):
+        with pytest.raises(BpError):
+            engine.search_batch(d, [h], first=first, count=count)
+
+
+def test_autotune_picks_a_measured_candidate(engine, workload, singles):
+    qs, db = workload
+    d = engine.database(db.residues, db.offsets)
+    hs = [engine.query(q) for q in qs]
+    best, trials = engine.autotune(d, hs, sample_subjects=3000, chunk_sizes=[1 << 14, 1 << 18], warp_caps=[0, 8],
+                                   schedules=(SCHED_DYNAMIC, SCHED_STATIC), reps=1)
+    assert len(trials) == 8
+    fastest = min(trials, key=lambda t: t["ms"])
+    assert (best["chunk_residues"], best["schedule"], best["max_warps"]) == (
+        fastest["chunk_residues"], fastest["schedule"], fastest["max_warps"])
+    b = engine.search_batch(d, hs, **best)
+    _check(b, singles, "autotuned")
+    b.close()

@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 from blastp_b200 import Mlp, costmodel, synth
-from blastp_b200._lib import SCHED_COSTS, SCHED_STATIC
+from blastp_b200._lib import SCHED_COSTS, SCHED_DYNAMIC, SCHED_STATIC
 from helpers import assert_same
 from mlp_ref import forward, loss_grad
 
@@ -118,3 +118,19 @@ def test_learned_schedule_beats_static(engine, matrix):
         for i, s in enumerate(singles):
             assert_same(b.fetch(i), (s.counters, s.hsp_off, s.hsps_as_array()), "schedule query %d" % i)
         b.close()
+
+
+def test_library_costs_match_python_costs(engine, matrix):
+    model = costmodel.CostModel.load(engine)
+    rng = np.random.default_rng(12)
+    qs = [synth.residues(rng, int(n)) for n in (50, 700)]
+    db = synth.make_database(rng, 2000, qs, 0.01, (60, 150), (0.3, 0.5), matrix)
+    d = engine.database(db.residues, db.offsets)
+    hq = [engine.query(q) for q in qs]
+    first = engine.plan_chunks(d, 1 << 16)
+    lib_costs = engine.predict_costs(model, d, hq, first, 0.01)
+    py_costs = model.item_costs(engine.batch_features(d, hq, first, 0.01))
+    assert np.allclose(lib_costs, py_costs, rtol=1e-4)
+    best, trials = engine.autotune(d, hq, model=model, planted_density=0.01, sample_subjects=1000,
+                                   chunk_sizes=[1 << 15], warp_caps=[0], reps=1)
+    assert sorted(t["schedule"] for t in trials) == [SCHED_DYNAMIC, SCHED_STATIC, SCHED_COSTS]
