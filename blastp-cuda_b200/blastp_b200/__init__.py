@@ -6,5 +6,6 @@ synthetic-data generators used by the benchmark and the tests.
 """
 from . import synth  # noqa: F401
 from ._lib import BpError, BpParams, lib  # noqa: F401
-from .api import HSP_DTYPE, Batch, Database, Engine, Mlp, PendingResult, Query, Result, blosum62, default_params  # noqa: F401
+from .api import (HSP_DTYPE, Batch, Database, Engine, Mlp, PendingResult, Query, Result, Server,  # noqa: F401
+                  blosum62, default_params)
 from . import costmodel  # noqa: F401,E402

@@ -40,6 +40,20 @@ class BpAutotuneOptions(ctypes.Structure):
                 ("planted_density", ctypes.c_float), ("sample_subjects", i32), ("reps", i32)]
 
 
+class BpServerOptions(ctypes.Structure):
+    _fields_ = [("max_batch_queries", i32), ("device_memory_budget", i64), ("chunk_residues", i32),
+                ("schedule", i32), ("lanes", i32), ("poll_us", i32), ("model", P),
+                ("cost_weights", ctypes.c_float * 3), ("planted_density", ctypes.c_float), ("params", BpParams)]
+
+
+class BpServerMetrics(ctypes.Structure):
+    _fields_ = [("completed", i64), ("failed", i64), ("batches", i64), ("pending", i64), ("mean_batch", ctypes.c_double),
+                ("max_in_flight", i32), ("mem_used", i64), ("mem_peak", i64), ("p50_ms", ctypes.c_double),
+                ("p99_ms", ctypes.c_double), ("max_ms", ctypes.c_double), ("queries_per_s", ctypes.c_double),
+                ("resq_per_s", ctypes.c_double)]
+
+
+REQ_STATES = {-1: "unknown", 0: "queued", 1: "admitted", 2: "running", 3: "done", 4: "failed"}
 SCHED_DYNAMIC, SCHED_STATIC, SCHED_COSTS = 0, 1, 2
 SCHED_NAMES = {0: "dynamic", 1: "static", 2: "learned"}
 COST_FEATURES = 24
@@ -104,6 +118,15 @@ SIGNATURES = {
     "bp_batch_predict_costs": (ctypes.c_int, [P, P, P, P, P, i32, P, i32, ctypes.c_float, P]),
     "bp_autotune_options_default": (None, [P]),
     "bp_batch_autotune": (ctypes.c_int, [P, P, P, i32, P, P, P, i32, P]),
+    "bp_server_options_default": (None, [P]),
+    "bp_server_create": (ctypes.c_int, [P, P, P, P]),
+    "bp_server_submit": (ctypes.c_int, [P, P, i32, P]),
+    "bp_server_state": (i32, [P, u64]),
+    "bp_server_wait": (ctypes.c_int, [P, u64, i32]),
+    "bp_server_result": (ctypes.c_int, [P, u64, P, P, P, P, P]),
+    "bp_server_release": (ctypes.c_int, [P, u64]),
+    "bp_server_stats": (ctypes.c_int, [P, P]),
+    "bp_server_destroy": (None, [P]),
     # reference-compatible entry points
     "GPU_BLASTP": (None, [P] * 7 + [ctypes.c_int, P, P, i32, P, i32] + [P] * 7),
     "GPU_BLASTP_get_data": (None, [P, P, i32, P, P, i32, i32]),

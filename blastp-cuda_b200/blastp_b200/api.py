@@ -9,7 +9,8 @@ import ctypes
 import numpy as np
 
 from . import _lib
-from ._lib import COST_FEATURES, BpAutotuneOptions, BpAutotuneTrial, BpBatchOptions, BpParams, check, lib
+from ._lib import (COST_FEATURES, BpAutotuneOptions, BpAutotuneTrial, BpBatchOptions, BpParams, BpServerMetrics,
+                   BpServerOptions, check, lib)
 
 HSP_DTYPE = np.dtype([("hsp_q", "<i4"), ("hsp_s", "<i4"), ("query_offset", "<i4"),
                       ("subject_offset", "<i4"), ("hsp_len", "<i4"), ("score", "<i4")])
@@ -415,6 +416,85 @@ class Mlp:
     def close(self):
         if self.h:
             lib().bp_mlp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous-batching request loop over a resident database
+    (bp_server_*): submit() from any thread, results per ticket."""
+
+    def __init__(self, engine: Engine, db: Database, max_batch_queries: int = 32, memory_budget: int = 16 << 30,
+                 chunk_residues: int = 1 << 20, schedule: int = 0, lanes: int = 2, model=None,
+                 planted_density: float = 0.0, params: BpParams | None = None, poll_us: int = 200):
+        o = BpServerOptions()
+        lib().bp_server_options_default(ctypes.byref(o))
+        o.max_batch_queries = max_batch_queries
+        o.device_memory_budget = memory_budget
+        o.chunk_residues = chunk_residues
+        o.schedule = schedule
+        o.lanes = lanes
+        o.poll_us = poll_us
+        if model is not None:
+            o.model = model.mlp.h.value
+            for i in range(3):
+                o.cost_weights[i] = float(model.weights[i])
+        o.planted_density = planted_density
+        if params is not None:
+            o.params = params
+        h = ctypes.c_void_p()
+        check(lib().bp_server_create(engine.h, db.h, ctypes.byref(o), ctypes.byref(h)), engine.h)
+        self.h = h
+        self.engine = engine
+        self._keep = (db, model)
+        self.n_subjects = db.n_subjects
+
+    def submit(self, query) -> int:
+        q = np.ascontiguousarray(query, dtype=np.uint8)
+        t = ctypes.c_uint64(0)
+        check(lib().bp_server_submit(self.h, _p(q), len(q), ctypes.byref(t)))
+        return int(t.value)
+
+    def state(self, ticket: int) -> int:
+        return int(lib().bp_server_state(self.h, ticket))
+
+    def wait(self, ticket: int, timeout_ms: int = -1):
+        check(lib().bp_server_wait(self.h, ticket, timeout_ms))
+
+    def result(self, ticket: int):
+        """(Result, latency in ms) of a finished request."""
+        nh = ctypes.c_int64(0)
+        lat = ctypes.c_double(0)
+        check(lib().bp_server_result(self.h, ticket, None, None, None, ctypes.byref(nh), ctypes.byref(lat)))
+        n = self.n_subjects
+        counters = np.zeros((n, 3), dtype=np.int32)
+        hoff = np.zeros(n + 1, dtype=np.int64)
+        hsps = np.zeros(max(nh.value, 1), dtype=HSP_DTYPE)
+        check(lib().bp_server_result(self.h, ticket, _p(counters), _p(hoff), _p(hsps), ctypes.byref(nh), None))
+        return Result(counters, hoff, hsps[:nh.value]), float(lat.value)
+
+    def latency(self, ticket: int) -> float:
+        """Arrival-to-completion time (ms) of a finished request."""
+        lat = ctypes.c_double(0)
+        check(lib().bp_server_result(self.h, ticket, None, None, None, None, ctypes.byref(lat)))
+        return float(lat.value)
+
+    def release(self, ticket: int):
+        check(lib().bp_server_release(self.h, ticket))
+
+    def stats(self) -> dict:
+        m = BpServerMetrics()
+        check(lib().bp_server_stats(self.h, ctypes.byref(m)))
+        return {k: getattr(m, k) for k, _ in BpServerMetrics._fields_}
+
+    def close(self):
+        if self.h:
+            lib().bp_server_destroy(self.h)
             self.h = None
 
     def __del__(self):

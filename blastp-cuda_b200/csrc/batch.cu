@@ -81,9 +81,11 @@ struct bp_batch {
 
 namespace {
 
+constexpr int32_t kBaseChunk = 1 << 16;   // the cost model's chunk (residues)
+
 // Chunk boundaries over subjects [s0, s1): each chunk holds at least one
 // subject, then as many more as keep it within chunk_residues residues.
-void plan_chunks(const bp_db* db, int32_t s0, int32_t s1, int32_t chunk_residues, std::vector<int32_t>& first) {
+void plan_direct(const bp_db* db, int32_t s0, int32_t s1, int32_t chunk_residues, std::vector<int32_t>& first) {
     first.clear();
     first.push_back(s0);
     const int64_t* off = db->h_off.data();
@@ -96,6 +98,22 @@ void plan_chunks(const bp_db* db, int32_t s0, int32_t s1, int32_t chunk_residues
         first.push_back(t);
         s = t;
     }
+}
+
+// Chunks of at least two base chunks are unions of consecutive base chunks
+// (64Ki residues, the cost model's unit), so an item's predicted cost is the
+// sum of its base chunks' predictions.
+void plan_chunks(const bp_db* db, int32_t s0, int32_t s1, int32_t chunk_residues, std::vector<int32_t>& first) {
+    if (chunk_residues < 2 * kBaseChunk) {
+        plan_direct(db, s0, s1, chunk_residues, first);
+        return;
+    }
+    std::vector<int32_t> base;
+    plan_direct(db, s0, s1, kBaseChunk, base);
+    const size_t k = (size_t)chunk_residues / kBaseChunk;
+    first.clear();
+    for (size_t i = 0; i + 1 < base.size(); i += k) first.push_back(base[i]);
+    first.push_back(base.back());
 }
 
 bool resolve_range(const bp_db* db, int32_t first, int32_t count, int32_t* s0, int32_t* s1) {
@@ -161,7 +179,7 @@ bp_status enqueue(bp_batch* b) {
 bp_status prepare(bp_batch* b) {
     bp_engine* e = b->e;
     if (!b->d_counts) {
-        CKB(cudaMalloc((void**)&b->d_counts, (4 + b->classes.size()) * sizeof(uint32_t)), "cudaMalloc(counts)");
+        CKB(cudaMallocAsync((void**)&b->d_counts, (4 + b->classes.size()) * sizeof(uint32_t), e->stream), "cudaMalloc(counts)");
         CKB(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming), "cudaEventCreate");
         for (size_t c = 1; c < b->classes.size(); ++c) {
             cudaStream_t st = nullptr;
@@ -171,25 +189,26 @@ bp_status prepare(bp_batch* b) {
             CKB(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreate");
             b->ev_join.push_back(ev);
         }
-        CKB(cudaMalloc((void**)&b->d_fill, (size_t)std::max<int64_t>(b->nseg, 1) * sizeof(int32_t)), "cudaMalloc(fill)");
-        CKB(cudaMalloc((void**)&b->d_blocksums,
-                       (size_t)std::max(bp_order_blocksums_needed((int32_t)b->nseg), 1) * sizeof(int64_t)),
+        CKB(cudaMallocAsync((void**)&b->d_fill, (size_t)std::max<int64_t>(b->nseg, 1) * sizeof(int32_t), e->stream), "cudaMalloc(fill)");
+        CKB(cudaMallocAsync((void**)&b->d_blocksums,
+                            (size_t)std::max(bp_order_blocksums_needed((int32_t)b->nseg), 1) * sizeof(int64_t),
+                            e->stream),
             "cudaMalloc(sums)");
         CKB(cudaEventCreate(&b->ev0), "cudaEventCreate");
         CKB(cudaEventCreate(&b->ev1), "cudaEventCreate");
     }
     if (b->alloc_cap < b->cap || !b->d_hsps) {
-        cudaFree(b->d_recs);
-        cudaFree(b->d_hsps);
-        cudaFree(b->d_keys);
+        if (b->d_recs) cudaFreeAsync(b->d_recs, e->stream);
+        if (b->d_hsps) cudaFreeAsync(b->d_hsps, e->stream);
+        if (b->d_keys) cudaFreeAsync(b->d_keys, e->stream);
         b->d_recs = nullptr;
         b->d_hsps = nullptr;
         b->d_keys = nullptr;
         b->alloc_cap = 0;
         const size_t n = std::max<uint32_t>(b->cap, 1);
-        CKB(cudaMalloc((void**)&b->d_recs, n * sizeof(HspRec)), "cudaMalloc(records)");
-        CKB(cudaMalloc((void**)&b->d_hsps, n * sizeof(bp_hsp)), "cudaMalloc(hsps)");
-        CKB(cudaMalloc((void**)&b->d_keys, n * sizeof(int32_t)), "cudaMalloc(keys)");
+        CKB(cudaMallocAsync((void**)&b->d_recs, n * sizeof(HspRec), e->stream), "cudaMalloc(records)");
+        CKB(cudaMallocAsync((void**)&b->d_hsps, n * sizeof(bp_hsp), e->stream), "cudaMalloc(hsps)");
+        CKB(cudaMallocAsync((void**)&b->d_keys, n * sizeof(int32_t), e->stream), "cudaMalloc(keys)");
         b->alloc_cap = b->cap;
     }
     return BP_OK;
@@ -393,24 +412,29 @@ bp_status bp_search_batch(bp_engine* e, const bp_db* db, const bp_query* const* 
     }
     b->item_queue.resize(item_pos.size());
     for (size_t i = 0; i < item_pos.size(); ++i) b->item_queue[i] = local_queue[(size_t)item_pos[i]];
-    // record capacity: 1 % of the expected word hits (extensions run on ~5 %
-    // of hits on background composition, fewer succeed); grown and re-run on
-    // overflow, then kept for later runs
-    b->cap = (uint32_t)std::min<double>(1 << 26, std::max(65536.0, 0.01 * hits_sum * (double)db->nres));
-    cudaError_t err = cudaMalloc((void**)&b->d_queries, std::max<size_t>(1, hq.size()) * sizeof(BatchQuery));
-    if (err == cudaSuccess) err = cudaMalloc((void**)&b->d_items, std::max<size_t>(1, items.size()) * sizeof(WorkItem));
-    if (err == cudaSuccess) err = cudaMalloc((void**)&b->d_queue_off, qoff.size() * sizeof(int32_t));
-    if (err == cudaSuccess) err = cudaMalloc((void**)&b->d_queue_items, std::max<size_t>(1, qitems.size()) * sizeof(int32_t));
-    if (err == cudaSuccess) err = cudaMalloc((void**)&b->d_counters, (size_t)std::max<int64_t>(b->nseg, 1) * 3 * sizeof(int32_t));
-    if (err == cudaSuccess) err = cudaMalloc((void**)&b->d_hsp_off, ((size_t)b->nseg + 1) * sizeof(int64_t));
+    // record capacity: 2.5e-4 HSPs per expected word hit (about 1e-4 are
+    // reported on background sequence with homologs planted at 0.2-0.5 %);
+    // grown and re-run on overflow, then kept for later runs
+    const double span_res = (double)(db->h_off[s1] - db->h_off[s0]);
+    b->cap = (uint32_t)std::min<double>(1 << 28, std::max(65536.0, 2.5e-4 * hits_sum * span_res));
+    cudaStream_t es = e->stream;
+    cudaError_t err = cudaMallocAsync((void**)&b->d_queries, std::max<size_t>(1, hq.size()) * sizeof(BatchQuery), es);
+    if (err == cudaSuccess) err = cudaMallocAsync((void**)&b->d_items, std::max<size_t>(1, items.size()) * sizeof(WorkItem), es);
+    if (err == cudaSuccess) err = cudaMallocAsync((void**)&b->d_queue_off, qoff.size() * sizeof(int32_t), es);
+    if (err == cudaSuccess) err = cudaMallocAsync((void**)&b->d_queue_items, std::max<size_t>(1, qitems.size()) * sizeof(int32_t), es);
+    if (err == cudaSuccess) err = cudaMallocAsync((void**)&b->d_counters, (size_t)std::max<int64_t>(b->nseg, 1) * 3 * sizeof(int32_t), es);
+    if (err == cudaSuccess) err = cudaMallocAsync((void**)&b->d_hsp_off, ((size_t)b->nseg + 1) * sizeof(int64_t), es);
     if (err == cudaSuccess && !(b->h_count = bp_pinned_get(e))) err = cudaErrorMemoryAllocation;
+    // the host tables are pageable: copy synchronously with respect to the host
+    // (cudaMemcpyAsync from pageable memory returns once staged)
     if (err == cudaSuccess && !hq.empty())
-        err = cudaMemcpy(b->d_queries, hq.data(), hq.size() * sizeof(BatchQuery), cudaMemcpyHostToDevice);
+        err = cudaMemcpyAsync(b->d_queries, hq.data(), hq.size() * sizeof(BatchQuery), cudaMemcpyHostToDevice, es);
     if (err == cudaSuccess && !items.empty())
-        err = cudaMemcpy(b->d_items, items.data(), items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice);
-    if (err == cudaSuccess) err = cudaMemcpy(b->d_queue_off, qoff.data(), qoff.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+        err = cudaMemcpyAsync(b->d_items, items.data(), items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice, es);
+    if (err == cudaSuccess)
+        err = cudaMemcpyAsync(b->d_queue_off, qoff.data(), qoff.size() * sizeof(int32_t), cudaMemcpyHostToDevice, es);
     if (err == cudaSuccess && !qitems.empty())
-        err = cudaMemcpy(b->d_queue_items, qitems.data(), qitems.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+        err = cudaMemcpyAsync(b->d_queue_items, qitems.data(), qitems.size() * sizeof(int32_t), cudaMemcpyHostToDevice, es);
     if (err != cudaSuccess) {
         bp_batch_destroy(b);
         return bp_set_cuda_error(e, err, "bp_search_batch: allocate");
@@ -502,29 +526,27 @@ bp_status bp_batch_item_queues(const bp_batch* b, int32_t* queue_of_item) {
 
 void bp_batch_destroy(bp_batch* b) {
     if (!b) return;
-    if (b->e) cudaStreamSynchronize(b->e->stream);
+    bp_engine* e = b->e;
+    if (e) {
+        cudaSetDevice(e->device);
+        cudaStreamSynchronize(e->stream);
+    }
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
-    cudaFree(b->d_queries);
-    cudaFree(b->d_items);
-    cudaFree(b->d_queue_off);
-    cudaFree(b->d_queue_items);
-    cudaFree(b->d_counters);
-    cudaFree(b->d_hsp_off);
-    cudaFree(b->d_hsps);
-    cudaFree(b->d_keys);
-    cudaFree(b->d_recs);
-    cudaFree(b->d_fill);
-    cudaFree(b->d_blocksums);
-    cudaFree(b->d_counts);
+    for (void* p : {(void*)b->d_queries, (void*)b->d_items, (void*)b->d_queue_off, (void*)b->d_queue_items,
+                    (void*)b->d_counters, (void*)b->d_hsp_off, (void*)b->d_hsps, (void*)b->d_keys, (void*)b->d_recs,
+                    (void*)b->d_fill, (void*)b->d_blocksums, (void*)b->d_counts})
+        if (p && e) cudaFreeAsync(p, e->stream);
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
     if (b->ev_fork) cudaEventDestroy(b->ev_fork);
     for (cudaEvent_t ev : b->ev_join) cudaEventDestroy(ev);
     for (cudaStream_t st : b->side) cudaStreamDestroy(st);
-    if (b->e) bp_pinned_put(b->e, b->h_count);
+    if (e) bp_pinned_put(e, b->h_count);
+    cudaGetLastError();
     delete b;
 }
+
 
 }  // extern "C"
 
@@ -537,18 +559,33 @@ bp_status bp_batch_predict_costs(bp_engine* e, bp_mlp* model, const float* weigh
                                  int32_t n_chunks, float planted_density, float* costs) {
     if (!e || !model || !weights || !db || !chunk_first || !costs || n_queries < 0 || n_chunks < 0)
         return BP_ERR_INVALID;
-    const size_t n = (size_t)n_queries * n_chunks;
-    if (n == 0) return BP_OK;
+    if ((size_t)n_queries * n_chunks == 0) return BP_OK;
+    // predict on base chunks when the chunks are unions of them, else directly
+    std::vector<int32_t> base;
+    plan_direct(db, chunk_first[0], chunk_first[n_chunks], kBaseChunk, base);
+    std::vector<int32_t> owner(base.size() - 1);
+    bool aligned = true;
+    for (size_t i = 0, c = 0; i + 1 < base.size(); ++i) {
+        while (c < (size_t)n_chunks && chunk_first[c + 1] <= base[i]) ++c;
+        if (c >= (size_t)n_chunks || base[i + 1] > chunk_first[c + 1]) { aligned = false; break; }
+        owner[i] = (int32_t)c;
+    }
+    const int32_t* f = aligned ? base.data() : chunk_first;
+    const int32_t nf = aligned ? (int32_t)base.size() - 1 : n_chunks;
+    const size_t n = (size_t)n_queries * nf;
     std::vector<float> X(n * BP_COST_FEATURES), Y(n * 2);
-    bp_status st = bp_batch_features(e, db, queries, n_queries, chunk_first, n_chunks, planted_density, X.data());
+    bp_status st = bp_batch_features(e, db, queries, n_queries, f, nf, planted_density, X.data());
     if (st == BP_OK) st = bp_mlp_predict(model, X.data(), (int32_t)n, Y.data());
     if (st != BP_OK) return st;
+    std::vector<double> acc((size_t)n_queries * n_chunks, 0.0);
     for (size_t i = 0; i < n; ++i) {
         const double res = expm1((double)X[i * BP_COST_FEATURES + 2]);
         const double hits = expm1(std::max(0.0, (double)Y[2 * i]));
         const double ext = expm1(std::max(0.0, (double)Y[2 * i + 1]));
-        costs[i] = (float)(weights[0] * res + weights[1] * hits + weights[2] * ext);
+        const size_t q = i / nf, c = i % nf;
+        acc[q * n_chunks + (aligned ? owner[c] : c)] += weights[0] * res + weights[1] * hits + weights[2] * ext;
     }
+    for (size_t i = 0; i < acc.size(); ++i) costs[i] = (float)acc[i];
     return BP_OK;
 }
 

@@ -400,10 +400,12 @@ bp_status bp_query_create(bp_engine* e, const uint8_t* residues, int32_t length,
     uint32_t* d_tmp = nullptr;
     do {
         cudaError_t err;
-        if ((err = cudaMalloc((void**)&q->d_q, (size_t)((length + 15) & ~15) + 16)) != cudaSuccess ||
-            (err = cudaMalloc((void**)&q->d_cells, (BP_NC + 1) * sizeof(uint32_t))) != cudaSuccess ||
-            (err = cudaMalloc((void**)&q->d_ctx, 3 * sizeof(int32_t))) != cudaSuccess ||
-            (err = cudaMalloc((void**)&d_tmp, BP_NC * sizeof(uint32_t))) != cudaSuccess) {
+        // stream-ordered allocations: no device-wide synchronisation, so a
+        // query can be built while searches run on other streams
+        if ((err = cudaMallocAsync((void**)&q->d_q, (size_t)((length + 15) & ~15) + 16, e->stream)) != cudaSuccess ||
+            (err = cudaMallocAsync((void**)&q->d_cells, (BP_NC + 1) * sizeof(uint32_t), e->stream)) != cudaSuccess ||
+            (err = cudaMallocAsync((void**)&q->d_ctx, 3 * sizeof(int32_t), e->stream)) != cudaSuccess ||
+            (err = cudaMallocAsync((void**)&d_tmp, BP_NC * sizeof(uint32_t), e->stream)) != cudaSuccess) {
             st = bp_set_cuda_error(e, err, "cudaMalloc(query)"); break;
         }
         if (length > 0 &&
@@ -424,15 +426,15 @@ bp_status bp_query_create(bp_engine* e, const uint8_t* residues, int32_t length,
         const uint32_t total = cells[BP_NC];
         q->n_entries = total;
         q->hits_per_residue = bp_expected_hits_per_residue(cells.data());
-        if ((err = cudaMalloc((void**)&q->d_entries, (size_t)std::max<uint32_t>(total, 1) * sizeof(uint16_t))) !=
-                cudaSuccess ||
+        if ((err = cudaMallocAsync((void**)&q->d_entries, (size_t)std::max<uint32_t>(total, 1) * sizeof(uint16_t),
+                                   e->stream)) != cudaSuccess ||
             (err = bp_launch_table_build(e, q->d_q, length, p->threshold, q->d_cells, q->d_entries, d_tmp, 1)) !=
                 cudaSuccess ||
             (err = cudaStreamSynchronize(e->stream)) != cudaSuccess) {
             st = bp_set_cuda_error(e, err, "table fill"); break;
         }
     } while (0);
-    cudaFree(d_tmp);
+    if (d_tmp) cudaFreeAsync(d_tmp, e->stream);
     if (st != BP_OK) {
         bp_query_destroy(q);
         return st;
@@ -443,10 +445,10 @@ bp_status bp_query_create(bp_engine* e, const uint8_t* residues, int32_t length,
 
 void bp_query_destroy(bp_query* q) {
     if (!q) return;
-    cudaFree(q->d_q);
-    cudaFree(q->d_cells);
-    cudaFree(q->d_entries);
-    cudaFree(q->d_ctx);
+    cudaSetDevice(q->e->device);
+    for (void* p : {(void*)q->d_q, (void*)q->d_cells, (void*)q->d_entries, (void*)q->d_ctx})
+        if (p) cudaFreeAsync(p, q->e->stream);
+    cudaGetLastError();
     delete q;
 }
 

@@ -1,0 +1,430 @@
+// Serving loop: continuous batching of arriving queries against one resident
+// database.
+//
+// The reference answers one blastp call at a time (gpu_blastp.cu:16-259); a
+// server keeps the database on the device and takes queries as they come:
+//  * submit() queues a request (any thread);
+//  * a dispatcher thread admits queued requests in arrival order while the
+//    device-memory budget allows (the request's neighbour table, its
+//    per-subject outputs and its share of the HSP record buffer), builds
+//    their tables and launches them as one batched persistent search on a
+//    free lane -- each lane has its own stream and engine scratch, and each
+//    lane's launch takes 1/lanes of the SMs, so a batch that starts while
+//    another is running overlaps it on the device;
+//  * finished batches are noticed by polling their streams; results stay on
+//    the device, in the batch's per-query segments, until the request is
+//    released, which is when its memory returns to the budget.
+// Every query's result is its single-query result (the batched kernel scans
+// each (query, subject) pair exactly as the plain kernel does).
+#include <string.h>
+
+#include <algorithm>
+#include <cmath>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "bp_internal.h"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+double now_ms() {
+    return std::chrono::duration<double, std::milli>(Clock::now().time_since_epoch()).count();
+}
+
+struct Job;
+
+struct Req {
+    uint64_t id = 0;
+    std::vector<uint8_t> residues;
+    double t_arrive = 0, t_start = 0, t_done = 0;
+    int state = BP_REQ_QUEUED;
+    bp_status status = BP_OK;
+    int64_t bytes = 0;
+    bp_query* query = nullptr;
+    Job* job = nullptr;
+    int index = -1;
+    bool released = false;
+};
+
+struct Job {
+    int lane = 0;
+    bp_batch* batch = nullptr;
+    std::vector<Req*> reqs;
+    int live = 0;             // requests not yet released
+    int64_t bytes = 0;
+    bool done = false;
+};
+
+}  // namespace
+
+struct bp_server {
+    bp_engine* e = nullptr;
+    const bp_db* db = nullptr;
+    bp_server_options o{};
+    std::vector<bp_engine*> lanes;
+    std::vector<Job*> lane_job;
+    std::thread th;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<Req*> pending;
+    std::unordered_map<uint64_t, Req*> reqs;
+    uint64_t next_id = 1;
+    int64_t mem_used = 0, mem_peak = 0;
+    bool stop = false;
+    // statistics
+    std::vector<double> latency_ms;
+    int64_t n_done = 0, n_failed = 0, n_batches = 0, batched_queries = 0;
+    double t_first = -1, t_last = 0, resq = 0;
+    int max_in_flight = 0, in_flight = 0;
+};
+
+namespace {
+
+// Device bytes a request holds while admitted: its table (cell starts +
+// entries, estimated from the query length), its per-subject outputs
+// (counters, CSR offsets, fill cursor) and its expected HSP records.
+int64_t request_bytes(const bp_server* s, int32_t qlen) {
+    const int64_t n = s->db->n;
+    const int64_t table = (BP_NC + 1) * 4 + (int64_t)qlen * 40 + 4096;
+    const int64_t outputs = n * (12 + 8 + 4) + 8;
+    const int64_t records = (int64_t)(3e-4 * 1.5 * (double)qlen / 500.0 * (double)s->db->nres) * 60;
+    return table + outputs + records;
+}
+
+void fail_request(bp_server* s, Req* r, bp_status st) {
+    r->state = BP_REQ_FAILED;
+    r->status = st;
+    r->t_done = now_ms();
+    s->n_failed += 1;
+}
+
+// Builds tables and launches one batch on `lane` (called without the lock;
+// the requests are already marked admitted and owned by the dispatcher).
+void launch_job(bp_server* s, Job* job) {
+    bp_engine* le = s->lanes[job->lane];
+    std::vector<const bp_query*> qs;
+    bp_status st = BP_OK;
+    for (Req* r : job->reqs) {
+        st = bp_query_create(le, r->residues.data(), (int32_t)r->residues.size(), &s->o.params, &r->query);
+        if (st != BP_OK) break;
+        qs.push_back(r->query);
+    }
+    bp_batch_options bo;
+    bp_batch_options_default(&bo);
+    bo.chunk_residues = s->o.chunk_residues > 0 ? s->o.chunk_residues : (1 << 20);
+    bo.schedule = s->o.schedule;
+    bo.use_graph = 0;
+    bo.ctas = std::max(1, le->sm_count / std::max(1, (int)s->lanes.size()));
+    std::vector<float> costs;
+    if (st == BP_OK && bo.schedule == BP_SCHED_COSTS) {
+        if (!s->o.model) {
+            bo.schedule = BP_SCHED_STATIC;   // no model: the static schedule
+        } else {
+            int32_t nc = 0;
+            st = bp_batch_plan(s->db, 0, -1, bo.chunk_residues, nullptr, &nc);
+            std::vector<int32_t> first((size_t)nc + 1);
+            if (st == BP_OK) st = bp_batch_plan(s->db, 0, -1, bo.chunk_residues, first.data(), &nc);
+            costs.resize((size_t)qs.size() * nc);
+            if (st == BP_OK)
+                st = bp_batch_predict_costs(le, s->o.model, s->o.cost_weights, s->db, qs.data(), (int32_t)qs.size(),
+                                            first.data(), nc, s->o.planted_density, costs.data());
+            bo.item_costs = costs.data();
+        }
+    }
+    if (st == BP_OK) st = bp_search_batch(le, s->db, qs.data(), (int32_t)qs.size(), &bo, &job->batch);
+    std::lock_guard<std::mutex> lock(s->mu);
+    const double t = now_ms();
+    for (size_t i = 0; i < job->reqs.size(); ++i) {
+        Req* r = job->reqs[i];
+        r->index = (int)i;
+        if (st == BP_OK) {
+            r->state = BP_REQ_RUNNING;
+            r->t_start = t;
+        } else {
+            fail_request(s, r, st);
+        }
+    }
+    if (st != BP_OK) {
+        job->done = true;
+        s->cv_done.notify_all();
+    }
+}
+
+// Frees a job whose requests have all been released.
+void retire_job(bp_server* s, Job* job) {
+    bp_batch_destroy(job->batch);
+    for (Req* r : job->reqs) {
+        bp_query_destroy(r->query);
+        r->query = nullptr;
+        s->reqs.erase(r->id);
+        delete r;
+    }
+    s->mem_used -= job->bytes;
+    delete job;
+}
+
+void dispatcher(bp_server* s) {
+    std::unique_lock<std::mutex> lock(s->mu);
+    while (!s->stop) {
+        bool worked = false;
+        // completions
+        for (size_t l = 0; l < s->lanes.size(); ++l) {
+            Job* job = s->lane_job[l];
+            if (!job) continue;
+            if (!job->done) {
+                if (cudaStreamQuery(s->lanes[l]->stream) == cudaErrorNotReady) continue;
+                cudaGetLastError();
+                lock.unlock();
+                const bp_status st = bp_batch_wait(job->batch);   // re-runs on record overflow
+                lock.lock();
+                const double t = now_ms();
+                for (Req* r : job->reqs) {
+                    if (r->state != BP_REQ_RUNNING) continue;
+                    if (st != BP_OK) {
+                        fail_request(s, r, st);
+                        continue;
+                    }
+                    r->state = BP_REQ_DONE;
+                    r->t_done = t;
+                    s->latency_ms.push_back(r->t_done - r->t_arrive);
+                    s->n_done += 1;
+                    s->resq += (double)r->residues.size() * (double)s->db->nres;
+                    s->t_last = std::max(s->t_last, t);
+                }
+                s->in_flight -= (int)job->reqs.size();
+                job->done = true;
+                s->cv_done.notify_all();
+                worked = true;
+            }
+            s->lane_job[l] = nullptr;   // the lane is free; the job lives until released
+            if (job->live == 0) retire_job(s, job);
+        }
+        // admissions: one batch per free lane, in arrival order, within budget
+        for (size_t l = 0; l < s->lanes.size() && !s->pending.empty(); ++l) {
+            if (s->lane_job[l]) continue;
+            Job* job = new Job();
+            job->lane = (int)l;
+            while (!s->pending.empty() && (int)job->reqs.size() < s->o.max_batch_queries) {
+                Req* r = s->pending.front();
+                if (s->mem_used + job->bytes + r->bytes > s->o.device_memory_budget && !(job->reqs.empty() &&
+                                                                                          s->mem_used == 0))
+                    break;   // wait for memory (a lone request on an idle server always goes)
+                s->pending.pop_front();
+                r->state = BP_REQ_ADMITTED;
+                r->job = job;
+                job->reqs.push_back(r);
+                job->bytes += r->bytes;
+            }
+            if (job->reqs.empty()) {
+                delete job;
+                break;
+            }
+            job->live = (int)job->reqs.size();
+            s->mem_used += job->bytes;
+            s->mem_peak = std::max(s->mem_peak, s->mem_used);
+            s->lane_job[l] = job;
+            s->n_batches += 1;
+            s->batched_queries += (int64_t)job->reqs.size();
+            s->in_flight += (int)job->reqs.size();
+            s->max_in_flight = std::max(s->max_in_flight, s->in_flight);
+            lock.unlock();
+            launch_job(s, job);
+            lock.lock();
+            if (job->done) {                 // failed to launch
+                s->in_flight -= (int)job->reqs.size();
+                s->lane_job[l] = nullptr;
+            }
+            worked = true;
+        }
+        if (!worked) s->cv_work.wait_for(lock, std::chrono::microseconds(s->o.poll_us > 0 ? s->o.poll_us : 200));
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+void bp_server_options_default(bp_server_options* o) {
+    memset(o, 0, sizeof(*o));
+    o->max_batch_queries = 32;
+    o->device_memory_budget = (int64_t)16 << 30;
+    o->chunk_residues = 1 << 20;
+    o->schedule = BP_SCHED_DYNAMIC;
+    o->lanes = 2;
+    o->poll_us = 200;
+    bp_params_default(&o->params);
+}
+
+bp_status bp_server_create(bp_engine* e, const bp_db* db, const bp_server_options* opt, bp_server** out) {
+    if (!e || !db || !out) return bp_set_error(e, BP_ERR_INVALID, "bp_server_create: bad argument");
+    *out = nullptr;
+    bp_server* s = new bp_server();
+    s->e = e;
+    s->db = db;
+    if (opt) s->o = *opt;
+    else bp_server_options_default(&s->o);
+    if (s->o.lanes < 1 || s->o.lanes > 16 || s->o.max_batch_queries < 1) {
+        delete s;
+        return bp_set_error(e, BP_ERR_INVALID, "bp_server_create: lanes must be 1..16, max_batch_queries >= 1");
+    }
+    for (int l = 0; l < s->o.lanes; ++l) {
+        bp_engine* le = nullptr;
+        const bp_status st = bp_engine_create(e->device, &le);
+        if (st != BP_OK) {
+            bp_server_destroy(s);
+            return bp_set_error(e, st, "bp_server_create: lane engine");
+        }
+        s->lanes.push_back(le);
+        s->lane_job.push_back(nullptr);
+    }
+    s->th = std::thread(dispatcher, s);
+    *out = s;
+    return BP_OK;
+}
+
+bp_status bp_server_submit(bp_server* s, const uint8_t* query, int32_t length, uint64_t* ticket) {
+    if (!s || !ticket || length < 0 || (length > 0 && !query)) return BP_ERR_INVALID;
+    if (length > BP_MAX_QUERY_LENGTH) return BP_ERR_TOO_LARGE;
+    for (int32_t i = 0; i < length; ++i)
+        if (query[i] == 0 || query[i] >= BP_ALPHABET) return BP_ERR_INVALID;
+    Req* r = new Req();
+    r->residues.assign(query, query + length);
+    r->t_arrive = now_ms();
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        r->id = s->next_id++;
+        r->bytes = request_bytes(s, length);
+        if (s->t_first < 0) s->t_first = r->t_arrive;
+        s->reqs[r->id] = r;
+        s->pending.push_back(r);
+        *ticket = r->id;
+    }
+    s->cv_work.notify_one();
+    return BP_OK;
+}
+
+int32_t bp_server_state(bp_server* s, uint64_t ticket) {
+    if (!s) return BP_REQ_UNKNOWN;
+    std::lock_guard<std::mutex> lock(s->mu);
+    auto it = s->reqs.find(ticket);
+    return it == s->reqs.end() ? BP_REQ_UNKNOWN : it->second->state;
+}
+
+bp_status bp_server_wait(bp_server* s, uint64_t ticket, int32_t timeout_ms) {
+    if (!s) return BP_ERR_INVALID;
+    std::unique_lock<std::mutex> lock(s->mu);
+    auto it = s->reqs.find(ticket);
+    if (it == s->reqs.end()) return BP_ERR_INVALID;
+    Req* r = it->second;
+    const auto pred = [r] { return r->state == BP_REQ_DONE || r->state == BP_REQ_FAILED; };
+    if (timeout_ms < 0) s->cv_done.wait(lock, pred);
+    else if (!s->cv_done.wait_for(lock, std::chrono::milliseconds(timeout_ms), pred)) return BP_ERR_NOT_READY;
+    return r->state == BP_REQ_DONE ? BP_OK : r->status;
+}
+
+bp_status bp_server_result(bp_server* s, uint64_t ticket, int32_t* counters, int64_t* hsp_off, bp_hsp* hsps,
+                           int64_t* n_hsps, double* latency_ms) {
+    if (!s) return BP_ERR_INVALID;
+    Job* job = nullptr;
+    int index = -1;
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        auto it = s->reqs.find(ticket);
+        if (it == s->reqs.end()) return BP_ERR_INVALID;
+        Req* r = it->second;
+        if (r->state == BP_REQ_FAILED) return r->status;
+        if (r->state != BP_REQ_DONE) return BP_ERR_NOT_READY;
+        if (latency_ms) *latency_ms = r->t_done - r->t_arrive;
+        job = r->job;
+        index = r->index;
+    }
+    // the job cannot be retired before this request is released
+    return bp_batch_copy_query(job->batch, index, counters, hsp_off, hsps, n_hsps);
+}
+
+bp_status bp_server_release(bp_server* s, uint64_t ticket) {
+    if (!s) return BP_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(s->mu);
+    auto it = s->reqs.find(ticket);
+    if (it == s->reqs.end()) return BP_ERR_INVALID;
+    Req* r = it->second;
+    if (r->state != BP_REQ_DONE && r->state != BP_REQ_FAILED) return BP_ERR_NOT_READY;
+    if (r->released) return BP_ERR_INVALID;
+    r->released = true;
+    Job* job = r->job;
+    if (!job) {                                  // failed before admission
+        s->reqs.erase(it);
+        delete r;
+        return BP_OK;
+    }
+    job->live -= 1;
+    const bool on_lane = std::find(s->lane_job.begin(), s->lane_job.end(), job) != s->lane_job.end();
+    if (job->live == 0 && job->done && !on_lane) retire_job(s, job);
+    s->cv_work.notify_one();
+    return BP_OK;
+}
+
+bp_status bp_server_stats(bp_server* s, bp_server_metrics* out) {
+    if (!s || !out) return BP_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(s->mu);
+    memset(out, 0, sizeof(*out));
+    out->completed = s->n_done;
+    out->failed = s->n_failed;
+    out->batches = s->n_batches;
+    out->mean_batch = s->n_batches ? (double)s->batched_queries / (double)s->n_batches : 0.0;
+    out->pending = (int64_t)s->pending.size();
+    out->max_in_flight = s->max_in_flight;
+    out->mem_used = s->mem_used;
+    out->mem_peak = s->mem_peak;
+    if (!s->latency_ms.empty()) {
+        std::vector<double> v = s->latency_ms;
+        std::sort(v.begin(), v.end());
+        auto pct = [&v](double p) {
+            const size_t i = (size_t)std::min<double>((double)v.size() - 1, std::ceil(p * (double)v.size()) - 1);
+            return v[i];
+        };
+        out->p50_ms = pct(0.50);
+        out->p99_ms = pct(0.99);
+        out->max_ms = v.back();
+        const double span = (s->t_last - s->t_first) / 1e3;
+        out->queries_per_s = span > 0 ? (double)s->n_done / span : 0.0;
+        out->resq_per_s = span > 0 ? s->resq / span : 0.0;
+    }
+    return BP_OK;
+}
+
+void bp_server_destroy(bp_server* s) {
+    if (!s) return;
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        s->stop = true;
+    }
+    s->cv_work.notify_all();
+    if (s->th.joinable()) s->th.join();
+    // release everything still held
+    std::vector<Job*> jobs;
+    for (auto& kv : s->reqs)
+        if (kv.second->job && std::find(jobs.begin(), jobs.end(), kv.second->job) == jobs.end())
+            jobs.push_back(kv.second->job);
+    for (Job* j : jobs) {
+        bp_batch_destroy(j->batch);
+        for (Req* r : j->reqs) {
+            bp_query_destroy(r->query);
+            s->reqs.erase(r->id);
+            delete r;
+        }
+        delete j;
+    }
+    for (auto& kv : s->reqs) delete kv.second;
+    for (bp_engine* le : s->lanes) bp_engine_destroy(le);
+    delete s;
+}
+
+}  // extern "C"

@@ -247,6 +247,62 @@ bp_status bp_batch_autotune(bp_engine* e, const bp_db* db, const bp_query* const
                             const bp_autotune_options* opt, bp_batch_options* best, bp_autotune_trial* trials,
                             int32_t trials_cap, int32_t* n_trials);
 
+/* ---- serving ---------------------------------------------------------------
+ * Continuous batching against one resident database.  Requests are admitted
+ * in arrival order while the device-memory budget allows, and launched as
+ * batched searches on free lanes (each lane: its own stream and scratch, a
+ * 1/lanes share of the SMs), so a batch admitted while another runs
+ * overlaps it.  A request's results stay on the device until it is
+ * released.  No counterpart in the reference. */
+typedef struct bp_server bp_server;
+
+enum {
+    BP_REQ_UNKNOWN = -1,
+    BP_REQ_QUEUED = 0,
+    BP_REQ_ADMITTED = 1,
+    BP_REQ_RUNNING = 2,
+    BP_REQ_DONE = 3,
+    BP_REQ_FAILED = 4
+};
+
+typedef struct {
+    int32_t max_batch_queries;      /* queries per launch */
+    int64_t device_memory_budget;   /* bytes held by admitted requests */
+    int32_t chunk_residues;
+    int32_t schedule;               /* bp_schedule; BP_SCHED_COSTS uses model */
+    int32_t lanes;                  /* batches in flight at once (1..16) */
+    int32_t poll_us;                /* dispatcher poll interval */
+    bp_mlp* model;                  /* used by the server's thread only while it exists */
+    float cost_weights[3];
+    float planted_density;
+    bp_params params;
+} bp_server_options;
+
+typedef struct {
+    int64_t completed, failed, batches, pending;
+    double mean_batch;
+    int32_t max_in_flight;
+    int64_t mem_used, mem_peak;
+    double p50_ms, p99_ms, max_ms;  /* arrival to completion, completed requests */
+    double queries_per_s;           /* completed / (last completion - first arrival) */
+    double resq_per_s;              /* database residues x query residues per second */
+} bp_server_metrics;
+
+void bp_server_options_default(bp_server_options* o);
+bp_status bp_server_create(bp_engine* e, const bp_db* db, const bp_server_options* opt, bp_server** out);
+/* Queues a query (residue codes 1..27); any thread. */
+bp_status bp_server_submit(bp_server* s, const uint8_t* query, int32_t length, uint64_t* ticket);
+int32_t bp_server_state(bp_server* s, uint64_t ticket);
+/* Waits for the request (timeout_ms < 0: no limit); BP_ERR_NOT_READY on timeout. */
+bp_status bp_server_wait(bp_server* s, uint64_t ticket, int32_t timeout_ms);
+/* The finished request's results, in the bp_result_copy layout. */
+bp_status bp_server_result(bp_server* s, uint64_t ticket, int32_t* counters, int64_t* hsp_off, bp_hsp* hsps,
+                           int64_t* n_hsps, double* latency_ms);
+/* Gives the request's device memory back to the budget. */
+bp_status bp_server_release(bp_server* s, uint64_t ticket);
+bp_status bp_server_stats(bp_server* s, bp_server_metrics* out);
+void bp_server_destroy(bp_server* s);
+
 /* The plain search for callers that cannot allocate device memory: a process
  * that hands out a fixed device-memory budget at start-up, a latency-critical
  * path where cudaMalloc/cudaFree would synchronise the device, or code whose

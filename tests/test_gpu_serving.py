@@ -1,0 +1,94 @@
+"""GPU checks of the serving loop (bp_server_*): requests that arrive while
+others run are admitted and overlap on the device, and every request's result
+is bit-identical to the plain single-query search of the same query alone."""
+import numpy as np
+import pytest
+
+from blastp_b200 import BpError, Server, costmodel, serving, synth
+from blastp_b200._lib import SCHED_COSTS
+from helpers import assert_same
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def world(engine, matrix):
+    rng = np.random.default_rng(55)
+    qs = synth.serving_queries(rng, 24, median=250, hi=1500)
+    db = synth.make_database(rng, 15_000, qs[:6], 0.01, (60, 150), (0.3, 0.5), matrix)
+    d = engine.database(db.residues, db.offsets)
+    alone = []
+    for q in qs:
+        h = engine.query(q)
+        alone.append(engine.search(d, h).fetch())
+        h.close()
+    return qs, db, d, alone
+
+
+def _check(results, alone, what):
+    for i, (r, a) in enumerate(zip(results, alone)):
+        assert_same(r, (a.counters, a.hsp_off, a.hsps_as_array()), "%s request %d" % (what, i))
+
+
+def test_mix_equals_alone_and_overlaps(engine, world):
+    qs, db, d, alone = world
+    srv = Server(engine, d, max_batch_queries=4, lanes=2, chunk_residues=1 << 18)
+    arr = serving.poisson_arrivals(np.random.default_rng(1), 2000.0, len(qs))
+    results, lat, _ = serving.drive(srv, qs, arr)
+    _check(results, alone, "mix")
+    st = srv.stats()
+    assert st["completed"] == len(qs) and st["failed"] == 0
+    assert st["batches"] >= len(qs) // 4
+    assert st["max_in_flight"] > 4          # a second batch was admitted while the first ran
+    assert st["p99_ms"] >= st["p50_ms"] > 0
+    assert abs(serving.percentile(lat, 50) - st["p50_ms"]) < 1e-6
+    assert st["mem_used"] == 0
+    srv.close()
+
+
+def test_memory_budget_limits_admission(engine, world):
+    qs, db, d, alone = world
+    per_request = 15_000 * 24 + (19684 * 4) + 40 * 1500 + 4096 + int(3e-4 * 1.5 * 3 * db.n_residues) * 60
+    srv = Server(engine, d, max_batch_queries=8, lanes=2, memory_budget=2 * per_request)
+    results, _, _ = serving.drive(srv, qs[:10], np.zeros(10))
+    _check(results, alone[:10], "budget")
+    st = srv.stats()
+    assert st["max_in_flight"] <= 4          # without the budget: 16 (two lanes of 8)
+    assert st["mem_peak"] <= 2 * per_request
+    srv.close()
+
+
+def test_learned_schedule_in_server(engine, world):
+    qs, db, d, alone = world
+    model = costmodel.CostModel.load(engine)
+    srv = Server(engine, d, max_batch_queries=6, lanes=2, schedule=SCHED_COSTS, model=model, planted_density=0.01)
+    results, _, _ = serving.drive(srv, qs[:12], serving.poisson_arrivals(np.random.default_rng(2), 500.0, 12))
+    _check(results, alone[:12], "learned")
+    srv.close()
+
+
+def test_results_stay_until_released(engine, world):
+    qs, db, d, alone = world
+    srv = Server(engine, d, max_batch_queries=2, lanes=1)
+    t = [srv.submit(q) for q in qs[:3]]
+    for x in t:
+        srv.wait(x)
+    assert srv.stats()["mem_used"] > 0
+    r, _ = srv.result(t[1])
+    _check([r], [alone[1]], "held")
+    for x in t:
+        srv.release(x)
+    with pytest.raises(BpError):
+        srv.release(t[0])
+    assert srv.stats()["mem_used"] == 0
+    srv.close()
+
+
+def test_bad_requests_rejected(engine, world):
+    qs, db, d, alone = world
+    srv = Server(engine, d)
+    with pytest.raises(BpError):
+        srv.submit(np.array([1, 0, 3], np.uint8))
+    with pytest.raises(BpError):
+        srv.submit(np.ones(70_000, np.uint8))
+    srv.close()
