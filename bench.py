@@ -48,6 +48,10 @@ def parse():
     ap.add_argument("--batch-subjects", type=int, default=2_000_000)
     ap.add_argument("--batch-queries", type=int, default=256)
     ap.add_argument("--batch-reps", type=int, default=1)
+    ap.add_argument("--serve", type=int, default=1, help="also measure the serving loop (1 GPU runs only)")
+    ap.add_argument("--serve-subjects", type=int, default=5_000_000)
+    ap.add_argument("--serve-requests", type=int, default=128)
+    ap.add_argument("--serve-rate", type=float, default=1000.0, help="offered load, queries/s (Poisson)")
     return ap.parse_args()
 
 
@@ -247,8 +251,9 @@ def run_batched(eng, matrix, args, torch):
                     np.array_equal(r.hsps_as_array(), p.hsps_as_array())):
                 identical = False
         if name == "learned":
-            # count error of the model on this workload: items of the checked queries
-            first = eng.plan_chunks(db, kw["chunk_residues"])
+            # count error of the model on this workload, per (query, 64Ki-residue
+            # chunk) -- the model's unit -- for the checked queries
+            first = eng.plan_chunks(db, costmodel.TRAIN_CHUNK_RESIDUES)
             nc = len(first) - 1
             X = eng.batch_features(db, [qs[i] for i in check_q], first, planted)
             pred = model.predict_counts(X)
@@ -268,6 +273,54 @@ def run_batched(eng, matrix, args, torch):
         pass
     for q in qs:
         q.close()
+    db.close()
+    return out
+
+
+def run_serving(eng, matrix, args):
+    """Poisson arrivals of log-normal queries (median 350, sigma 0.7, 20-4000
+    aa) against a resident 5,000,000-subject database, served with continuous
+    batching and the learned schedule; p50/p99 latency and throughput at the
+    offered rate and at 80 % of the measured capacity."""
+    from blastp_b200 import Server, costmodel, serving, synth
+    from blastp_b200._lib import SCHED_COSTS
+    rng = np.random.default_rng(5000)
+    lengths = synth.lognormal_lengths(rng, args.serve_subjects, 300, 0.6, 30, 5000)
+    off = np.zeros(args.serve_subjects + 1, dtype=np.int64)
+    np.cumsum(lengths, out=off[1:])
+    res = synth.residues(rng, int(off[-1]))
+    db = eng.database(res, off)
+    nres = int(off[-1])
+    del res
+    model = costmodel.CostModel.load(eng)
+    out = {"workload": "serve_vs_5M", "subjects": args.serve_subjects, "residues": nres,
+           "schedule": "learned", "lanes": 2, "max_batch_queries": 32, "memory_budget_gb": 16}
+    runs = {}
+    capacity = None
+    for label, rate, n in (("offered", args.serve_rate, args.serve_requests),
+                           ("sustainable", None, max(16, args.serve_requests // 2))):
+        if rate is None:
+            rate = 0.8 * capacity
+        qs = synth.serving_queries(rng, n)
+        srv = Server(eng, db, max_batch_queries=32, lanes=2, schedule=SCHED_COSTS, model=model,
+                     chunk_residues=1 << 20)
+        arrivals = serving.poisson_arrivals(rng, rate, n)
+        t0 = time.perf_counter()
+        _, lat, late = serving.drive(srv, qs, arrivals, keep_results=False)
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+        srv.close()
+        qres = float(sum(len(q) for q in qs))
+        runs[label] = {"offered_qps": rate, "requests": n, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+                       "max_ms": st["max_ms"], "throughput_qps": st["queries_per_s"],
+                       "value": st["resq_per_s"], "unit": UNIT, "batches": st["batches"],
+                       "mean_batch": st["mean_batch"], "max_in_flight": st["max_in_flight"],
+                       "mem_peak_gb": st["mem_peak"] / 1e9, "wall_s": wall,
+                       "submit_lateness_ms_max": float(late.max()) if len(late) else 0.0,
+                       "query_residues": qres}
+        if capacity is None:
+            capacity = st["queries_per_s"]
+    out["runs"] = runs
     db.close()
     return out
 
@@ -429,6 +482,8 @@ def run_ours(args):
     line["clocks"] = clk.summary()
     if world == 1 and args.batched:
         line["batched"] = run_batched(eng, matrix, args, torch)
+    if world == 1 and args.serve:
+        line["serving"] = run_serving(eng, matrix, args)
     if rank == 0:
         sys.path.insert(0, ROOT)
         line["cpu_baseline"] = cpu_baseline(matrix, w, args.cpu_seconds, os.cpu_count() or 1)
