@@ -61,7 +61,7 @@ struct bp_batch {
     int64_t n_hsps = -1;
     int32_t n_items = 0;
     struct Class {
-        int32_t max_qlen = 0, max_mask = 0;
+        int32_t max_qlen = 0, max_len = 0;      // longest query and diagonal array
         int64_t max_entries = 0;
         int32_t item_lo = 0, item_hi = 0;      // its items in d_items
         int32_t queue_lo = 0;                  // its queue offsets start at d_queue_off[queue_lo]
@@ -158,7 +158,7 @@ bp_status enqueue(bp_batch* b) {
         a.rec_cap = b->cap;
         a.rec_count = b->d_counts;
         if (a.n_items > 0)
-            CKB(bp_launch_scan_batch(e, st, a, k.max_qlen, k.max_mask, k.max_entries, k.grid, b->opt.max_warps),
+            CKB(bp_launch_scan_batch(e, st, a, k.max_qlen, k.max_len, k.max_entries, k.grid, b->opt.max_warps),
                 "batched scan launch");
         if (c > 0) {
             CKB(cudaEventRecord(b->ev_join[c - 1], st), "cudaEventRecord");
@@ -325,27 +325,34 @@ bp_status bp_search_batch(bp_engine* e, const bp_db* db, const bp_query* const* 
         hq[i].qlen = q->qlen;
         hq[i].n_entries = (int32_t)q->n_entries;
         hq[i].n_ctx = q->n_ctx;
-        hq[i].diag_mask = q->diag_mask;
-        if (!bp_scan_fits(q->qlen, q->diag_mask, q->n_entries, e->smem_optin)) {
+        hq[i].diag_len = q->diag_len;
+        if (!bp_scan_fits(q->qlen, q->diag_len, q->n_entries, e->smem_optin)) {
             delete b;
             return bp_set_error(e, BP_ERR_TOO_LARGE, "bp_search_batch: a query is too long for the diagonal array");
         }
         hits_sum += q->hits_per_residue;
     }
-    // classes: one per distinct diagonal-array size, longest first
+    // classes: queries whose diagonal arrays round up to the same power of
+    // two share a launch (its layout is sized for the class's longest array);
+    // longest first
+    auto bucket = [&](int32_t i) {
+        int32_t b = 128;
+        while (b < hq[i].diag_len) b <<= 1;
+        return b;
+    };
     std::vector<int32_t> order(n_queries);
     std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(),
-                     [&](int32_t x, int32_t y) { return hq[x].diag_mask > hq[y].diag_mask; });
+    std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) { return bucket(x) > bucket(y); });
     std::vector<WorkItem> items;
     items.reserve((size_t)n_queries * n_chunks);
     std::vector<int32_t> item_pos((size_t)n_queries * n_chunks);   // caller's item index -> position
     for (size_t i = 0; i < order.size();) {
         bp_batch::Class k;
-        k.max_mask = hq[order[i]].diag_mask;
+        const int32_t cls = bucket(order[i]);
         k.item_lo = (int32_t)items.size();
-        for (; i < order.size() && hq[order[i]].diag_mask == k.max_mask; ++i) {
+        for (; i < order.size() && bucket(order[i]) == cls; ++i) {
             const int32_t qi = order[i];
+            k.max_len = std::max(k.max_len, hq[qi].diag_len);
             k.max_qlen = std::max(k.max_qlen, hq[qi].qlen);
             k.max_entries = std::max<int64_t>(k.max_entries, hq[qi].n_entries);
             k.est += queries[qi]->hits_per_residue;

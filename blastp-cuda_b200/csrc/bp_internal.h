@@ -72,7 +72,7 @@ struct bp_query {
     int32_t n_ctx = 1;
     int32_t* d_ctx = nullptr;            // n_ctx x {query_offset, x_dropoff, cutoff}
     bp_params p{};
-    int32_t diag_mask = 0;
+    int32_t diag_len = 0;                // diagonal entries (query + window, see bp_diag_len)
     float hits_per_residue = 0.f;        // expected word hits per subject residue (background composition)
 };
 
@@ -107,7 +107,7 @@ struct ScanArgs {
     int32_t n_ctx;
     const int8_t* matrix;       // [28][32]
     int32_t window;
-    int32_t diag_mask;
+    int32_t diag_len;           // diagonal array entries, >= qlen + window
     int32_t* counters;          // 3 per scanned subject
     HspRec* recs;
     uint32_t rec_cap;
@@ -122,7 +122,7 @@ struct BatchQuery {
     const uint32_t* cells;
     const uint16_t* entries;
     const int32_t* ctx;
-    int32_t qlen, n_entries, n_ctx, diag_mask;
+    int32_t qlen, n_entries, n_ctx, diag_len;
 };
 struct WorkItem {
     int32_t qid;            // query of the batch
@@ -158,16 +158,20 @@ void bp_fill_matrix28(int8_t out[28 * 28]);
 // Robinson background, from its compact cell starts (BP_NC + 1).
 float bp_expected_hits_per_residue(const uint32_t* cells);
 int bp_cell_to_code15(int cell);
-// Largest query the scan kernel can take for a given window (shared-memory
-// diagonal array of one consumer warp).
-bool bp_scan_fits(int32_t qlen, int32_t diag_mask, int64_t n_entries, int smem_optin);
+// Diagonal-array length for a query: qlen + window rounded up to 32, at
+// least 128.  Any length >= qlen + window gives the same results (two live
+// diagonals differ by less than qlen + window, so they never share an entry).
+int bp_diag_len(int qlen, int window);
+// Whether the scan kernel can take a query (its diagonal array must fit
+// shared memory next to the table).
+bool bp_scan_fits(int32_t qlen, int32_t diag_len, int64_t n_entries, int smem_optin);
 
 // ---- launchers ------------------------------------------------------------
 cudaError_t bp_launch_table_build(bp_engine* e, const uint8_t* d_q, int32_t qlen, int32_t threshold,
                                   uint32_t* d_cells, uint16_t* d_entries, uint32_t* d_counts_tmp, int pass);
 cudaError_t bp_launch_scan(bp_engine* e, const ScanArgs& a);
 cudaError_t bp_launch_scan_batch(bp_engine* e, cudaStream_t stream, const BatchArgs& b, int32_t max_qlen,
-                                 int32_t max_diag_mask, int64_t max_entries, int grid, int max_warps);
+                                 int32_t max_diag_len, int64_t max_entries, int grid, int max_warps);
 cudaError_t bp_launch_order(bp_engine* e, int32_t n, const int32_t* d_counters, int64_t* d_hsp_off,
                             const HspRec* d_recs, uint32_t rec_cap, const uint32_t* d_rec_count,
                             int32_t* d_fill, bp_hsp* d_out, int32_t* d_keys, int64_t* d_blocksums);

@@ -34,12 +34,6 @@ bp_status bp_set_error(bp_engine* e, bp_status s, const std::string& msg) {
 
 namespace {
 
-int diag_mask_for(int qlen, int window) {
-    int n = 1;
-    while (n < qlen + window) n <<= 1;
-    return n - 1;
-}
-
 // Sets *bad when any residue code is >= 28 (16 bytes per thread per step).
 __global__ void check_residues(const uint8_t* __restrict__ res, int64_t n, uint32_t* bad) {
     const int64_t n16 = n / 16;
@@ -141,7 +135,7 @@ bp_status bp_run_search(bp_engine* e, bp_result* r) {
     a.n_ctx = q->n_ctx;
     a.matrix = e->d_matrix;
     a.window = q->p.window;
-    a.diag_mask = q->diag_mask;
+    a.diag_len = q->diag_len;
     a.counters = r->d_counters;
     a.recs = e->d_recs;
     a.rec_cap = std::min(e->rec_cap, r->cap);
@@ -384,8 +378,9 @@ bp_status bp_query_create(bp_engine* e, const uint8_t* residues, int32_t length,
     *out = nullptr;
     if (length > BP_MAX_QUERY_LENGTH)
         return bp_set_error(e, BP_ERR_TOO_LARGE, "bp_query_create: query longer than 65535");
-    if (p->word_length != BP_WORD || p->window < 1 || p->x_dropoff < 0)
-        return bp_set_error(e, BP_ERR_INVALID, "bp_query_create: word_length must be 3, window >= 1, x_dropoff >= 0");
+    if (p->word_length != BP_WORD || p->window < 1 || p->window > 65535 || p->x_dropoff < 0)
+        return bp_set_error(e, BP_ERR_INVALID,
+                            "bp_query_create: word_length must be 3, window 1..65535, x_dropoff >= 0");
     for (int32_t i = 0; i < length; ++i)
         if (residues[i] == 0 || residues[i] >= BP_ALPHABET)
             return bp_set_error(e, BP_ERR_INVALID, "bp_query_create: query residue codes must be 1..27");
@@ -395,7 +390,7 @@ bp_status bp_query_create(bp_engine* e, const uint8_t* residues, int32_t length,
     q->qlen = length;
     q->p = *p;
     q->n_ctx = 1;
-    q->diag_mask = diag_mask_for(length, p->window);
+    q->diag_len = bp_diag_len(length, p->window);
     bp_status st = BP_OK;
     uint32_t* d_tmp = nullptr;
     do {
@@ -483,7 +478,7 @@ bp_status bp_search(bp_engine* e, const bp_db* db, const bp_query* q, int32_t fi
         return bp_set_error(e, BP_ERR_INVALID, "bp_search: bad argument");
     *out = nullptr;
     if (count < 0 || count > db->n - first) count = db->n - first;
-    if (!bp_scan_fits(q->qlen, q->diag_mask, q->n_entries, e->smem_optin))
+    if (!bp_scan_fits(q->qlen, q->diag_len, q->n_entries, e->smem_optin))
         return bp_set_error(e, BP_ERR_TOO_LARGE, "bp_search: query too long for the shared-memory diagonal array");
     CK(cudaSetDevice(e->device), "cudaSetDevice");
     bp_result* r = new bp_result();

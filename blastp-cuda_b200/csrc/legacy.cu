@@ -159,7 +159,7 @@ Boolean GPU_BLASTP_check_memory(const LookupTableWrap* lookup_wrap, const Blast_
         return FALSE;
     }
     // any table size fits when it stays in global memory; the diagonal array must fit shared memory
-    if (!bp_scan_fits(query_length, ewp->diag_table->diag_mask, 1 << 30, optin)) return FALSE;
+    if (!bp_scan_fits(query_length, bp_diag_len(query_length, ewp->diag_table->window), 1 << 30, optin)) return FALSE;
     const size_t n = (size_t)gpu_options->num_sequences_to;
     size_t need = 2 * (size_t)h_Database2Dpadded_bytes + 8 * (n + 1) + (size_t)h_Hits_bytes +
                   3 * (size_t)h_GPUBlastInitHitList_bytes + (BP_NCELL + 1) * 4 +
@@ -250,7 +250,11 @@ void GPU_BLASTP(const BLAST_SequenceBlk* query, const BlastQueryInfo* query_info
         for (uint16_t x : entries)
             if ((int32_t)x + 3 > Q) { why = "lookup table lists an offset beyond the query"; break; }
         if (why) break;
-        if (!bp_scan_fits(Q, ewp->diag_table->diag_mask, (int64_t)cell_start[BP_NC], e->smem_optin)) {
+        if (ewp->diag_table->window < 1 || ewp->diag_table->window > 65535) {
+            why = "two-hit window outside 1..65535";
+            break;
+        }
+        if (!bp_scan_fits(Q, bp_diag_len(Q, ewp->diag_table->window), (int64_t)cell_start[BP_NC], e->smem_optin)) {
             why = "query too long for the shared-memory diagonal array";
             break;
         }
@@ -339,7 +343,9 @@ void GPU_BLASTP(const BLAST_SequenceBlk* query, const BlastQueryInfo* query_info
         job->q.d_ctx = d_ctx;
         job->q.p.word_length = 3;
         job->q.p.window = ewp->diag_table->window;
-        job->q.diag_mask = ewp->diag_table->diag_mask;
+        // any array of at least Q + window entries gives the reference's results
+        // with its power-of-two diag_mask table (gpu_blastp_kernel.cu:202)
+        job->q.diag_len = bp_diag_len(Q, ewp->diag_table->window);
         job->q.hits_per_residue = bp_expected_hits_per_residue(cell_start.data());
         job->r.e = e;
         job->r.n = n;

@@ -109,7 +109,7 @@ extern "C" bp_status bp_search_noalloc(const uint8_t* d_query, int32_t qlen, con
     if (!p || !d_offsets || !d_counters || !d_hsp_off || !n_hsps || n_subjects < 0 || n_residues < 0 || qlen < 0 ||
         hsp_cap < 0 || (qlen > 0 && !d_query) || (n_residues > 0 && !d_residues) || (hsp_cap > 0 && !d_hsps))
         return BP_ERR_INVALID;
-    if (p->word_length != BP_WORD || p->window < 1 || p->x_dropoff < 0) return BP_ERR_INVALID;
+    if (p->word_length != BP_WORD || p->window < 1 || p->window > 65535 || p->x_dropoff < 0) return BP_ERR_INVALID;
     if (n_subjects > kMaxSubjects || qlen > kMaxQuery) return BP_ERR_TOO_LARGE;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
@@ -138,8 +138,7 @@ extern "C" bp_status bp_search_noalloc(const uint8_t* d_query, int32_t qlen, con
     int64_t* sums = (int64_t*)(s->base + kOffSums);
     cudaStream_t cs = e.stream;
 
-    int diag = 1;
-    while (diag < qlen + p->window) diag <<= 1;
+    const int diag = bp_diag_len(qlen, p->window);
     const int32_t ctx_h[4] = {0, p->x_dropoff, p->cutoff_score, 0};
     uint32_t hostc[5] = {0, 0, 0, 0, 0};
     uint32_t total = 0;
@@ -165,7 +164,7 @@ extern "C" bp_status bp_search_noalloc(const uint8_t* d_query, int32_t qlen, con
         return BP_ERR_CUDA;
     }
     if ((int64_t)total > kMaxEntries) return BP_ERR_TOO_LARGE;
-    if (!bp_scan_fits(qlen, diag - 1, total, s->smem_optin)) return BP_ERR_TOO_LARGE;
+    if (!bp_scan_fits(qlen, diag, total, s->smem_optin)) return BP_ERR_TOO_LARGE;
     err = bp_launch_table_build(&e, d_query, qlen, p->threshold, cells, entries, tmp, 1);
 
     const uint32_t cap = (uint32_t)(hsp_cap < kMaxRecords ? hsp_cap : kMaxRecords);
@@ -183,7 +182,7 @@ extern "C" bp_status bp_search_noalloc(const uint8_t* d_query, int32_t qlen, con
     a.n_ctx = 1;
     a.matrix = e.d_matrix;
     a.window = p->window;
-    a.diag_mask = diag - 1;
+    a.diag_len = diag;
     a.counters = d_counters;
     a.recs = recs;
     a.rec_cap = cap;

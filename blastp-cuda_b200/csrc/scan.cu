@@ -1,31 +1,39 @@
-// Plain scan kernel: one query against a range of subjects.
+// Scan kernels: one query against a range of subjects (scan_kernel), and many
+// queries against one resident database (scan_batch_kernel).
 //
 // Semantics follow the reference kernel GPU_BLASTP_kernelTwoHit
 // (gpu_blastp_kernel.cu:42-320) and its extenders (:341-549); the mapping to
 // the hardware does not:
 //  * one persistent CTA per SM with up to 32 warps; the query, the scoring
 //    matrix and (when they fit) the compact neighbour-word table are loaded
-//    into shared memory once and shared by every warp for the whole launch;
-//  * a warp owns one subject at a time, taken from a global cursor.  Each
-//    warp runs a three-stage software pipeline over its subjects: cursor grab
-//    (i+3), offsets load (i+2), cp.async.bulk L2 prefetch of the residues
-//    (i+1), scan (i) -- so the database is streamed from HBM into L2 ahead of
-//    the warp that reads it;
+//    into shared memory and shared by every warp;
+//  * a warp owns one subject at a time.  In the plain kernel it takes
+//    subjects from a global cursor through a three-stage software pipeline:
+//    cursor grab (i+3), offsets load (i+2), cp.async.bulk L2 prefetch of the
+//    residues (i+1), scan (i) -- so the database is streamed from HBM into L2
+//    ahead of the warp that reads it;
 //  * the warp reads 128 consecutive word positions (4 per lane, contiguous),
 //    loading the next window's residues while it works on the current one,
 //    looks the words up in the table and flattens the resulting word hits
 //    into chunks of 32 -- one hit per lane, whatever the per-position hit
 //    counts are;
 //  * the per-diagonal two-hit state lives in shared memory, one array per
-//    warp (the reference keeps it in global memory, one per thread);
+//    warp of L = Q + window entries (rounded up to 32, at least 128),
+//    indexed by (q - s) mod L (the reference keeps a power-of-two array in
+//    global memory, one per thread);
 //  * hits of one chunk on the same diagonal are applied in word-position
 //    order (__match_any_sync), the only order the state machine depends on;
 //    distinct diagonals are independent;
-//  * each X-drop extension is walked by the whole warp, 32 letters per step:
-//    prefix sums give the running scores, prefix maxima the best score so
-//    far, and a ballot the first letter where the drop reaches x_drop (or,
-//    walking right, where the score falls to 0) -- the same stop and the same
-//    best offset as the reference's letter-by-letter loops;
+//  * for queries of 320 letters and more, a hit pair that calls for an
+//    extension does not stop the warp: it becomes a task and its diagonal is
+//    marked pending; later hits on a pending diagonal wait, in order, in a
+//    blocked list.  When the queue fills, or the subject ends, the warp walks
+//    the queued extensions -- one lane per extension when there are enough
+//    of them, the whole warp per extension otherwise -- writes their outcomes
+//    into the diagonal states and replays the blocked hits.  Every diagonal
+//    therefore sees exactly the reference's sequence of events; only the
+//    interleaving of independent diagonals changes.  Shorter queries extend
+//    each pair at once, the whole warp walking 32 letters per step;
 //  * surviving HSPs are compacted with a warp ballot into one global append
 //    buffer, tagged with the subject and the hit's index in the subject's hit
 //    stream, from which the ordering pass restores the discovery order.
@@ -36,9 +44,17 @@ extern __shared__ __align__(128) uint8_t bp_smem[];
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
-constexpr uint32_t kFlag = 0x80000000u;
+constexpr uint32_t kFlag = 0x80000000u;     // diagonal: an extension reached past this point
+constexpr uint32_t kPend = 0x40000000u;     // diagonal: an extension waits in the task queue
 constexpr int kP = 4;                       // word positions per lane per window
 constexpr int kMaxWarps = 32;
+constexpr int kTaskCap = 64;                // queued extensions per warp
+constexpr int kBlkCap = 64;                 // hits waiting behind queued extensions, per warp
+constexpr int kLaneWalkMin = 6;             // from this many queued extensions on, one lane walks each
+// Queries at least this long queue their extensions (kDefer); shorter ones
+// have too few extensions per subject for one-lane-per-extension walks to pay
+// for the queue, and extend each pair at once with the whole warp.
+constexpr int kDeferMinQlen = 320;
 
 }  // namespace
 
@@ -47,13 +63,20 @@ struct ScanLayout {
     int warps;
     int cells_mode;        // 0: u16 starts in smem, 1: u32 starts in smem, 2: u32 starts in global
     int entries_smem;
-    int L;
+    int L;                 // diagonal entries per warp (the longest query's)
     int off_cells, off_entries, off_query, off_warps, off_ctl;
-    int warp_bytes;        // diagonal array + per-lane position table
+    int warp_bytes;        // diagonal array + per-lane position table + task queue + blocked list
     int total;
 };
 
 namespace {
+
+// A queued extension (diff = hs - previous hit on the diagonal) or a blocked
+// hit (diff = 0).
+struct Task {
+    int hs, key, d;
+    uint32_t hqx;          // query offset | diff << 16
+};
 
 struct ExtOut {
     int hsp_q, hsp_s, len, score, s_last, right_ext;
@@ -118,11 +141,54 @@ __device__ __forceinline__ void warp_xdrop(const int8_t* m, const uint8_t* __res
     }
 }
 
-// s_BlastAaExtendTwoHit (gpu_blastp_kernel.cu:341-415) with the left
-// (:435-481) and right (:503-549) walks done by the whole warp.  Every lane
-// passes the same arguments and gets the same result.
-__device__ ExtOut warp_extend_two_hit(const int8_t* m, const uint8_t* __restrict__ subj, int slen, const uint8_t* qry,
-                                      int qlen, int s_left, int s_right, int q_right, int xdrop, int lane) {
+// The same walk by one lane, letter by letter as in the reference's loops
+// (gpu_blastp_kernel.cu:435-481, :503-549); residues are fetched four
+// letters ahead so the loads overlap the dependent score chain.
+template <bool kRight>
+__device__ __forceinline__ void lane_xdrop(const int8_t* m, const uint8_t* __restrict__ subj, const uint8_t* qry,
+                                           int s0, int q0, int n, int start, int xdrop, int& best, int& best_i,
+                                           int& stop_i) {
+    int run = start;
+    best = start;
+    best_i = -1;
+    stop_i = n;
+    for (int i0 = 0; i0 < n; i0 += 4) {
+        int sc[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int i = i0 + k;
+            sc[k] = i < n ? (kRight ? msc(m, qry[q0 + i], __ldg(subj + s0 + i))
+                                    : msc(m, qry[q0 - i], __ldg(subj + s0 - i)))
+                          : 0;
+        }
+        bool stop = false;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (!stop && i0 + k < n) {
+                run += sc[k];
+                if (run > best) {
+                    best = run;
+                    best_i = i0 + k;
+                }
+                if (best - run >= xdrop || (kRight && run <= 0)) {
+                    stop = true;
+                    stop_i = i0 + k;
+                }
+            }
+        }
+        if (stop) break;
+    }
+}
+
+// s_BlastAaExtendTwoHit (gpu_blastp_kernel.cu:341-415): the word-start shift,
+// the left walk, which must reach s_left for the right walk to run, and the
+// right walk starting from the left score.  kWarp: every lane passes the
+// same arguments, the walks use the whole warp and every lane gets the
+// result; otherwise each lane extends its own hit pair.
+template <bool kWarp>
+__device__ __forceinline__ ExtOut extend_two_hit(const int8_t* m, const uint8_t* __restrict__ subj, int slen,
+                                                 const uint8_t* qry, int qlen, int s_left, int s_right, int q_right,
+                                                 int xdrop, int lane) {
     int score = 0, left_score = 0, shift = 0;
 #pragma unroll
     for (int i = 0; i < BP_WORD; ++i) {
@@ -136,8 +202,9 @@ __device__ ExtOut warp_extend_two_hit(const int8_t* m, const uint8_t* __restrict
     s_right += shift;
 
     int lbest, lbest_k, lstop;
-    const int nl = min(s_right - 1, q_right - 1) + 1;
-    warp_xdrop<false>(m, subj, qry, s_right - 1, q_right - 1, nl, 0, xdrop, lane, lbest, lbest_k, lstop);
+    const int nl = min(s_right, q_right);
+    if (kWarp) warp_xdrop<false>(m, subj, qry, s_right - 1, q_right - 1, nl, 0, xdrop, lane, lbest, lbest_k, lstop);
+    else lane_xdrop<false>(m, subj, qry, s_right - 1, q_right - 1, nl, 0, xdrop, lbest, lbest_k, lstop);
     const int left_d = lbest_k + 1;
     left_score = lbest;
 
@@ -149,7 +216,8 @@ __device__ ExtOut warp_extend_two_hit(const int8_t* m, const uint8_t* __restrict
         o.right_ext = 1;
         const int nr = min(slen - s_right, qlen - q_right);
         int rbest, rbest_i, rstop;
-        warp_xdrop<true>(m, subj, qry, s_right, q_right, nr, left_score, xdrop, lane, rbest, rbest_i, rstop);
+        if (kWarp) warp_xdrop<true>(m, subj, qry, s_right, q_right, nr, left_score, xdrop, lane, rbest, rbest_i, rstop);
+        else lane_xdrop<true>(m, subj, qry, s_right, q_right, nr, left_score, xdrop, rbest, rbest_i, rstop);
         right_d = rbest_i + 1;
         right_score = rbest;
         o.s_last = s_right + rstop;
@@ -182,17 +250,205 @@ __device__ __forceinline__ void load_window(const uint8_t* __restrict__ sub, int
     for (int i = 0; i < kP + 2; ++i) r[i] = (sl + i < slen) ? (int)__ldg(sub + sl + i) - 1 : -1;
 }
 
-template <typename CellT>
+// One warp's view of the subject it is scanning.
+struct WarpScan {
+    const ScanArgs* a;
+    const int8_t* m;
+    const uint8_t* qs;
+    uint32_t* diag;
+    Task* tasks;
+    Task* blocked;
+    const uint8_t* sub;
+    int slen, oid, base, lane;
+    unsigned lt;
+    int nt, nb;            // queued tasks and blocked hits (warp-uniform)
+    int ext, succ;         // this lane's share of the subject's counters
+};
+
+// Appends the reported HSPs of this round (one candidate per lane).
+__device__ __forceinline__ void emit(WarpScan& w, bool found, int key, int hs, int hq, const ExtOut& x) {
+    const unsigned fm = __ballot_sync(kFull, found);
+    if (!fm) return;
+    uint32_t pos0 = 0;
+    if (w.lane == 0) pos0 = atomicAdd(w.a->rec_count, (uint32_t)__popc(fm));
+    pos0 = __shfl_sync(kFull, pos0, 0);
+    if (found) {
+        const uint32_t pos = pos0 + (uint32_t)__popc(fm & w.lt);
+        if (pos < w.a->rec_cap) {
+            HspRec rec;
+            rec.oid = w.oid;
+            rec.key = key;
+            rec.h.hsp_q = x.hsp_q;
+            rec.h.hsp_s = x.hsp_s;
+            rec.h.query_offset = hq;
+            rec.h.subject_offset = hs;
+            rec.h.hsp_len = x.len;
+            rec.h.score = x.score;
+            w.a->recs[pos] = rec;
+        }
+        ++w.succ;
+    }
+}
+
+__device__ __forceinline__ uint32_t diag_after(const ExtOut& x, int hs, int base) {
+    return x.right_ext ? ((uint32_t)(x.s_last - (BP_WORD - 1) + base) | kFlag) : (uint32_t)(hs + base);
+}
+
+// Applies up to 32 hits (one per lane, in hit-stream order by lane) to the
+// diagonal states.  Hits on the same diagonal go one per round in lane order.
+// kDefer: a pair within the window becomes a task and marks its diagonal
+// pending, and a hit on a pending diagonal joins the blocked list (needs room
+// for 32 more tasks and 32 more blocked hits).  Otherwise each pair is
+// extended at once by the whole warp, one after the other.
+template <bool kDefer>
+__device__ __forceinline__ void apply_hits(WarpScan& w, bool hv, int hs, int hq, int d, int key) {
+    const unsigned vmask = __ballot_sync(kFull, hv);
+    if (!vmask) return;
+    unsigned peers = 0;
+    if (hv) peers = __match_any_sync(vmask, d);
+    bool pending = hv, found = false;
+    ExtOut res{0, 0, 0, 0, 0, 0};
+    const int window = w.a->window;
+    for (;;) {
+        const unsigned pend = __ballot_sync(kFull, pending);
+        if (!pend) break;
+        bool need = false, blk = false;
+        int diff = 0;
+        if (pending && (peers & pend & w.lt) == 0) {
+            pending = false;
+            const uint32_t v = w.diag[d];
+            const int stamp = hs + w.base;
+            if (kDefer && (v & kPend)) {
+                blk = true;
+            } else if (v & kFlag) {
+                // an extension already covered this hit; the first hit past it restarts the diagonal
+                if (stamp >= (int)(v & ~kFlag)) w.diag[d] = (uint32_t)stamp;
+            } else {
+                diff = hs - ((int)v - w.base);
+                if (diff >= window) w.diag[d] = (uint32_t)stamp;
+                else if (diff >= BP_WORD) need = true;
+            }
+        }
+        if (kDefer) {
+            const unsigned bm = __ballot_sync(kFull, blk);
+            if (blk) w.blocked[w.nb + __popc(bm & w.lt)] = Task{hs, key, d, (uint32_t)hq};
+            w.nb += __popc(bm);
+            const unsigned nm = __ballot_sync(kFull, need);
+            if (need) {
+                w.tasks[w.nt + __popc(nm & w.lt)] = Task{hs, key, d, (uint32_t)hq | ((uint32_t)diff << 16)};
+                w.diag[d] = kPend | (uint32_t)(hs + w.base);
+                ++w.ext;
+            }
+            w.nt += __popc(nm);
+        } else {
+            // this round's extensions, one after the other, each by the whole warp
+            unsigned E = __ballot_sync(kFull, need);
+            while (E) {
+                const int leader = __ffs(E) - 1;
+                E &= E - 1;
+                const int e_s = __shfl_sync(kFull, hs, leader);
+                const int e_q = __shfl_sync(kFull, hq, leader);
+                const int e_diff = __shfl_sync(kFull, diff, leader);
+                const ScanArgs& a = *w.a;
+                const int k = a.n_ctx == 1 ? 0 : context_of(a.ctx, a.n_ctx, e_q);
+                const ExtOut x = extend_two_hit<true>(w.m, w.sub, w.slen, w.qs, a.qlen, e_s - e_diff + BP_WORD, e_s,
+                                                      e_q, __ldg(a.ctx + 3 * k + 1), w.lane);
+                if (w.lane == leader) {
+                    res = x;
+                    ++w.ext;
+                    found = x.score >= __ldg(a.ctx + 3 * k + 2);
+                    w.diag[d] = x.right_ext ? ((uint32_t)(x.s_last - (BP_WORD - 1) + w.base) | kFlag)
+                                            : (uint32_t)(hs + w.base);
+                }
+            }
+            __syncwarp();
+        }
+    }
+    if (!kDefer) emit(w, found, key, hs, hq, res);
+}
+
+// Walks every queued extension and writes its outcome into its diagonal.
+__device__ void flush_tasks(WarpScan& w) {
+    const ScanArgs& a = *w.a;
+    const int nt = w.nt;
+    if (nt >= kLaneWalkMin) {
+        for (int t0 = 0; t0 < nt; t0 += 32) {
+            const int t = t0 + w.lane;
+            bool found = false;
+            Task tk{0, 0, 0, 0};
+            ExtOut x{0, 0, 0, 0, 0, 0};
+            if (t < nt) {
+                tk = w.tasks[t];
+                const int hq = (int)(tk.hqx & 0xffffu), diff = (int)(tk.hqx >> 16);
+                const int k = a.n_ctx == 1 ? 0 : context_of(a.ctx, a.n_ctx, hq);
+                x = extend_two_hit<false>(w.m, w.sub, w.slen, w.qs, a.qlen, tk.hs - diff + BP_WORD, tk.hs, hq,
+                                          __ldg(a.ctx + 3 * k + 1), w.lane);
+                found = x.score >= __ldg(a.ctx + 3 * k + 2);
+                w.diag[tk.d] = diag_after(x, tk.hs, w.base);
+            }
+            emit(w, found, tk.key, tk.hs, (int)(tk.hqx & 0xffffu), x);
+        }
+    } else {
+        for (int t = 0; t < nt; ++t) {
+            const Task tk = w.tasks[t];
+            const int hq = (int)(tk.hqx & 0xffffu), diff = (int)(tk.hqx >> 16);
+            const int k = a.n_ctx == 1 ? 0 : context_of(a.ctx, a.n_ctx, hq);
+            const ExtOut x = extend_two_hit<true>(w.m, w.sub, w.slen, w.qs, a.qlen, tk.hs - diff + BP_WORD, tk.hs,
+                                                  hq, __ldg(a.ctx + 3 * k + 1), w.lane);
+            const bool found = w.lane == 0 && x.score >= __ldg(a.ctx + 3 * k + 2);
+            if (w.lane == 0) w.diag[tk.d] = diag_after(x, tk.hs, w.base);
+            emit(w, found, tk.key, tk.hs, hq, x);
+        }
+    }
+    __syncwarp();
+    w.nt = 0;
+}
+
+// Resolves the queued extensions, then replays the blocked hits once, in
+// order.  A replayed hit may queue a new extension (and block the hits after
+// it on its diagonal again); the blocked list is rewritten in place.
+__device__ void resolve(WarpScan& w) {
+    flush_tasks(w);
+    const int n = w.nb;
+    w.nb = 0;
+    for (int r = 0; r < n; r += 32) {
+        const int i = r + w.lane;
+        const bool hv = i < n;
+        Task b{0, 0, 0, 0};
+        if (hv) b = w.blocked[i];
+        __syncwarp();
+        apply_hits<true>(w, hv, b.hs, (int)(b.hqx & 0xffffu), b.d, b.key);
+    }
+    __syncwarp();
+}
+
+template <typename CellT, bool kDefer>
 __device__ void scan_subject(const ScanArgs& a, const int8_t* m, const uint8_t* qs, const CellT* cells,
-                             const uint16_t* entries, uint32_t* diag, uint32_t* lane_pos, int oid,
-                             const uint8_t* __restrict__ sub, int slen, int& base, int lane) {
-    const unsigned lt = (1u << lane) - 1u;
+                             const uint16_t* entries, uint32_t* diag, uint32_t* lane_pos, Task* tasks,
+                             Task* blocked, int oid, const uint8_t* __restrict__ sub, int slen, int& base, int lane) {
+    const int L = a.diag_len;
     if (base + slen + a.window > (1 << 30)) {
-        for (int i = lane; i <= a.diag_mask; i += 32) diag[i] = 0;
+        for (int i = lane; i < L; i += 32) diag[i] = 0;
         __syncwarp();
         base = a.window;
     }
-    int hits = 0, ext = 0, succ = 0, key_base = 0;
+    WarpScan w;
+    w.a = &a;
+    w.m = m;
+    w.qs = qs;
+    w.diag = diag;
+    w.tasks = tasks;
+    w.blocked = blocked;
+    w.sub = sub;
+    w.slen = slen;
+    w.oid = oid;
+    w.base = base;
+    w.lane = lane;
+    w.lt = (1u << lane) - 1u;
+    w.nt = w.nb = 0;
+    w.ext = w.succ = 0;
+    int hits = 0, key_base = 0;
+    int s0m = 0;                         // s0 mod L
     const int last_pos = slen - BP_WORD;
     const uint32_t* my_row = lane_pos - lane * kP * 2;
     int r[kP + 2];
@@ -219,6 +475,8 @@ __device__ void scan_subject(const ScanArgs& a, const int8_t* m, const uint8_t* 
         const uint32_t total = __shfl_sync(kFull, incl, 31);
         __syncwarp();
         for (uint32_t hb = 0; hb < total; hb += 32) {
+            if (kDefer)
+                while (w.nt > kTaskCap - 32 || w.nb > kBlkCap - 32) resolve(w);
             const uint32_t j = hb + lane;
             const bool hv = j < total;
             // owner lane: first lane whose inclusive prefix exceeds j
@@ -240,86 +498,29 @@ __device__ void scan_subject(const ScanArgs& a, const int8_t* m, const uint8_t* 
                     if (op[t] <= local) p = t;
                 hs = s0 + lo * kP + p;
                 hq = entries[op[kP + p] + (local - op[p])];
-                d = (hq - hs) & a.diag_mask;
+                // (hq - hs) mod L, from s0 mod L: lo*kP + p < 128 <= L
+                int hm = s0m + lo * kP + p;
+                if (hm >= L) hm -= L;
+                d = hq - hm;
+                if (d < 0) d += L;
             }
-            const unsigned vmask = __ballot_sync(kFull, hv);
-            unsigned peers = 0;
-            if (hv) peers = __match_any_sync(vmask, d);
-            bool pending = hv, found = false;
-            ExtOut res;
-            res.hsp_q = res.hsp_s = res.len = res.score = res.s_last = res.right_ext = 0;
-            for (;;) {
-                const unsigned pend = __ballot_sync(kFull, pending);
-                if (!pend) break;
-                bool need = false;
-                int prev = 0;
-                if (pending && (peers & pend & lt) == 0) {
-                    pending = false;
-                    const uint32_t v = diag[d];
-                    const int stamp = hs + base;
-                    if (v & kFlag) {
-                        // an extension already covered this hit; the first hit past it restarts the diagonal
-                        if (stamp >= (int)(v & ~kFlag)) diag[d] = (uint32_t)stamp;
-                    } else {
-                        prev = (int)v - base;
-                        const int diff = hs - prev;
-                        if (diff >= a.window) diag[d] = (uint32_t)stamp;
-                        else if (diff >= BP_WORD) need = true;
-                    }
-                }
-                // extensions of this round, one after the other, each by the whole warp
-                unsigned E = __ballot_sync(kFull, need);
-                while (E) {
-                    const int leader = __ffs(E) - 1;
-                    E &= E - 1;
-                    const int e_s = __shfl_sync(kFull, hs, leader);
-                    const int e_q = __shfl_sync(kFull, hq, leader);
-                    const int e_prev = __shfl_sync(kFull, prev, leader);
-                    const int k = a.n_ctx == 1 ? 0 : context_of(a.ctx, a.n_ctx, e_q);
-                    const ExtOut x = warp_extend_two_hit(m, sub, slen, qs, a.qlen, e_prev + BP_WORD, e_s, e_q,
-                                                         __ldg(a.ctx + 3 * k + 1), lane);
-                    if (lane == leader) {
-                        res = x;
-                        ++ext;
-                        found = x.score >= __ldg(a.ctx + 3 * k + 2);
-                        diag[d] = x.right_ext ? ((uint32_t)(x.s_last - (BP_WORD - 1) + base) | kFlag)
-                                              : (uint32_t)(hs + base);
-                    }
-                }
-                __syncwarp();
-            }
-            const unsigned fm = __ballot_sync(kFull, found);
-            if (fm) {
-                uint32_t pos0 = 0;
-                if (lane == 0) pos0 = atomicAdd(a.rec_count, (uint32_t)__popc(fm));
-                pos0 = __shfl_sync(kFull, pos0, 0);
-                if (found) {
-                    const uint32_t pos = pos0 + (uint32_t)__popc(fm & lt);
-                    if (pos < a.rec_cap) {
-                        HspRec rec;
-                        rec.oid = oid;
-                        rec.key = key_base + (int)j;
-                        rec.h.hsp_q = res.hsp_q;
-                        rec.h.hsp_s = res.hsp_s;
-                        rec.h.query_offset = hq;
-                        rec.h.subject_offset = hs;
-                        rec.h.hsp_len = res.len;
-                        rec.h.score = res.score;
-                        a.recs[pos] = rec;
-                    }
-                }
-                succ += __popc(fm);
-            }
+            apply_hits<kDefer>(w, hv, hs, hq, d, key_base + (int)j);
         }
         key_base += (int)total;
+        s0m += 32 * kP;
+        if (s0m >= L) s0m -= L;
         __syncwarp();
 #pragma unroll
         for (int i = 0; i < kP + 2; ++i) r[i] = rn[i];
     }
+    if (kDefer)
+        while (w.nt > 0 || w.nb > 0) resolve(w);
+    int ext = w.ext, succ = w.succ;
 #pragma unroll
     for (int o = 16; o >= 1; o >>= 1) {
         hits += __shfl_xor_sync(kFull, hits, o);
         ext += __shfl_xor_sync(kFull, ext, o);
+        succ += __shfl_xor_sync(kFull, succ, o);
     }
     if (lane == 0) {
         a.counters[3 * (int64_t)oid + 0] = hits;
@@ -329,7 +530,25 @@ __device__ void scan_subject(const ScanArgs& a, const int8_t* m, const uint8_t* 
     base += slen + a.window;
 }
 
-template <typename CellT, bool kCellsSmem>
+// Per-warp regions: diagonal array, lane position table, task queue, blocked list.
+struct WarpRegions {
+    uint32_t* diag;
+    uint32_t* lane_pos;
+    Task* tasks;
+    Task* blocked;
+};
+
+__device__ __forceinline__ WarpRegions warp_regions(const ScanLayout& lay, int warp, int lane) {
+    uint8_t* wr = bp_smem + lay.off_warps + (size_t)warp * lay.warp_bytes;
+    WarpRegions r;
+    r.diag = reinterpret_cast<uint32_t*>(wr);
+    r.lane_pos = reinterpret_cast<uint32_t*>(wr + (size_t)lay.L * 4) + lane * kP * 2;
+    r.tasks = reinterpret_cast<Task*>(wr + (size_t)lay.L * 4 + 32 * kP * 2 * 4);
+    r.blocked = r.tasks + kTaskCap;
+    return r;
+}
+
+template <typename CellT, bool kCellsSmem, bool kDefer>
 __global__ void __launch_bounds__(kMaxWarps * 32, 1)
 scan_kernel(ScanArgs a, ScanLayout lay) {
     uint8_t* sm = bp_smem;
@@ -350,10 +569,8 @@ scan_kernel(ScanArgs a, ScanLayout lay) {
     }
     for (int i = threadIdx.x; i < a.qlen; i += blockDim.x) qs[i] = a.query[i];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    uint8_t* wr = sm + lay.off_warps + (size_t)warp * lay.warp_bytes;
-    uint32_t* diag = reinterpret_cast<uint32_t*>(wr);
-    uint32_t* lane_pos = reinterpret_cast<uint32_t*>(wr + (size_t)lay.L * 4) + lane * kP * 2;
-    for (int i = lane; i < lay.L; i += 32) diag[i] = 0;
+    const WarpRegions wr = warp_regions(lay, warp, lane);
+    for (int i = lane; i < lay.L; i += 32) wr.diag[i] = 0;
     __syncthreads();
 
     // Subject pipeline, kept by lane 0.  At the top of iteration i:
@@ -391,7 +608,8 @@ scan_kernel(ScanArgs a, ScanLayout lay) {
             }
             oid3 = (int)atomicAdd(a.cursor, 1u);
         }
-        scan_subject<CellT>(a, m, qs, cells, entries, diag, lane_pos, cur, a.db + cs, (int)(ce - cs), base, lane);
+        scan_subject<CellT, kDefer>(a, m, qs, cells, entries, wr.diag, wr.lane_pos, wr.tasks, wr.blocked, cur,
+                                    a.db + cs, (int)(ce - cs), base, lane);
         int nxt = 0;
         long long ns = 0, ne = 0;
         if (lane == 0) {
@@ -424,7 +642,7 @@ struct BatchCtl {
 // (query, subject) pair is scanned by scan_subject exactly as in the
 // single-query kernel, so every query's result is the single-query result;
 // counters and records are indexed by segment = query * n_subjects + subject.
-template <typename CellT, bool kCellsSmem>
+template <typename CellT, bool kCellsSmem, bool kDefer>
 __global__ void __launch_bounds__(kMaxWarps * 32, 1)
 scan_batch_kernel(BatchArgs b, ScanLayout lay) {
     uint8_t* sm = bp_smem;
@@ -433,10 +651,8 @@ scan_batch_kernel(BatchArgs b, ScanLayout lay) {
     BatchCtl* ctl = reinterpret_cast<BatchCtl*>(sm + lay.off_ctl);
     for (int i = threadIdx.x; i < 28 * BP_MROW; i += blockDim.x) m[i] = b.matrix[i];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    uint8_t* wr = sm + lay.off_warps + (size_t)warp * lay.warp_bytes;
-    uint32_t* diag = reinterpret_cast<uint32_t*>(wr);
-    uint32_t* lane_pos = reinterpret_cast<uint32_t*>(wr + (size_t)lay.L * 4) + lane * kP * 2;
-    for (int i = lane; i < lay.L; i += 32) diag[i] = 0;
+    const WarpRegions wr = warp_regions(lay, warp, lane);
+    for (int i = lane; i < lay.L; i += 32) wr.diag[i] = 0;
     int base = b.window;   // diagonal stamp offset, carried across queries (stale stamps stay stale)
     int cur_q = -1;
     const CellT* cells = nullptr;
@@ -486,7 +702,7 @@ scan_batch_kernel(BatchArgs b, ScanLayout lay) {
                 a.ctx = bq.ctx;
                 a.n_ctx = bq.n_ctx;
                 a.window = b.window;
-                a.diag_mask = bq.diag_mask;
+                a.diag_len = bq.diag_len;
                 a.counters = b.counters;
                 a.recs = b.recs;
                 a.rec_cap = b.rec_cap;
@@ -515,13 +731,13 @@ scan_batch_kernel(BatchArgs b, ScanLayout lay) {
             const long long so = b.db_off[oid], eo = b.db_off[oid + 1];
             if (base + (int)(eo - so) + b.window > (1 << 30)) {
                 // the stamp offset is about to wrap: clear the whole array, since
-                // queries with a wider mask than this one read past its mask
-                for (int i = lane; i < lay.L; i += 32) diag[i] = 0;
+                // queries with a longer array than this one read past its end
+                for (int i = lane; i < lay.L; i += 32) wr.diag[i] = 0;
                 __syncwarp();
                 base = b.window;
             }
-            scan_subject<CellT>(ctl->args, m, qs, cells, entries, diag, lane_pos, (int)(seg0 + oid - b.subject_first),
-                                b.db + so, (int)(eo - so), base, lane);
+            scan_subject<CellT, kDefer>(ctl->args, m, qs, cells, entries, wr.diag, wr.lane_pos, wr.tasks, wr.blocked,
+                                        (int)(seg0 + oid - b.subject_first), b.db + so, (int)(eo - so), base, lane);
         }
         __syncthreads();
     }
@@ -545,7 +761,7 @@ ScanLayout make_layout(int qlen, int L, int64_t n_entries, int warps, int cells_
     l.off_query = (int)off;
     off = al(off + qlen, 16);
     l.off_warps = (int)off;
-    const long long wb = al((long long)L * 4 + 32 * kP * 2 * 4, 16);
+    const long long wb = al((long long)L * 4 + 32 * kP * 2 * 4 + (kTaskCap + kBlkCap) * (long long)sizeof(Task), 16);
     l.warp_bytes = (int)(wb > big ? big : wb);
     off += (long long)warps * wb;
     off = al(off, 16);
@@ -574,9 +790,9 @@ bool choose_layout(int qlen, int L, int64_t n_entries, int smem_optin, ScanLayou
     return false;
 }
 
-template <typename CellT, bool kCellsSmem>
+template <typename CellT, bool kCellsSmem, bool kDefer>
 cudaError_t launch(bp_engine* e, const ScanArgs& a, const ScanLayout& lay) {
-    auto kern = scan_kernel<CellT, kCellsSmem>;
+    auto kern = scan_kernel<CellT, kCellsSmem, kDefer>;
     cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, lay.total);
     if (err != cudaSuccess) return err;
     int grid = e->sm_count;
@@ -587,9 +803,9 @@ cudaError_t launch(bp_engine* e, const ScanArgs& a, const ScanLayout& lay) {
     return cudaGetLastError();
 }
 
-template <typename CellT, bool kCellsSmem>
+template <typename CellT, bool kCellsSmem, bool kDefer>
 cudaError_t launch_batch(bp_engine* e, cudaStream_t stream, const BatchArgs& b, const ScanLayout& lay, int grid) {
-    auto kern = scan_batch_kernel<CellT, kCellsSmem>;
+    auto kern = scan_batch_kernel<CellT, kCellsSmem, kDefer>;
     cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, lay.total);
     if (err != cudaSuccess) return err;
     kern<<<grid, lay.warps * 32, lay.total, stream>>>(b, lay);
@@ -600,28 +816,44 @@ cudaError_t launch_batch(bp_engine* e, cudaStream_t stream, const BatchArgs& b, 
 }  // namespace
 
 static_assert(sizeof(BatchCtl) <= 512, "batched control block must fit its shared-memory slot");
+static_assert(sizeof(Task) == 16, "task layout");
 
-cudaError_t bp_launch_scan_batch(bp_engine* e, cudaStream_t stream, const BatchArgs& b, int32_t max_qlen,
-                                 int32_t max_diag_mask, int64_t max_entries, int grid, int max_warps) {
-    ScanLayout lay;
-    if (!choose_layout(max_qlen, max_diag_mask + 1, max_entries, e->smem_optin, &lay)) return cudaErrorInvalidValue;
-    if (max_warps > 0 && lay.warps > max_warps) {
-        lay = make_layout(max_qlen, max_diag_mask + 1, max_entries, max_warps, lay.cells_mode, lay.entries_smem);
-    }
-    if (lay.cells_mode == 0) return launch_batch<uint16_t, true>(e, stream, b, lay, grid);
-    if (lay.cells_mode == 1) return launch_batch<uint32_t, true>(e, stream, b, lay, grid);
-    return launch_batch<uint32_t, false>(e, stream, b, lay, grid);
+int bp_diag_len(int qlen, int window) {
+    const long long n = ((long long)qlen + window + 31) / 32 * 32;
+    return (int)(n < 128 ? 128 : (n > (1LL << 30) ? (1LL << 30) : n));
 }
 
-bool bp_scan_fits(int32_t qlen, int32_t diag_mask, int64_t n_entries, int smem_optin) {
+cudaError_t bp_launch_scan_batch(bp_engine* e, cudaStream_t stream, const BatchArgs& b, int32_t max_qlen,
+                                 int32_t max_diag_len, int64_t max_entries, int grid, int max_warps) {
+    ScanLayout lay;
+    if (!choose_layout(max_qlen, max_diag_len, max_entries, e->smem_optin, &lay)) return cudaErrorInvalidValue;
+    if (max_warps > 0 && lay.warps > max_warps) {
+        lay = make_layout(max_qlen, max_diag_len, max_entries, max_warps, lay.cells_mode, lay.entries_smem);
+    }
+    if (max_qlen >= kDeferMinQlen) {
+        if (lay.cells_mode == 0) return launch_batch<uint16_t, true, true>(e, stream, b, lay, grid);
+        if (lay.cells_mode == 1) return launch_batch<uint32_t, true, true>(e, stream, b, lay, grid);
+        return launch_batch<uint32_t, false, true>(e, stream, b, lay, grid);
+    }
+    if (lay.cells_mode == 0) return launch_batch<uint16_t, true, false>(e, stream, b, lay, grid);
+    if (lay.cells_mode == 1) return launch_batch<uint32_t, true, false>(e, stream, b, lay, grid);
+    return launch_batch<uint32_t, false, false>(e, stream, b, lay, grid);
+}
+
+bool bp_scan_fits(int32_t qlen, int32_t diag_len, int64_t n_entries, int smem_optin) {
     ScanLayout l;
-    return choose_layout(qlen, diag_mask + 1, n_entries, smem_optin, &l);
+    return choose_layout(qlen, diag_len, n_entries, smem_optin, &l);
 }
 
 cudaError_t bp_launch_scan(bp_engine* e, const ScanArgs& a) {
     ScanLayout lay;
-    if (!choose_layout(a.qlen, a.diag_mask + 1, a.n_entries, e->smem_optin, &lay)) return cudaErrorInvalidValue;
-    if (lay.cells_mode == 0) return launch<uint16_t, true>(e, a, lay);
-    if (lay.cells_mode == 1) return launch<uint32_t, true>(e, a, lay);
-    return launch<uint32_t, false>(e, a, lay);
+    if (!choose_layout(a.qlen, a.diag_len, a.n_entries, e->smem_optin, &lay)) return cudaErrorInvalidValue;
+    if (a.qlen >= kDeferMinQlen) {
+        if (lay.cells_mode == 0) return launch<uint16_t, true, true>(e, a, lay);
+        if (lay.cells_mode == 1) return launch<uint32_t, true, true>(e, a, lay);
+        return launch<uint32_t, false, true>(e, a, lay);
+    }
+    if (lay.cells_mode == 0) return launch<uint16_t, true, false>(e, a, lay);
+    if (lay.cells_mode == 1) return launch<uint32_t, true, false>(e, a, lay);
+    return launch<uint32_t, false, false>(e, a, lay);
 }

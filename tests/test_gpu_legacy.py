@@ -88,5 +88,11 @@ def test_check_availability_and_memory_gate(matrix):
     vol, glen, flat, poff = gpu_volume(w.db.residues, w.db.offsets, 32)
     ok = LegacyCall(q, [(0, 16, 41)], table[0], table[1], 40, 512, vol, glen, 64, 1, 32)
     assert ok.check_memory()
-    huge = LegacyCall(q, [(0, 16, 41)], table[0], table[1], 40, 1 << 20, vol, glen, 64, 1, 32)
+    # the engine sizes its own diagonal array from query + window, whatever
+    # the caller's diag table is; a query whose array cannot fit shared
+    # memory is refused
+    assert LegacyCall(q, [(0, 16, 41)], table[0], table[1], 40, 1 << 20, vol, glen, 64, 1, 32).check_memory()
+    qlong = synth.residues(np.random.default_rng(9), 60_000)
+    tl = oracle.build_table(qlong, matrix, 11)
+    huge = LegacyCall(qlong, [(0, 16, 41)], tl[0], tl[1], 40, 1 << 16, vol, glen, 64, 1, 32)
     assert not huge.check_memory()      # diagonal array beyond shared memory
