@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--batch-subjects", type=int, default=2_000_000)
     ap.add_argument("--batch-queries", type=int, default=256)
     ap.add_argument("--batch-reps", type=int, default=1)
+    ap.add_argument("--batch-autotune", type=int, default=1, help="run the autotuner (0: skip it)")
     ap.add_argument("--serve", type=int, default=1, help="also measure the serving loop (1 GPU runs only)")
     ap.add_argument("--serve-subjects", type=int, default=5_000_000)
     ap.add_argument("--serve-requests", type=int, default=128)
@@ -212,17 +213,18 @@ def run_batched(eng, matrix, args, torch):
            "residues": w.db.n_residues, "plain": {"ms": plain_ms, "value": work / (plain_ms / 1e3)}}
     model = costmodel.CostModel.load(eng)
     planted = 0.002
-    t0 = time.perf_counter()
-    best, trials = eng.autotune(db, qs, model=model, planted_density=planted,
-                                sample_subjects=max(1, w.db.n_subjects // 16), reps=1)
-    out["autotune"] = {"sample_subjects": max(1, w.db.n_subjects // 16), "seconds": time.perf_counter() - t0,
-                       "best": dict(best, schedule=SCHED_NAMES[best["schedule"]]),
-                       "trials": [[t["chunk_residues"], SCHED_NAMES[t["schedule"]], t["max_warps"], round(t["ms"], 3)]
-                                  for t in trials]}
     variants = {"static": dict(chunk_residues=1 << 20, schedule=SCHED_STATIC),
                 "dynamic": dict(chunk_residues=1 << 20, schedule=SCHED_DYNAMIC),
-                "learned": dict(chunk_residues=1 << 20, schedule=SCHED_COSTS),
-                "autotuned": dict(best)}
+                "learned": dict(chunk_residues=1 << 20, schedule=SCHED_COSTS)}
+    if args.batch_autotune:
+        t0 = time.perf_counter()
+        best, trials = eng.autotune(db, qs, model=model, planted_density=planted,
+                                    sample_subjects=max(1, w.db.n_subjects // 16), reps=1)
+        out["autotune"] = {"sample_subjects": max(1, w.db.n_subjects // 16), "seconds": time.perf_counter() - t0,
+                           "best": dict(best, schedule=SCHED_NAMES[best["schedule"]]),
+                           "trials": [[t["chunk_residues"], SCHED_NAMES[t["schedule"]], t["max_warps"],
+                                       round(t["ms"], 3)] for t in trials]}
+        variants["autotuned"] = dict(best)
     identical = True
     res = {}
     for name, kw in variants.items():

@@ -134,6 +134,7 @@ SIGNATURES = {
     "GPU_BLASTP_check_memory": (ctypes.c_uint8, [P, P, P, ctypes.c_int, i32, i32, i32, i32, i32]),
     "GPU_BLAST_check_availability": (ctypes.c_uint8, []),
     "Round2Multiple": (None, [P]),
+    "GPU_BLASTP_get_hsps": (ctypes.c_uint8, [P, P, P, i64, P]),
 }
 
 _lib = None

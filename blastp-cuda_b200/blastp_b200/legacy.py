@@ -175,5 +175,15 @@ class LegacyCall:
                                   self.slots[1], self.list_bytes, self.n)
         return hits, ring
 
+    def get_hsps(self):
+        """The complete HSP set (hsp_off [n+1], hsps [k, 6]) after get_data."""
+        k = ctypes.c_int64(0)
+        assert lib().GPU_BLASTP_get_hsps(self.slots[0], None, None, 0, ctypes.byref(k))
+        off = np.zeros(self.n + 1, dtype=np.int64)
+        hsps = np.zeros((max(k.value, 1), 6), dtype=np.int32)
+        assert lib().GPU_BLASTP_get_hsps(self.slots[0], off.ctypes.data, hsps.ctypes.data, k.value,
+                                         ctypes.byref(k))
+        return off, hsps[:k.value]
+
     def free(self):
         lib().GPU_BLASTP_free_memory(*[ctypes.byref(x) for x in self.slots])

@@ -402,6 +402,19 @@ void GPU_BLASTP_get_data(Int4* h_Hits, Int4* d_Hits, const Int4 h_Hits_bytes,
     }
 }
 
+Boolean GPU_BLASTP_get_hsps(Int4* d_Hits, int64_t* hsp_off, GPUBlastInitHitList* hsps, int64_t hsp_cap,
+                            int64_t* n_hsps) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    auto it = g_jobs.find(d_Hits);
+    if (it == g_jobs.end() || !it->second->ok) return FALSE;
+    LegacyJob* job = it->second;
+    if (bp_result_wait(&job->r) != BP_OK) return FALSE;
+    const int64_t k = bp_result_hsps(&job->r);
+    if (n_hsps) *n_hsps = k;
+    if (hsps && k > hsp_cap) return FALSE;
+    return bp_result_copy(&job->r, nullptr, hsp_off, reinterpret_cast<bp_hsp*>(hsps)) == BP_OK ? TRUE : FALSE;
+}
+
 void GPU_BLASTP_free_memory(Int4** d_Hits, GPUBlastInitHitList** d_GPUBlastInitHitList,
                             Int4** d_Database2Dpadded, Int4** d_RepeatedSubstitutionMatrix,
                             Int4** d_RepeatedSequence_length_vector, PV_ARRAY_TYPE** d_RepeatedPV,

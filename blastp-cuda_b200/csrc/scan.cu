@@ -793,7 +793,10 @@ bool choose_layout(int qlen, int L, int64_t n_entries, int smem_optin, ScanLayou
 template <typename CellT, bool kCellsSmem, bool kDefer>
 cudaError_t launch(bp_engine* e, const ScanArgs& a, const ScanLayout& lay) {
     auto kern = scan_kernel<CellT, kCellsSmem, kDefer>;
-    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, lay.total);
+    // the largest allowed size, not this launch's: launches of one instance
+    // with different layouts (batch classes, captured graph nodes replayed
+    // later) must all stay valid whatever order the attribute was set in
+    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, e->smem_optin);
     if (err != cudaSuccess) return err;
     int grid = e->sm_count;
     const int need = (a.n + lay.warps - 1) / lay.warps;   // no more CTAs than subjects to feed them
@@ -806,7 +809,10 @@ cudaError_t launch(bp_engine* e, const ScanArgs& a, const ScanLayout& lay) {
 template <typename CellT, bool kCellsSmem, bool kDefer>
 cudaError_t launch_batch(bp_engine* e, cudaStream_t stream, const BatchArgs& b, const ScanLayout& lay, int grid) {
     auto kern = scan_batch_kernel<CellT, kCellsSmem, kDefer>;
-    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, lay.total);
+    // the largest allowed size, not this launch's: launches of one instance
+    // with different layouts (batch classes, captured graph nodes replayed
+    // later) must all stay valid whatever order the attribute was set in
+    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, e->smem_optin);
     if (err != cudaSuccess) return err;
     kern<<<grid, lay.warps * 32, lay.total, stream>>>(b, lay);
     e->launches += 1;

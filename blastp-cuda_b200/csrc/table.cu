@@ -109,8 +109,10 @@ cudaError_t bp_launch_table_build(bp_engine* e, const uint8_t* d_q, int32_t qlen
                                   uint32_t* d_cells, uint16_t* d_entries, uint32_t* d_counts_tmp, int pass) {
     const size_t smem = 28 * BP_MROW + (size_t)qlen;
     if (smem > 48 * 1024) {
+        // the device limit, not this query's size, so that concurrent builds
+        // for other queries (other threads, other engines) stay valid
         cudaError_t err =
-            cudaFuncSetAttribute(table_walk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            cudaFuncSetAttribute(table_walk, cudaFuncAttributeMaxDynamicSharedMemorySize, e->smem_optin);
         if (err != cudaSuccess) return err;
     }
     const int grid = (BP_NC + kCountThreads - 1) / kCountThreads;

@@ -89,6 +89,18 @@ Boolean GPU_BLAST_check_availability(void);
 
 void Round2Multiple(Int4* MaxLength);
 
+/* Addition (no counterpart in the reference): the complete HSP set of the
+ * last GPU_BLASTP call on d_Hits, valid between GPU_BLASTP_get_data and
+ * GPU_BLASTP_free_memory.  hsp_off[num_sequences+1] (int64) indexes hsps per
+ * subject, in discovery order.  With it a caller fills its initial-hit lists
+ * for every subject, including those with more than two HSPs, which the
+ * two-slot ring cannot hold and which the reference sends back to the CPU
+ * (blast_engine.c:529-538).  hsps may be NULL to learn the count (n_hsps);
+ * returns FALSE when there is no such search, it failed, or hsp_cap is too
+ * small. */
+Boolean GPU_BLASTP_get_hsps(Int4* d_Hits, int64_t* hsp_off, GPUBlastInitHitList* hsps, int64_t hsp_cap,
+                            int64_t* n_hsps);
+
 #ifdef __cplusplus
 }
 #endif

@@ -44,8 +44,12 @@ def run_case(matrix, query, contexts, residues, offsets, blocks, threads, sort=F
     assert call.check_memory()
     call.run()
     hits, ring = call.get_data()
+    full_off, full_hsps = call.get_hsps()
     call.free()
     counters, hoff, hsps = oracle.scan(flat, poff, query, table, matrix, contexts, window=40, diag_mask=L - 1)
+    # the complete set, not only the two ring slots: every subject's HSPs
+    assert (full_off == hoff).all()
+    assert full_hsps.shape == hsps.shape and (full_hsps == hsps).all()
     return hits, ring, counters, hoff, hsps
 
 
@@ -57,7 +61,28 @@ def test_gpu_blastp_drop_in(matrix, blocks, threads, sort):
                                                 blocks, threads, sort)
     assert (hits == counters).all()
     assert (ring == expected_ring(counters, hoff, hsps)).all()
-    assert counters[:, 1].sum() > 0 and (counters[:, 1] > 2).any() is not None
+    assert counters[:, 1].sum() > 0
+
+
+def test_gpu_blastp_full_hsp_set_beyond_ring(matrix):
+    # subjects holding several separated copies of query segments have more
+    # HSPs than the two ring slots; GPU_BLASTP_get_hsps returns all of them
+    rng = np.random.default_rng(21)
+    q = synth.residues(rng, 400)
+    parts = []
+    for i in range(300):
+        if i % 3 == 0:
+            segs = [q[a:a + 60] for a in (0, 100, 200, 300)]
+            fill = [synth.residues(rng, 50) for _ in segs]
+            parts.append(np.concatenate([x for pair in zip(fill, segs) for x in pair]))
+        else:
+            parts.append(synth.residues(rng, int(rng.integers(50, 400))))
+    res = np.concatenate(parts).astype(np.uint8)
+    off = np.concatenate([[0], np.cumsum([len(p) for p in parts])]).astype(np.int64)
+    hits, ring, counters, hoff, hsps = run_case(matrix, q, [(0, 16, 41)], res, off, 4, 32)
+    assert (counters[:, 1] > 2).sum() >= 90
+    assert (hits == counters).all()
+    assert (ring == expected_ring(counters, hoff, hsps)).all()
 
 
 def test_gpu_blastp_multi_context(matrix):
