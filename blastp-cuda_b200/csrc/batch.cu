@@ -332,29 +332,38 @@ bp_status bp_search_batch(bp_engine* e, const bp_db* db, const bp_query* const* 
         }
         hits_sum += q->hits_per_residue;
     }
-    // classes: queries whose diagonal arrays round up to the same power of
-    // two share a launch (its layout is sized for the class's longest array);
-    // longest first
-    auto bucket = [&](int32_t i) {
-        int32_t b = 128;
-        while (b < hq[i].diag_len) b <<= 1;
-        return b;
+    // classes: a launch's layout is sized for its longest query, so queries
+    // share a launch only when that leaves each of them the warps per CTA it
+    // would get alone, and when they extend the same way; longest first
+    auto own_warps = [&](int32_t i) {
+        return bp_scan_warps(hq[i].qlen, hq[i].diag_len, hq[i].n_entries, e->smem_optin);
     };
     std::vector<int32_t> order(n_queries);
     std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) { return bucket(x) > bucket(y); });
+    std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) {
+        return hq[x].diag_len != hq[y].diag_len ? hq[x].diag_len > hq[y].diag_len : hq[x].n_entries > hq[y].n_entries;
+    });
     std::vector<WorkItem> items;
     items.reserve((size_t)n_queries * n_chunks);
     std::vector<int32_t> item_pos((size_t)n_queries * n_chunks);   // caller's item index -> position
     for (size_t i = 0; i < order.size();) {
         bp_batch::Class k;
-        const int32_t cls = bucket(order[i]);
         k.item_lo = (int32_t)items.size();
-        for (; i < order.size() && bucket(order[i]) == cls; ++i) {
+        const int32_t q0 = order[i];
+        const bool defers = bp_scan_defers(hq[q0].qlen);
+        int warps = 0;
+        for (; i < order.size(); ++i) {
             const int32_t qi = order[i];
+            if (qi != q0) {
+                if (bp_scan_defers(hq[qi].qlen) != defers || own_warps(qi) != warps) break;
+                const int w = bp_scan_warps(std::max(k.max_qlen, hq[qi].qlen), std::max(k.max_len, hq[qi].diag_len),
+                                            std::max<int64_t>(k.max_entries, hq[qi].n_entries), e->smem_optin);
+                if (w != warps) break;
+            }
             k.max_len = std::max(k.max_len, hq[qi].diag_len);
             k.max_qlen = std::max(k.max_qlen, hq[qi].qlen);
             k.max_entries = std::max<int64_t>(k.max_entries, hq[qi].n_entries);
+            if (qi == q0) warps = own_warps(qi);
             k.est += queries[qi]->hits_per_residue;
             for (int32_t c = 0; c < n_chunks; ++c) {
                 item_pos[(size_t)qi * n_chunks + c] = (int32_t)items.size();

@@ -165,6 +165,10 @@ int bp_diag_len(int qlen, int window);
 // Whether the scan kernel can take a query (its diagonal array must fit
 // shared memory next to the table).
 bool bp_scan_fits(int32_t qlen, int32_t diag_len, int64_t n_entries, int smem_optin);
+// Warps per CTA the scan kernel runs with for such a query (0: does not fit),
+// and whether it queues its extensions (the launch's longest query decides).
+int bp_scan_warps(int32_t qlen, int32_t diag_len, int64_t n_entries, int smem_optin);
+bool bp_scan_defers(int32_t qlen);
 
 // ---- launchers ------------------------------------------------------------
 cudaError_t bp_launch_table_build(bp_engine* e, const uint8_t* d_q, int32_t qlen, int32_t threshold,

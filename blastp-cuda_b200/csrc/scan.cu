@@ -846,6 +846,13 @@ cudaError_t bp_launch_scan_batch(bp_engine* e, cudaStream_t stream, const BatchA
     return launch_batch<uint32_t, false, false>(e, stream, b, lay, grid);
 }
 
+int bp_scan_warps(int32_t qlen, int32_t diag_len, int64_t n_entries, int smem_optin) {
+    ScanLayout l;
+    return choose_layout(qlen, diag_len, n_entries, smem_optin, &l) ? l.warps : 0;
+}
+
+bool bp_scan_defers(int32_t qlen) { return qlen >= kDeferMinQlen; }
+
 bool bp_scan_fits(int32_t qlen, int32_t diag_len, int64_t n_entries, int smem_optin) {
     ScanLayout l;
     return choose_layout(qlen, diag_len, n_entries, smem_optin, &l);
