@@ -213,7 +213,8 @@ def run_batched(eng, matrix, args, torch):
            "residues": w.db.n_residues, "plain": {"ms": plain_ms, "value": work / (plain_ms / 1e3)}}
     model = costmodel.CostModel.load(eng)
     planted = 0.002
-    variants = {"static": dict(chunk_residues=1 << 20, schedule=SCHED_STATIC),
+    variants = {"unpacked_dynamic": dict(chunk_residues=1 << 20, schedule=SCHED_DYNAMIC, pack_residues=0),
+                "static": dict(chunk_residues=1 << 20, schedule=SCHED_STATIC),
                 "dynamic": dict(chunk_residues=1 << 20, schedule=SCHED_DYNAMIC),
                 "learned": dict(chunk_residues=1 << 20, schedule=SCHED_COSTS)}
     if args.batch_autotune:
@@ -222,8 +223,9 @@ def run_batched(eng, matrix, args, torch):
                                     sample_subjects=max(1, w.db.n_subjects // 16), reps=1)
         out["autotune"] = {"sample_subjects": max(1, w.db.n_subjects // 16), "seconds": time.perf_counter() - t0,
                            "best": dict(best, schedule=SCHED_NAMES[best["schedule"]]),
-                           "trials": [[t["chunk_residues"], SCHED_NAMES[t["schedule"]], t["max_warps"],
-                                       round(t["ms"], 3)] for t in trials]}
+                           "trials": [[t["chunk_residues"], t["pack_residues"], SCHED_NAMES[t["schedule"]],
+                                       t["max_warps"], round(t["ms"], 3)] for t in trials],
+                           "trial_fields": ["chunk_residues", "pack_residues", "schedule", "max_warps", "ms"]}
         variants["autotuned"] = dict(best)
     identical = True
     res = {}
@@ -242,6 +244,7 @@ def run_batched(eng, matrix, args, torch):
         ms = float(min(ms_runs))
         res[name] = {"ms": ms, "value": work / (ms / 1e3), "speedup_vs_plain": plain_ms / ms,
                      "chunk_residues": kw["chunk_residues"], "schedule": SCHED_NAMES[kw["schedule"]],
+                     "pack_residues": kw.get("pack_residues", 512),
                      "max_warps": kw.get("max_warps", 0), "items": b.n_items,
                      "launches_per_run": (eng.launches - launches0) // max(1, args.batch_reps)}
         if b.n_hsps != sum(plain_counts):

@@ -27,17 +27,20 @@ class BpParams(ctypes.Structure):
 
 class BpBatchOptions(ctypes.Structure):
     _fields_ = [("chunk_residues", i32), ("schedule", i32), ("ctas", i32), ("max_warps", i32),
-                ("use_graph", i32), ("item_costs", P), ("subject_first", i32), ("subject_count", i32)]
+                ("use_graph", i32), ("item_costs", P), ("subject_first", i32), ("subject_count", i32),
+                ("pack_residues", i32)]
 
 
 class BpAutotuneTrial(ctypes.Structure):
-    _fields_ = [("chunk_residues", i32), ("schedule", i32), ("max_warps", i32), ("ms", ctypes.c_float)]
+    _fields_ = [("chunk_residues", i32), ("schedule", i32), ("max_warps", i32), ("ms", ctypes.c_float),
+                ("pack_residues", i32)]
 
 
 class BpAutotuneOptions(ctypes.Structure):
     _fields_ = [("chunk_sizes", P), ("n_chunk_sizes", i32), ("warp_caps", P), ("n_warp_caps", i32),
                 ("schedules_mask", i32), ("model", P), ("cost_weights", ctypes.c_float * 3),
-                ("planted_density", ctypes.c_float), ("sample_subjects", i32), ("reps", i32)]
+                ("planted_density", ctypes.c_float), ("sample_subjects", i32), ("reps", i32),
+                ("pack_sizes", P), ("n_pack_sizes", i32)]
 
 
 class BpServerOptions(ctypes.Structure):

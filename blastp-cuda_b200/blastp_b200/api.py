@@ -102,7 +102,7 @@ class Engine:
 
     def search_batch(self, db: "Database", queries, chunk_residues: int = 1 << 18, schedule: int = 0,
                      ctas: int = 0, max_warps: int = 0, use_graph: bool = True, item_costs=None,
-                     first: int = 0, count: int = -1) -> "Batch":
+                     first: int = 0, count: int = -1, pack_residues: int = 512) -> "Batch":
         """Many queries against db in one persistent launch; each query's
         result equals its single-query search."""
         o = BpBatchOptions()
@@ -114,6 +114,7 @@ class Engine:
         o.use_graph = int(bool(use_graph))
         o.subject_first = first
         o.subject_count = count
+        o.pack_residues = pack_residues
         costs = None
         if item_costs is not None:
             costs = np.ascontiguousarray(item_costs, dtype=np.float32)
@@ -157,7 +158,7 @@ class Engine:
         return out
 
     def autotune(self, db: "Database", queries, model=None, planted_density: float = 0.0, sample_subjects: int = 0,
-                 chunk_sizes=None, warp_caps=None, schedules=(0, 1, 2), reps: int = 2):
+                 chunk_sizes=None, warp_caps=None, schedules=(0, 1, 2), reps: int = 2, pack_sizes=None):
         """Times candidate batch configurations on a sample of the subjects
         (bp_batch_autotune); returns (best options dict, list of trials)."""
         o = BpAutotuneOptions()
@@ -173,6 +174,11 @@ class Engine:
             keep.append(wc)
             o.warp_caps = wc.ctypes.data
             o.n_warp_caps = len(wc)
+        if pack_sizes is not None:
+            ps = np.ascontiguousarray(pack_sizes, dtype=np.int32)
+            keep.append(ps)
+            o.pack_sizes = ps.ctypes.data
+            o.n_pack_sizes = len(ps)
         o.schedules_mask = sum(1 << s for s in schedules)
         if model is not None:
             o.model = model.mlp.h.value
@@ -188,9 +194,9 @@ class Engine:
         check(lib().bp_batch_autotune(self.h, db.h, arr, len(queries), ctypes.byref(o), ctypes.byref(best), trials,
                                       256, ctypes.byref(nt)), self.h)
         out = [{"chunk_residues": t.chunk_residues, "schedule": t.schedule, "max_warps": t.max_warps,
-                "ms": float(t.ms)} for t in trials[:min(nt.value, 256)]]
-        return ({"chunk_residues": best.chunk_residues, "schedule": best.schedule, "max_warps": best.max_warps},
-                out)
+                "pack_residues": t.pack_residues, "ms": float(t.ms)} for t in trials[:min(nt.value, 256)]]
+        return ({"chunk_residues": best.chunk_residues, "schedule": best.schedule, "max_warps": best.max_warps,
+                 "pack_residues": best.pack_residues}, out)
 
     def blastp_host(self, query, params, residues, offsets, hsp_cap=None):
         """End-to-end: host buffers in, host buffers out (one C call)."""

@@ -67,6 +67,7 @@ struct bp_batch {
         int32_t queue_lo = 0;                  // its queue offsets start at d_queue_off[queue_lo]
         int32_t grid = 0;
         double est = 0;                        // expected word hits, to order the launches
+        bool packed = false;                   // its units are packed tables
     };
     std::vector<Class> classes;
     std::vector<cudaStream_t> side;          // one per class after the first
@@ -77,6 +78,8 @@ struct bp_batch {
     cudaGraphExec_t exec = nullptr;
     std::vector<double> queue_cost;         // predicted cost per CTA queue (cost schedules)
     std::vector<int32_t> item_queue;        // caller's item index -> queue (-1: dynamic)
+    std::vector<void*> pack_mem;            // device buffers of the packed tables
+    int32_t n_units = 0, n_packs = 0;
 };
 
 namespace {
@@ -158,7 +161,8 @@ bp_status enqueue(bp_batch* b) {
         a.rec_cap = b->cap;
         a.rec_count = b->d_counts;
         if (a.n_items > 0)
-            CKB(bp_launch_scan_batch(e, st, a, k.max_qlen, k.max_len, k.max_entries, k.grid, b->opt.max_warps),
+            CKB(bp_launch_scan_batch(e, st, a, k.max_qlen, k.max_len, k.max_entries, k.grid, b->opt.max_warps,
+                                     k.packed),
                 "batched scan launch");
         if (c > 0) {
             CKB(cudaEventRecord(b->ev_join[c - 1], st), "cudaEventRecord");
@@ -257,6 +261,83 @@ bp_status launch_batch(bp_batch* b) {
     return enqueue(b);
 }
 
+// Builds one packed table on the device: the members' residues end to end
+// with `window` offsets between them (so no two members' hits can meet on one
+// diagonal within the window), their tables merged cell by cell, the member
+// of every offset, and each member's {index, offset, length, x-drop, cutoff}.
+bp_status build_pack(bp_batch* b, const std::vector<BatchQuery>& hq, const bp_query* const* queries,
+                     const std::vector<int32_t>& g, int window, BatchQuery* out) {
+    bp_engine* e = b->e;
+    cudaStream_t es = e->stream;
+    std::vector<int32_t> members;
+    std::vector<PackSrc> src;
+    int32_t P = 0;
+    int64_t n_entries = 0;
+    for (size_t i = 0; i < g.size(); ++i) {
+        const bp_query* q = queries[g[i]];
+        if (i) P += window;
+        members.insert(members.end(), {g[i], P, q->qlen, q->p.x_dropoff, q->p.cutoff_score});
+        src.push_back(PackSrc{q->d_cells, q->d_entries, P, 0});
+        P += q->qlen;
+        n_entries += q->n_entries;
+    }
+    const int32_t L = bp_diag_len(P, window);
+    if (P > 65535 || n_entries >= (1LL << 31) || bp_scan_warps(P, L, n_entries, e->smem_optin, true) == 0)
+        return BP_ERR_TOO_LARGE;
+    std::vector<uint8_t> mof((size_t)P, 0xff);
+    for (size_t i = 0; i < g.size(); ++i)
+        memset(mof.data() + members[5 * i + 1], (int)i, (size_t)members[5 * i + 2]);
+    uint8_t* d_q = nullptr;
+    uint8_t* d_mof = nullptr;
+    uint32_t* d_cells = nullptr;
+    uint32_t* d_tmp = nullptr;
+    uint16_t* d_entries = nullptr;
+    int32_t* d_members = nullptr;
+    PackSrc* d_src = nullptr;
+    auto track = [&](void* p) { b->pack_mem.push_back(p); };
+    CKB(cudaMallocAsync((void**)&d_q, (size_t)((P + 15) & ~15) + 16, es), "cudaMallocAsync(pack)");
+    track(d_q);
+    CKB(cudaMallocAsync((void**)&d_mof, (size_t)P + 16, es), "cudaMallocAsync(pack)");
+    track(d_mof);
+    CKB(cudaMallocAsync((void**)&d_cells, (BP_NC + 1) * sizeof(uint32_t), es), "cudaMallocAsync(pack)");
+    track(d_cells);
+    CKB(cudaMallocAsync((void**)&d_tmp, BP_NC * sizeof(uint32_t), es), "cudaMallocAsync(pack)");
+    track(d_tmp);
+    CKB(cudaMallocAsync((void**)&d_entries, (size_t)std::max<int64_t>(n_entries, 1) * sizeof(uint16_t), es),
+        "cudaMallocAsync(pack)");
+    track(d_entries);
+    CKB(cudaMallocAsync((void**)&d_members, members.size() * sizeof(int32_t), es), "cudaMallocAsync(pack)");
+    track(d_members);
+    CKB(cudaMallocAsync((void**)&d_src, src.size() * sizeof(PackSrc), es), "cudaMallocAsync(pack)");
+    track(d_src);
+    CKB(cudaMemsetAsync(d_q, 0, (size_t)((P + 15) & ~15) + 16, es), "memset(pack)");
+    for (size_t i = 0; i < g.size(); ++i)
+        if (hq[g[i]].qlen > 0)
+            CKB(cudaMemcpyAsync(d_q + members[5 * i + 1], hq[g[i]].query, (size_t)hq[g[i]].qlen,
+                                cudaMemcpyDeviceToDevice, es),
+                "pack residues");
+    CKB(cudaMemcpyAsync(d_mof, mof.data(), (size_t)P, cudaMemcpyHostToDevice, es), "pack members");
+    CKB(cudaMemcpyAsync(d_members, members.data(), members.size() * sizeof(int32_t), cudaMemcpyHostToDevice, es),
+        "pack members");
+    CKB(cudaMemcpyAsync(d_src, src.data(), src.size() * sizeof(PackSrc), cudaMemcpyHostToDevice, es), "pack tables");
+    CKB(bp_launch_pack_table(e, es, d_src, (int)g.size(), d_tmp, d_cells, d_entries), "pack table launch");
+    BatchQuery u;
+    u.query = d_q;
+    u.cells = d_cells;
+    u.entries = d_entries;
+    u.ctx = nullptr;
+    u.qlen = P;
+    u.n_entries = (int32_t)n_entries;
+    u.n_ctx = 1;
+    u.diag_len = L;
+    u.members = d_members;
+    u.member_of = d_mof;
+    u.n_members = (int32_t)g.size();
+    u.seg_query = -1;
+    *out = u;
+    return BP_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -268,6 +349,7 @@ void bp_batch_options_default(bp_batch_options* o) {
     o->use_graph = 1;
     o->subject_first = 0;
     o->subject_count = -1;
+    o->pack_residues = 512;
 }
 
 bp_status bp_batch_plan(const bp_db* db, int32_t subject_first, int32_t subject_count, int32_t chunk_residues,
@@ -326,49 +408,104 @@ bp_status bp_search_batch(bp_engine* e, const bp_db* db, const bp_query* const* 
         hq[i].n_entries = (int32_t)q->n_entries;
         hq[i].n_ctx = q->n_ctx;
         hq[i].diag_len = q->diag_len;
+        hq[i].members = nullptr;
+        hq[i].member_of = nullptr;
+        hq[i].n_members = 0;
+        hq[i].seg_query = i;
         if (!bp_scan_fits(q->qlen, q->diag_len, q->n_entries, e->smem_optin)) {
             delete b;
             return bp_set_error(e, BP_ERR_TOO_LARGE, "bp_search_batch: a query is too long for the diagonal array");
         }
         hits_sum += q->hits_per_residue;
     }
-    // classes: a launch's layout is sized for its longest query, so queries
-    // share a launch only when that leaves each of them the warps per CTA it
-    // would get alone, and when they extend the same way; longest first
+    // units: short queries packed into shared tables, the others alone
+    std::vector<std::vector<int32_t>> unit_queries;
+    std::vector<BatchQuery> units;
+    {
+        const int32_t pmax = std::min(o.pack_residues, 65535);
+        std::vector<char> packed(n_queries, 0);
+        if (pmax > 0) {
+            std::vector<int32_t> cand;
+            for (int32_t i = 0; i < n_queries; ++i)
+                if (hq[i].qlen <= pmax / 2 && queries[i]->n_ctx == 1) cand.push_back(i);
+            std::stable_sort(cand.begin(), cand.end(), [&](int32_t x, int32_t y) { return hq[x].qlen < hq[y].qlen; });
+            std::vector<std::vector<int32_t>> groups;
+            int32_t P = 0;
+            for (int32_t qi : cand) {
+                const int32_t need = hq[qi].qlen + (groups.empty() || groups.back().empty() ? 0 : window);
+                if (groups.empty() || (int)groups.back().size() == BP_MAX_PACK_MEMBERS || P + need > pmax) {
+                    groups.emplace_back();
+                    P = 0;
+                }
+                P += hq[qi].qlen + (groups.back().empty() ? 0 : window);
+                groups.back().push_back(qi);
+            }
+            for (const auto& g : groups) {
+                if (g.size() < 2) continue;
+                BatchQuery u;
+                bp_status st = build_pack(b, hq, queries, g, window, &u);
+                if (st == BP_ERR_TOO_LARGE) continue;            // does not fit shared memory: leave unpacked
+                if (st != BP_OK) {
+                    bp_batch_destroy(b);
+                    return st;
+                }
+                for (int32_t qi : g) packed[qi] = 1;
+                units.push_back(u);
+                unit_queries.push_back(g);
+                b->n_packs += 1;
+            }
+        }
+        for (int32_t i = 0; i < n_queries; ++i)
+            if (!packed[i]) {
+                units.push_back(hq[i]);
+                unit_queries.push_back(std::vector<int32_t>(1, i));
+            }
+    }
+    const int32_t n_units = (int32_t)units.size();
+    b->n_units = n_units;
+    // classes: a launch's layout is sized for its longest unit, so units share
+    // a launch only when that leaves each of them the warps per CTA it would
+    // get alone, and when they extend the same way; longest first
     auto own_warps = [&](int32_t i) {
-        return bp_scan_warps(hq[i].qlen, hq[i].diag_len, hq[i].n_entries, e->smem_optin);
+        return bp_scan_warps(units[i].qlen, units[i].diag_len, units[i].n_entries, e->smem_optin,
+                             units[i].n_members > 0);
     };
-    std::vector<int32_t> order(n_queries);
+    std::vector<int32_t> order(n_units);
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) {
-        return hq[x].diag_len != hq[y].diag_len ? hq[x].diag_len > hq[y].diag_len : hq[x].n_entries > hq[y].n_entries;
+        const bool px = units[x].n_members > 0, py = units[y].n_members > 0;
+        if (px != py) return px;
+        return units[x].diag_len != units[y].diag_len ? units[x].diag_len > units[y].diag_len
+                                                       : units[x].n_entries > units[y].n_entries;
     });
     std::vector<WorkItem> items;
-    items.reserve((size_t)n_queries * n_chunks);
+    items.reserve((size_t)n_units * n_chunks);
     std::vector<int32_t> item_pos((size_t)n_queries * n_chunks);   // caller's item index -> position
     for (size_t i = 0; i < order.size();) {
         bp_batch::Class k;
         k.item_lo = (int32_t)items.size();
-        const int32_t q0 = order[i];
-        const bool defers = bp_scan_defers(hq[q0].qlen);
+        const int32_t u0 = order[i];
+        const bool defers = bp_scan_defers(units[u0].qlen);
+        k.packed = units[u0].n_members > 0;
         int warps = 0;
         for (; i < order.size(); ++i) {
-            const int32_t qi = order[i];
-            if (qi != q0) {
-                if (bp_scan_defers(hq[qi].qlen) != defers || own_warps(qi) != warps) break;
-                const int w = bp_scan_warps(std::max(k.max_qlen, hq[qi].qlen), std::max(k.max_len, hq[qi].diag_len),
-                                            std::max<int64_t>(k.max_entries, hq[qi].n_entries), e->smem_optin);
+            const int32_t ui = order[i];
+            const BatchQuery& u = units[ui];
+            if (ui != u0) {
+                if ((u.n_members > 0) != k.packed || bp_scan_defers(u.qlen) != defers || own_warps(ui) != warps) break;
+                const int w = bp_scan_warps(std::max(k.max_qlen, u.qlen), std::max(k.max_len, u.diag_len),
+                                            std::max<int64_t>(k.max_entries, u.n_entries), e->smem_optin, k.packed);
                 if (w != warps) break;
             }
-            k.max_len = std::max(k.max_len, hq[qi].diag_len);
-            k.max_qlen = std::max(k.max_qlen, hq[qi].qlen);
-            k.max_entries = std::max<int64_t>(k.max_entries, hq[qi].n_entries);
-            if (qi == q0) warps = own_warps(qi);
-            k.est += queries[qi]->hits_per_residue;
+            k.max_len = std::max(k.max_len, u.diag_len);
+            k.max_qlen = std::max(k.max_qlen, u.qlen);
+            k.max_entries = std::max<int64_t>(k.max_entries, u.n_entries);
+            if (ui == u0) warps = own_warps(ui);
+            for (int32_t qi : unit_queries[ui]) k.est += queries[qi]->hits_per_residue;
             for (int32_t c = 0; c < n_chunks; ++c) {
-                item_pos[(size_t)qi * n_chunks + c] = (int32_t)items.size();
+                for (int32_t qi : unit_queries[ui]) item_pos[(size_t)qi * n_chunks + c] = (int32_t)items.size();
                 WorkItem w;
-                w.qid = qi;
+                w.qid = ui;
                 w.first = b->chunk_first[c];
                 w.count = b->chunk_first[c + 1] - b->chunk_first[c];
                 w.pad = 0;
@@ -396,11 +533,12 @@ bp_status bp_search_batch(bp_engine* e, const bp_db* db, const bp_query* const* 
             // reloads a query's table only when the query changes
             std::vector<int32_t> loc(nk);
             std::iota(loc.begin(), loc.end(), 0);
-            std::vector<float> cost(nk);
+            std::vector<float> cost(nk, 0.f);
             for (int32_t qi = 0; qi < n_queries; ++qi)
                 for (int32_t c = 0; c < n_chunks; ++c) {
                     const int32_t pos = item_pos[(size_t)qi * n_chunks + c];
-                    if (pos >= k.item_lo && pos < k.item_hi) cost[pos - k.item_lo] = std::max(0.f, o.item_costs[(size_t)qi * n_chunks + c]);
+                    if (pos >= k.item_lo && pos < k.item_hi)   // a packed item costs its queries' sum
+                        cost[pos - k.item_lo] += std::max(0.f, o.item_costs[(size_t)qi * n_chunks + c]);
                 }
             std::stable_sort(loc.begin(), loc.end(), [&](int32_t x, int32_t y) { return cost[x] > cost[y]; });
             typedef std::pair<double, int> Load;
@@ -434,7 +572,7 @@ bp_status bp_search_batch(bp_engine* e, const bp_db* db, const bp_query* const* 
     const double span_res = (double)(db->h_off[s1] - db->h_off[s0]);
     b->cap = (uint32_t)std::min<double>(1 << 28, std::max(65536.0, 2.5e-4 * hits_sum * span_res));
     cudaStream_t es = e->stream;
-    cudaError_t err = cudaMallocAsync((void**)&b->d_queries, std::max<size_t>(1, hq.size()) * sizeof(BatchQuery), es);
+    cudaError_t err = cudaMallocAsync((void**)&b->d_queries, std::max<size_t>(1, units.size()) * sizeof(BatchQuery), es);
     if (err == cudaSuccess) err = cudaMallocAsync((void**)&b->d_items, std::max<size_t>(1, items.size()) * sizeof(WorkItem), es);
     if (err == cudaSuccess) err = cudaMallocAsync((void**)&b->d_queue_off, qoff.size() * sizeof(int32_t), es);
     if (err == cudaSuccess) err = cudaMallocAsync((void**)&b->d_queue_items, std::max<size_t>(1, qitems.size()) * sizeof(int32_t), es);
@@ -443,8 +581,8 @@ bp_status bp_search_batch(bp_engine* e, const bp_db* db, const bp_query* const* 
     if (err == cudaSuccess && !(b->h_count = bp_pinned_get(e))) err = cudaErrorMemoryAllocation;
     // the host tables are pageable: copy synchronously with respect to the host
     // (cudaMemcpyAsync from pageable memory returns once staged)
-    if (err == cudaSuccess && !hq.empty())
-        err = cudaMemcpyAsync(b->d_queries, hq.data(), hq.size() * sizeof(BatchQuery), cudaMemcpyHostToDevice, es);
+    if (err == cudaSuccess && !units.empty())
+        err = cudaMemcpyAsync(b->d_queries, units.data(), units.size() * sizeof(BatchQuery), cudaMemcpyHostToDevice, es);
     if (err == cudaSuccess && !items.empty())
         err = cudaMemcpyAsync(b->d_items, items.data(), items.size() * sizeof(WorkItem), cudaMemcpyHostToDevice, es);
     if (err == cudaSuccess)
@@ -553,6 +691,8 @@ void bp_batch_destroy(bp_batch* b) {
                     (void*)b->d_counters, (void*)b->d_hsp_off, (void*)b->d_hsps, (void*)b->d_keys, (void*)b->d_recs,
                     (void*)b->d_fill, (void*)b->d_blocksums, (void*)b->d_counts})
         if (p && e) cudaFreeAsync(p, e->stream);
+    for (void* p : b->pack_mem)
+        if (p && e) cudaFreeAsync(p, e->stream);
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
     if (b->ev_fork) cudaEventDestroy(b->ev_fork);
@@ -607,6 +747,7 @@ bp_status bp_batch_predict_costs(bp_engine* e, bp_mlp* model, const float* weigh
 
 void bp_autotune_options_default(bp_autotune_options* o) {
     memset(o, 0, sizeof(*o));
+    o->pack_sizes = nullptr;
     o->schedules_mask = (1 << BP_SCHED_DYNAMIC) | (1 << BP_SCHED_STATIC) | (1 << BP_SCHED_COSTS);
     o->reps = 2;
 }
@@ -624,67 +765,91 @@ bp_status bp_batch_autotune(bp_engine* e, const bp_db* db, const bp_query* const
     else bp_autotune_options_default(&o);
     static const int32_t kChunks[] = {1 << 16, 1 << 18, 1 << 20, 1 << 22};
     static const int32_t kWarps[] = {0, 16};
+    static const int32_t kPacks[] = {0, 512, 1024};
     const int32_t* chunks = o.chunk_sizes ? o.chunk_sizes : kChunks;
     const int n_chunk_sizes = o.chunk_sizes ? o.n_chunk_sizes : 4;
     const int32_t* warps = o.warp_caps ? o.warp_caps : kWarps;
     const int n_warp_caps = o.warp_caps ? o.n_warp_caps : 2;
+    const int32_t* packs = o.pack_sizes ? o.pack_sizes : kPacks;
+    const int n_pack_sizes = o.pack_sizes ? o.n_pack_sizes : 3;
     const int32_t sample = o.sample_subjects > 0 ? std::min(o.sample_subjects, db->n) : std::max(1, db->n / 16);
     const int reps = std::max(1, o.reps);
     bp_batch_options_default(best);
     float best_ms = 1e30f;
     int32_t nt = 0;
-    for (int ci = 0; ci < n_chunk_sizes; ++ci) {
-        std::vector<float> costs;
-        for (int sched = 0; sched < 3; ++sched) {
-            if (!(o.schedules_mask & (1 << sched))) continue;
-            if (sched == BP_SCHED_COSTS) {
-                if (!o.model) continue;
-                if (costs.empty()) {
-                    std::vector<int32_t> first;
-                    plan_chunks(db, 0, sample, chunks[ci], first);
-                    costs.resize((size_t)n_queries * (first.size() - 1));
-                    bp_status st = bp_batch_predict_costs(e, o.model, o.cost_weights, db, queries, n_queries,
-                                                          first.data(), (int32_t)first.size() - 1,
-                                                          o.planted_density, costs.data());
-                    if (st != BP_OK) return st;
-                }
-            }
-            for (int wi = 0; wi < n_warp_caps; ++wi) {
-                bp_batch_options bo;
-                bp_batch_options_default(&bo);
-                bo.chunk_residues = chunks[ci];
-                bo.schedule = sched;
-                bo.max_warps = warps[wi];
-                bo.item_costs = sched == BP_SCHED_COSTS ? costs.data() : nullptr;
-                bo.subject_first = 0;
-                bo.subject_count = sample;
-                bp_batch* b = nullptr;
-                bp_status st = bp_search_batch(e, db, queries, n_queries, &bo, &b);
-                if (st == BP_OK) st = bp_batch_wait(b);
-                float ms = 1e30f;
-                for (int r = 0; r < reps && st == BP_OK; ++r) {
-                    st = bp_batch_run(b);
-                    if (st == BP_OK) st = bp_batch_wait(b);
-                    if (st == BP_OK) ms = std::min(ms, b->last_ms);
-                }
-                bp_batch_destroy(b);
+    std::vector<float> costs;
+    int32_t costs_chunk = -1;
+    auto trial = [&](int32_t chunk, int32_t pack, int sched, int32_t max_warps) -> bp_status {
+        bp_batch_options bo;
+        bp_batch_options_default(&bo);
+        bo.chunk_residues = chunk;
+        bo.pack_residues = pack;
+        bo.schedule = sched;
+        bo.max_warps = max_warps;
+        bo.subject_first = 0;
+        bo.subject_count = sample;
+        if (sched == BP_SCHED_COSTS) {
+            if (costs_chunk != chunk) {
+                std::vector<int32_t> first;
+                plan_chunks(db, 0, sample, chunk, first);
+                costs.assign((size_t)n_queries * (first.size() - 1), 0.f);
+                bp_status st = bp_batch_predict_costs(e, o.model, o.cost_weights, db, queries, n_queries,
+                                                      first.data(), (int32_t)first.size() - 1, o.planted_density,
+                                                      costs.data());
                 if (st != BP_OK) return st;
-                if (trials && nt < trials_cap) {
-                    trials[nt].chunk_residues = bo.chunk_residues;
-                    trials[nt].schedule = bo.schedule;
-                    trials[nt].max_warps = bo.max_warps;
-                    trials[nt].ms = ms;
-                }
-                ++nt;
-                if (ms < best_ms) {
-                    best_ms = ms;
-                    *best = bo;
-                    best->item_costs = nullptr;
-                    best->subject_first = 0;
-                    best->subject_count = -1;
-                }
+                costs_chunk = chunk;
             }
+            bo.item_costs = costs.data();
         }
+        bp_batch* b = nullptr;
+        bp_status st = bp_search_batch(e, db, queries, n_queries, &bo, &b);
+        if (st == BP_OK) st = bp_batch_wait(b);
+        float ms = 1e30f;
+        for (int r = 0; r < reps && st == BP_OK; ++r) {
+            st = bp_batch_run(b);
+            if (st == BP_OK) st = bp_batch_wait(b);
+            if (st == BP_OK) ms = std::min(ms, b->last_ms);
+        }
+        bp_batch_destroy(b);
+        if (st != BP_OK) return st;
+        if (trials && nt < trials_cap) {
+            trials[nt].chunk_residues = chunk;
+            trials[nt].schedule = sched;
+            trials[nt].max_warps = max_warps;
+            trials[nt].ms = ms;
+            trials[nt].pack_residues = pack;
+        }
+        ++nt;
+        if (ms < best_ms) {
+            best_ms = ms;
+            *best = bo;
+            best->item_costs = nullptr;
+            best->subject_first = 0;
+            best->subject_count = -1;
+        }
+        return BP_OK;
+    };
+    // stage 1: chunk size x packing, dynamic schedule, all warps
+    const int sched0 = (o.schedules_mask & (1 << BP_SCHED_DYNAMIC)) ? BP_SCHED_DYNAMIC
+                       : (o.schedules_mask & (1 << BP_SCHED_STATIC)) ? BP_SCHED_STATIC : BP_SCHED_COSTS;
+    if (sched0 == BP_SCHED_COSTS && !o.model) return bp_set_error(e, BP_ERR_INVALID, "bp_batch_autotune: no schedule");
+    for (int ci = 0; ci < n_chunk_sizes; ++ci)
+        for (int pi = 0; pi < n_pack_sizes; ++pi) {
+            bp_status st = trial(chunks[ci], packs[pi], sched0, 0);
+            if (st != BP_OK) return st;
+        }
+    // stage 2: the other schedules, then the warp caps, at the best chunk and packing
+    const int32_t chunk = best->chunk_residues, pack = best->pack_residues;
+    for (int sched = 0; sched < 3; ++sched) {
+        if (sched == sched0 || !(o.schedules_mask & (1 << sched)) || (sched == BP_SCHED_COSTS && !o.model)) continue;
+        bp_status st = trial(chunk, pack, sched, 0);
+        if (st != BP_OK) return st;
+    }
+    const int sched = best->schedule;
+    for (int wi = 0; wi < n_warp_caps; ++wi) {
+        if (warps[wi] == 0) continue;
+        bp_status st = trial(chunk, pack, sched, warps[wi]);
+        if (st != BP_OK) return st;
     }
     if (n_trials) *n_trials = nt;
     return BP_OK;

@@ -14,6 +14,7 @@
 #define BP_NC 19683             // compact layout: 27^3 words of letters 1..27
 #define BP_WORD 3
 #define BP_MROW 32              // device matrix row stride (28 used)
+#define BP_MAX_PACK_MEMBERS 32  // queries per packed table
 
 // One reported HSP before ordering: owning subject (relative to the search's
 // first subject), its discovery key (index of the triggering word hit in the
@@ -114,15 +115,28 @@ struct ScanArgs {
     uint32_t* rec_count;
     uint32_t* cursor;           // subject cursor (chunks of 32)
     uint32_t* error;            // set when a bounded wait runs out
+    // packed tables (batched kernel): per query {id, offset, length, x-drop,
+    // cutoff}, the query of every packed offset, and the segment stride
+    const int32_t* members;
+    const uint8_t* member_of;
+    int32_t n_members;
+    int32_t seg_stride;
 };
 
 // Batched form: one query of a batch, one work item, and the launch arguments.
+// A unit of a batch: one query (seg_query = its index in the batch), or a
+// packed table of several short queries laid end to end with `window`
+// offsets between them (members: 5 int32 per query {index, offset, length,
+// x-drop, cutoff}; member_of: the member of every packed offset).
 struct BatchQuery {
     const uint8_t* query;
     const uint32_t* cells;
     const uint16_t* entries;
     const int32_t* ctx;
     int32_t qlen, n_entries, n_ctx, diag_len;
+    const int32_t* members;
+    const uint8_t* member_of;
+    int32_t n_members, seg_query;
 };
 struct WorkItem {
     int32_t qid;            // query of the batch
@@ -167,7 +181,7 @@ int bp_diag_len(int qlen, int window);
 bool bp_scan_fits(int32_t qlen, int32_t diag_len, int64_t n_entries, int smem_optin);
 // Warps per CTA the scan kernel runs with for such a query (0: does not fit),
 // and whether it queues its extensions (the launch's longest query decides).
-int bp_scan_warps(int32_t qlen, int32_t diag_len, int64_t n_entries, int smem_optin);
+int bp_scan_warps(int32_t qlen, int32_t diag_len, int64_t n_entries, int smem_optin, bool packed);
 bool bp_scan_defers(int32_t qlen);
 
 // ---- launchers ------------------------------------------------------------
@@ -175,7 +189,18 @@ cudaError_t bp_launch_table_build(bp_engine* e, const uint8_t* d_q, int32_t qlen
                                   uint32_t* d_cells, uint16_t* d_entries, uint32_t* d_counts_tmp, int pass);
 cudaError_t bp_launch_scan(bp_engine* e, const ScanArgs& a);
 cudaError_t bp_launch_scan_batch(bp_engine* e, cudaStream_t stream, const BatchArgs& b, int32_t max_qlen,
-                                 int32_t max_diag_len, int64_t max_entries, int grid, int max_warps);
+                                 int32_t max_diag_len, int64_t max_entries, int grid, int max_warps, bool packed);
+// Packed table of several queries: cells = sum of the members' cells,
+// entries = each cell's member entries in member order, shifted by the
+// member's offset (d_src: one PackSrc per member, device memory).
+struct PackSrc {
+    const uint32_t* cells;
+    const uint16_t* entries;
+    int32_t off;
+    int32_t pad;
+};
+cudaError_t bp_launch_pack_table(bp_engine* e, cudaStream_t stream, const PackSrc* d_src, int n_members,
+                                 uint32_t* d_counts_tmp, uint32_t* d_cells, uint16_t* d_entries);
 cudaError_t bp_launch_order(bp_engine* e, int32_t n, const int32_t* d_counters, int64_t* d_hsp_off,
                             const HspRec* d_recs, uint32_t rec_cap, const uint32_t* d_rec_count,
                             int32_t* d_fill, bp_hsp* d_out, int32_t* d_keys, int64_t* d_blocksums);

@@ -55,6 +55,7 @@ constexpr int kLaneWalkMin = 6;             // from this many queued extensions 
 // have too few extensions per subject for one-lane-per-extension walks to pay
 // for the queue, and extend each pair at once with the whole warp.
 constexpr int kDeferMinQlen = 320;
+constexpr int kMaxMembers = 32;             // queries per packed table (BP_MAX_PACK_MEMBERS)
 
 }  // namespace
 
@@ -64,8 +65,9 @@ struct ScanLayout {
     int cells_mode;        // 0: u16 starts in smem, 1: u32 starts in smem, 2: u32 starts in global
     int entries_smem;
     int L;                 // diagonal entries per warp (the longest query's)
-    int off_cells, off_entries, off_query, off_warps, off_ctl;
+    int off_cells, off_entries, off_query, off_members, off_mof, off_warps, off_ctl;
     int warp_bytes;        // diagonal array + per-lane position table + task queue + blocked list
+                           // (+ per-member counters when packed)
     int total;
 };
 
@@ -182,13 +184,14 @@ __device__ __forceinline__ void lane_xdrop(const int8_t* m, const uint8_t* __res
 
 // s_BlastAaExtendTwoHit (gpu_blastp_kernel.cu:341-415): the word-start shift,
 // the left walk, which must reach s_left for the right walk to run, and the
-// right walk starting from the left score.  kWarp: every lane passes the
+// right walk starting from the left score.  The walks stay within query
+// offsets [q_lo, q_hi): the whole query, or one query of a packed table.  kWarp: every lane passes the
 // same arguments, the walks use the whole warp and every lane gets the
 // result; otherwise each lane extends its own hit pair.
 template <bool kWarp>
 __device__ __forceinline__ ExtOut extend_two_hit(const int8_t* m, const uint8_t* __restrict__ subj, int slen,
-                                                 const uint8_t* qry, int qlen, int s_left, int s_right, int q_right,
-                                                 int xdrop, int lane) {
+                                                 const uint8_t* qry, int q_lo, int q_hi, int s_left, int s_right,
+                                                 int q_right, int xdrop, int lane) {
     int score = 0, left_score = 0, shift = 0;
 #pragma unroll
     for (int i = 0; i < BP_WORD; ++i) {
@@ -202,7 +205,7 @@ __device__ __forceinline__ ExtOut extend_two_hit(const int8_t* m, const uint8_t*
     s_right += shift;
 
     int lbest, lbest_k, lstop;
-    const int nl = min(s_right, q_right);
+    const int nl = min(s_right, q_right - q_lo);
     if (kWarp) warp_xdrop<false>(m, subj, qry, s_right - 1, q_right - 1, nl, 0, xdrop, lane, lbest, lbest_k, lstop);
     else lane_xdrop<false>(m, subj, qry, s_right - 1, q_right - 1, nl, 0, xdrop, lbest, lbest_k, lstop);
     const int left_d = lbest_k + 1;
@@ -214,7 +217,7 @@ __device__ __forceinline__ ExtOut extend_two_hit(const int8_t* m, const uint8_t*
     int right_d = 0, right_score = 0;
     if (left_d >= s_right - s_left) {
         o.right_ext = 1;
-        const int nr = min(slen - s_right, qlen - q_right);
+        const int nr = min(slen - s_right, q_hi - q_right);
         int rbest, rbest_i, rstop;
         if (kWarp) warp_xdrop<true>(m, subj, qry, s_right, q_right, nr, left_score, xdrop, lane, rbest, rbest_i, rstop);
         else lane_xdrop<true>(m, subj, qry, s_right, q_right, nr, left_score, xdrop, rbest, rbest_i, rstop);
@@ -259,13 +262,44 @@ struct WarpScan {
     Task* tasks;
     Task* blocked;
     const uint8_t* sub;
-    int slen, oid, base, lane;
+    int slen, oid, base, lane;   // oid: the subject's segment (packed: its index in the batch's range)
     unsigned lt;
     int nt, nb;            // queued tasks and blocked hits (warp-uniform)
     int ext, succ;         // this lane's share of the subject's counters
+    int* wcnt;             // packed: per-member hits, successes, extensions (shared memory)
 };
 
-// Appends the reported HSPs of this round (one candidate per lane).
+// The query an offset belongs to: its bounds, x-drop and cutoff.  Packed
+// tables look the member up in the offset-to-member table; otherwise the
+// context is the last one starting at or before the offset.
+struct Member {
+    int k, q_lo, q_hi, xdrop, cutoff;
+};
+
+template <bool kPacked>
+__device__ __forceinline__ Member member_at(const WarpScan& w, int hq) {
+    const ScanArgs& a = *w.a;
+    Member r;
+    if (kPacked) {
+        r.k = a.member_of[hq];
+        const int32_t* mm = a.members + 5 * r.k;
+        r.q_lo = mm[1];
+        r.q_hi = mm[1] + mm[2];
+        r.xdrop = mm[3];
+        r.cutoff = mm[4];
+    } else {
+        r.k = a.n_ctx == 1 ? 0 : context_of(a.ctx, a.n_ctx, hq);
+        r.q_lo = 0;
+        r.q_hi = a.qlen;
+        r.xdrop = __ldg(a.ctx + 3 * r.k + 1);
+        r.cutoff = __ldg(a.ctx + 3 * r.k + 2);
+    }
+    return r;
+}
+
+// Appends the reported HSPs of this round (one candidate per lane).  Packed:
+// the record goes to its query's segment, with query offsets relative to it.
+template <bool kPacked>
 __device__ __forceinline__ void emit(WarpScan& w, bool found, int key, int hs, int hq, const ExtOut& x) {
     const unsigned fm = __ballot_sync(kFull, found);
     if (!fm) return;
@@ -273,20 +307,28 @@ __device__ __forceinline__ void emit(WarpScan& w, bool found, int key, int hs, i
     if (w.lane == 0) pos0 = atomicAdd(w.a->rec_count, (uint32_t)__popc(fm));
     pos0 = __shfl_sync(kFull, pos0, 0);
     if (found) {
+        int seg = w.oid, q0 = 0;
+        if (kPacked) {
+            const int k = w.a->member_of[hq];
+            seg = w.a->members[5 * k] * w.a->seg_stride + w.oid;
+            q0 = w.a->members[5 * k + 1];
+            atomicAdd(&w.wcnt[3 * k + 1], 1);
+        } else {
+            ++w.succ;
+        }
         const uint32_t pos = pos0 + (uint32_t)__popc(fm & w.lt);
         if (pos < w.a->rec_cap) {
             HspRec rec;
-            rec.oid = w.oid;
+            rec.oid = seg;
             rec.key = key;
-            rec.h.hsp_q = x.hsp_q;
+            rec.h.hsp_q = x.hsp_q - q0;
             rec.h.hsp_s = x.hsp_s;
-            rec.h.query_offset = hq;
+            rec.h.query_offset = hq - q0;
             rec.h.subject_offset = hs;
             rec.h.hsp_len = x.len;
             rec.h.score = x.score;
             w.a->recs[pos] = rec;
         }
-        ++w.succ;
     }
 }
 
@@ -300,10 +342,11 @@ __device__ __forceinline__ uint32_t diag_after(const ExtOut& x, int hs, int base
 // pending, and a hit on a pending diagonal joins the blocked list (needs room
 // for 32 more tasks and 32 more blocked hits).  Otherwise each pair is
 // extended at once by the whole warp, one after the other.
-template <bool kDefer>
-__device__ __forceinline__ void apply_hits(WarpScan& w, bool hv, int hs, int hq, int d, int key) {
+template <bool kDefer, bool kPacked>
+__device__ __forceinline__ void apply_hits(WarpScan& w, bool hv, int hs, int hq, int d, int key, bool count) {
     const unsigned vmask = __ballot_sync(kFull, hv);
     if (!vmask) return;
+    if (kPacked && count && hv) atomicAdd(&w.wcnt[3 * w.a->member_of[hq]], 1);   // word hits per query
     unsigned peers = 0;
     if (hv) peers = __match_any_sync(vmask, d);
     bool pending = hv, found = false;
@@ -337,7 +380,8 @@ __device__ __forceinline__ void apply_hits(WarpScan& w, bool hv, int hs, int hq,
             if (need) {
                 w.tasks[w.nt + __popc(nm & w.lt)] = Task{hs, key, d, (uint32_t)hq | ((uint32_t)diff << 16)};
                 w.diag[d] = kPend | (uint32_t)(hs + w.base);
-                ++w.ext;
+                if (kPacked) atomicAdd(&w.wcnt[3 * w.a->member_of[hq] + 2], 1);
+                else ++w.ext;
             }
             w.nt += __popc(nm);
         } else {
@@ -349,14 +393,14 @@ __device__ __forceinline__ void apply_hits(WarpScan& w, bool hv, int hs, int hq,
                 const int e_s = __shfl_sync(kFull, hs, leader);
                 const int e_q = __shfl_sync(kFull, hq, leader);
                 const int e_diff = __shfl_sync(kFull, diff, leader);
-                const ScanArgs& a = *w.a;
-                const int k = a.n_ctx == 1 ? 0 : context_of(a.ctx, a.n_ctx, e_q);
-                const ExtOut x = extend_two_hit<true>(w.m, w.sub, w.slen, w.qs, a.qlen, e_s - e_diff + BP_WORD, e_s,
-                                                      e_q, __ldg(a.ctx + 3 * k + 1), w.lane);
+                const Member mb = member_at<kPacked>(w, e_q);
+                const ExtOut x = extend_two_hit<true>(w.m, w.sub, w.slen, w.qs, mb.q_lo, mb.q_hi,
+                                                      e_s - e_diff + BP_WORD, e_s, e_q, mb.xdrop, w.lane);
                 if (w.lane == leader) {
                     res = x;
-                    ++w.ext;
-                    found = x.score >= __ldg(a.ctx + 3 * k + 2);
+                    if (kPacked) atomicAdd(&w.wcnt[3 * mb.k + 2], 1);
+                    else ++w.ext;
+                    found = x.score >= mb.cutoff;
                     w.diag[d] = x.right_ext ? ((uint32_t)(x.s_last - (BP_WORD - 1) + w.base) | kFlag)
                                             : (uint32_t)(hs + w.base);
                 }
@@ -364,12 +408,12 @@ __device__ __forceinline__ void apply_hits(WarpScan& w, bool hv, int hs, int hq,
             __syncwarp();
         }
     }
-    if (!kDefer) emit(w, found, key, hs, hq, res);
+    if (!kDefer) emit<kPacked>(w, found, key, hs, hq, res);
 }
 
 // Walks every queued extension and writes its outcome into its diagonal.
+template <bool kPacked>
 __device__ void flush_tasks(WarpScan& w) {
-    const ScanArgs& a = *w.a;
     const int nt = w.nt;
     if (nt >= kLaneWalkMin) {
         for (int t0 = 0; t0 < nt; t0 += 32) {
@@ -380,24 +424,24 @@ __device__ void flush_tasks(WarpScan& w) {
             if (t < nt) {
                 tk = w.tasks[t];
                 const int hq = (int)(tk.hqx & 0xffffu), diff = (int)(tk.hqx >> 16);
-                const int k = a.n_ctx == 1 ? 0 : context_of(a.ctx, a.n_ctx, hq);
-                x = extend_two_hit<false>(w.m, w.sub, w.slen, w.qs, a.qlen, tk.hs - diff + BP_WORD, tk.hs, hq,
-                                          __ldg(a.ctx + 3 * k + 1), w.lane);
-                found = x.score >= __ldg(a.ctx + 3 * k + 2);
+                const Member mb = member_at<kPacked>(w, hq);
+                x = extend_two_hit<false>(w.m, w.sub, w.slen, w.qs, mb.q_lo, mb.q_hi, tk.hs - diff + BP_WORD, tk.hs,
+                                          hq, mb.xdrop, w.lane);
+                found = x.score >= mb.cutoff;
                 w.diag[tk.d] = diag_after(x, tk.hs, w.base);
             }
-            emit(w, found, tk.key, tk.hs, (int)(tk.hqx & 0xffffu), x);
+            emit<kPacked>(w, found, tk.key, tk.hs, (int)(tk.hqx & 0xffffu), x);
         }
     } else {
         for (int t = 0; t < nt; ++t) {
             const Task tk = w.tasks[t];
             const int hq = (int)(tk.hqx & 0xffffu), diff = (int)(tk.hqx >> 16);
-            const int k = a.n_ctx == 1 ? 0 : context_of(a.ctx, a.n_ctx, hq);
-            const ExtOut x = extend_two_hit<true>(w.m, w.sub, w.slen, w.qs, a.qlen, tk.hs - diff + BP_WORD, tk.hs,
-                                                  hq, __ldg(a.ctx + 3 * k + 1), w.lane);
-            const bool found = w.lane == 0 && x.score >= __ldg(a.ctx + 3 * k + 2);
+            const Member mb = member_at<kPacked>(w, hq);
+            const ExtOut x = extend_two_hit<true>(w.m, w.sub, w.slen, w.qs, mb.q_lo, mb.q_hi, tk.hs - diff + BP_WORD,
+                                                  tk.hs, hq, mb.xdrop, w.lane);
+            const bool found = w.lane == 0 && x.score >= mb.cutoff;
             if (w.lane == 0) w.diag[tk.d] = diag_after(x, tk.hs, w.base);
-            emit(w, found, tk.key, tk.hs, hq, x);
+            emit<kPacked>(w, found, tk.key, tk.hs, hq, x);
         }
     }
     __syncwarp();
@@ -407,8 +451,9 @@ __device__ void flush_tasks(WarpScan& w) {
 // Resolves the queued extensions, then replays the blocked hits once, in
 // order.  A replayed hit may queue a new extension (and block the hits after
 // it on its diagonal again); the blocked list is rewritten in place.
+template <bool kPacked>
 __device__ void resolve(WarpScan& w) {
-    flush_tasks(w);
+    flush_tasks<kPacked>(w);
     const int n = w.nb;
     w.nb = 0;
     for (int r = 0; r < n; r += 32) {
@@ -417,15 +462,18 @@ __device__ void resolve(WarpScan& w) {
         Task b{0, 0, 0, 0};
         if (hv) b = w.blocked[i];
         __syncwarp();
-        apply_hits<true>(w, hv, b.hs, (int)(b.hqx & 0xffffu), b.d, b.key);
+        apply_hits<true, kPacked>(w, hv, b.hs, (int)(b.hqx & 0xffffu), b.d, b.key, false);
     }
     __syncwarp();
 }
 
-template <typename CellT, bool kDefer>
+// Scans one subject.  oid: the subject's counter/record segment; packed: its
+// index in the batch's subject range (each query's segment is derived).
+template <typename CellT, bool kDefer, bool kPacked>
 __device__ void scan_subject(const ScanArgs& a, const int8_t* m, const uint8_t* qs, const CellT* cells,
                              const uint16_t* entries, uint32_t* diag, uint32_t* lane_pos, Task* tasks,
-                             Task* blocked, int oid, const uint8_t* __restrict__ sub, int slen, int& base, int lane) {
+                             Task* blocked, int* wcnt, int oid, const uint8_t* __restrict__ sub, int slen, int& base,
+                             int lane) {
     const int L = a.diag_len;
     if (base + slen + a.window > (1 << 30)) {
         for (int i = lane; i < L; i += 32) diag[i] = 0;
@@ -447,6 +495,11 @@ __device__ void scan_subject(const ScanArgs& a, const int8_t* m, const uint8_t* 
     w.lt = (1u << lane) - 1u;
     w.nt = w.nb = 0;
     w.ext = w.succ = 0;
+    w.wcnt = wcnt;
+    if (kPacked) {
+        for (int i = lane; i < 3 * a.n_members; i += 32) wcnt[i] = 0;
+        __syncwarp();
+    }
     int hits = 0, key_base = 0;
     int s0m = 0;                         // s0 mod L
     const int last_pos = slen - BP_WORD;
@@ -476,7 +529,7 @@ __device__ void scan_subject(const ScanArgs& a, const int8_t* m, const uint8_t* 
         __syncwarp();
         for (uint32_t hb = 0; hb < total; hb += 32) {
             if (kDefer)
-                while (w.nt > kTaskCap - 32 || w.nb > kBlkCap - 32) resolve(w);
+                while (w.nt > kTaskCap - 32 || w.nb > kBlkCap - 32) resolve<kPacked>(w);
             const uint32_t j = hb + lane;
             const bool hv = j < total;
             // owner lane: first lane whose inclusive prefix exceeds j
@@ -504,7 +557,7 @@ __device__ void scan_subject(const ScanArgs& a, const int8_t* m, const uint8_t* 
                 d = hq - hm;
                 if (d < 0) d += L;
             }
-            apply_hits<kDefer>(w, hv, hs, hq, d, key_base + (int)j);
+            apply_hits<kDefer, kPacked>(w, hv, hs, hq, d, key_base + (int)j, true);
         }
         key_base += (int)total;
         s0m += 32 * kP;
@@ -514,7 +567,20 @@ __device__ void scan_subject(const ScanArgs& a, const int8_t* m, const uint8_t* 
         for (int i = 0; i < kP + 2; ++i) r[i] = rn[i];
     }
     if (kDefer)
-        while (w.nt > 0 || w.nb > 0) resolve(w);
+        while (w.nt > 0 || w.nb > 0) resolve<kPacked>(w);
+    if (kPacked) {
+        // every query of the packed table gets its own counters for this subject
+        __syncwarp();
+        for (int k = lane; k < a.n_members; k += 32) {
+            const int64_t seg = (int64_t)a.members[5 * k] * a.seg_stride + oid;
+            a.counters[3 * seg + 0] = wcnt[3 * k + 0];
+            a.counters[3 * seg + 1] = wcnt[3 * k + 1];
+            a.counters[3 * seg + 2] = wcnt[3 * k + 2];
+        }
+        __syncwarp();
+        base += slen + a.window;
+        return;
+    }
     int ext = w.ext, succ = w.succ;
 #pragma unroll
     for (int o = 16; o >= 1; o >>= 1) {
@@ -530,12 +596,14 @@ __device__ void scan_subject(const ScanArgs& a, const int8_t* m, const uint8_t* 
     base += slen + a.window;
 }
 
-// Per-warp regions: diagonal array, lane position table, task queue, blocked list.
+// Per-warp regions: diagonal array, lane position table, task queue, blocked
+// list, and (packed layouts) per-member counters.
 struct WarpRegions {
     uint32_t* diag;
     uint32_t* lane_pos;
     Task* tasks;
     Task* blocked;
+    int* wcnt;
 };
 
 __device__ __forceinline__ WarpRegions warp_regions(const ScanLayout& lay, int warp, int lane) {
@@ -545,6 +613,7 @@ __device__ __forceinline__ WarpRegions warp_regions(const ScanLayout& lay, int w
     r.lane_pos = reinterpret_cast<uint32_t*>(wr + (size_t)lay.L * 4) + lane * kP * 2;
     r.tasks = reinterpret_cast<Task*>(wr + (size_t)lay.L * 4 + 32 * kP * 2 * 4);
     r.blocked = r.tasks + kTaskCap;
+    r.wcnt = reinterpret_cast<int*>(r.blocked + kBlkCap);
     return r;
 }
 
@@ -608,8 +677,8 @@ scan_kernel(ScanArgs a, ScanLayout lay) {
             }
             oid3 = (int)atomicAdd(a.cursor, 1u);
         }
-        scan_subject<CellT, kDefer>(a, m, qs, cells, entries, wr.diag, wr.lane_pos, wr.tasks, wr.blocked, cur,
-                                    a.db + cs, (int)(ce - cs), base, lane);
+        scan_subject<CellT, kDefer, false>(a, m, qs, cells, entries, wr.diag, wr.lane_pos, wr.tasks, wr.blocked,
+                                           wr.wcnt, cur, a.db + cs, (int)(ce - cs), base, lane);
         int nxt = 0;
         long long ns = 0, ne = 0;
         if (lane == 0) {
@@ -635,14 +704,15 @@ struct BatchCtl {
 };
 
 // Batched form: many queries against one resident database in one launch.
-// Work items are (query, subject chunk) pairs; a CTA takes items from its own
-// queue (per-CTA schedule) or from a global cursor, loads a query's table
-// into shared memory only when the query changes, prefetches the chunk's
+// Work items are (unit, subject chunk) pairs, a unit being one query or (kPacked)
+// a packed table of several short queries; a CTA takes items from its own
+// queue (per-CTA schedule) or from a global cursor, loads a unit's table
+// into shared memory only when the unit changes, prefetches the chunk's
 // residues into L2, and its warps share the chunk's subjects.  Each
-// (query, subject) pair is scanned by scan_subject exactly as in the
-// single-query kernel, so every query's result is the single-query result;
-// counters and records are indexed by segment = query * n_subjects + subject.
-template <typename CellT, bool kCellsSmem, bool kDefer>
+// (query, subject) pair sees exactly the plain kernel's sequence of events,
+// so every query's result is its single-query result; counters and records
+// are indexed by segment = query * n_subjects + subject.
+template <typename CellT, bool kCellsSmem, bool kDefer, bool kPacked>
 __global__ void __launch_bounds__(kMaxWarps * 32, 1)
 scan_batch_kernel(BatchArgs b, ScanLayout lay) {
     uint8_t* sm = bp_smem;
@@ -695,8 +765,18 @@ scan_batch_kernel(BatchArgs b, ScanLayout lay) {
             } else {
                 entries = bq.entries;
             }
+            if (kPacked) {
+                int32_t* mm = reinterpret_cast<int32_t*>(sm + lay.off_members);
+                for (int i = threadIdx.x; i < 5 * bq.n_members; i += blockDim.x) mm[i] = bq.members[i];
+                uint8_t* mof = sm + lay.off_mof;
+                for (int i = threadIdx.x; i < bq.qlen; i += blockDim.x) mof[i] = bq.member_of[i];
+            }
             if (threadIdx.x == 0) {
                 ScanArgs& a = ctl->args;
+                a.members = reinterpret_cast<const int32_t*>(sm + lay.off_members);
+                a.member_of = sm + lay.off_mof;
+                a.n_members = bq.n_members;
+                a.seg_stride = b.n_subjects;
                 a.query = bq.query;
                 a.qlen = bq.qlen;
                 a.ctx = bq.ctx;
@@ -721,7 +801,8 @@ scan_batch_kernel(BatchArgs b, ScanLayout lay) {
                 lo += n;
             }
         }
-        const long long seg0 = (long long)wi.qid * b.n_subjects;
+        const BatchQuery* unit = b.queries + wi.qid;
+        const long long seg0 = kPacked ? 0 : (long long)__ldg(&unit->seg_query) * b.n_subjects;
         for (;;) {
             unsigned s = 0;
             if (lane == 0) s = atomicAdd(&ctl->sub_ctr, 1u);
@@ -736,14 +817,16 @@ scan_batch_kernel(BatchArgs b, ScanLayout lay) {
                 __syncwarp();
                 base = b.window;
             }
-            scan_subject<CellT, kDefer>(ctl->args, m, qs, cells, entries, wr.diag, wr.lane_pos, wr.tasks, wr.blocked,
-                                        (int)(seg0 + oid - b.subject_first), b.db + so, (int)(eo - so), base, lane);
+            scan_subject<CellT, kDefer, kPacked>(ctl->args, m, qs, cells, entries, wr.diag, wr.lane_pos, wr.tasks,
+                                                 wr.blocked, wr.wcnt, (int)(seg0 + oid - b.subject_first), b.db + so,
+                                                 (int)(eo - so), base, lane);
         }
         __syncthreads();
     }
 }
 
-ScanLayout make_layout(int qlen, int L, int64_t n_entries, int warps, int cells_mode, int entries_smem) {
+ScanLayout make_layout(int qlen, int L, int64_t n_entries, int warps, int cells_mode, int entries_smem,
+                       bool packed) {
     ScanLayout l{};
     l.warps = warps;
     l.cells_mode = cells_mode;
@@ -760,8 +843,17 @@ ScanLayout make_layout(int qlen, int L, int64_t n_entries, int warps, int cells_
     if (off > big) off = big;
     l.off_query = (int)off;
     off = al(off + qlen, 16);
+    l.off_members = (int)off;
+    l.off_mof = (int)off;
+    if (packed) {
+        off = al(off + 5 * 4 * kMaxMembers, 16);
+        l.off_mof = (int)off;
+        off = al(off + qlen, 16);
+    }
     l.off_warps = (int)off;
-    const long long wb = al((long long)L * 4 + 32 * kP * 2 * 4 + (kTaskCap + kBlkCap) * (long long)sizeof(Task), 16);
+    const long long wb = al((long long)L * 4 + 32 * kP * 2 * 4 + (kTaskCap + kBlkCap) * (long long)sizeof(Task) +
+                                (packed ? 3 * 4 * kMaxMembers : 0),
+                            16);
     l.warp_bytes = (int)(wb > big ? big : wb);
     off += (long long)warps * wb;
     off = al(off, 16);
@@ -773,14 +865,14 @@ ScanLayout make_layout(int qlen, int L, int64_t n_entries, int warps, int cells_
 
 // Picks the layout with the most warps, preferring the whole table in shared
 // memory as long as that still leaves at least 16 warps.
-bool choose_layout(int qlen, int L, int64_t n_entries, int smem_optin, ScanLayout* out) {
+bool choose_layout(int qlen, int L, int64_t n_entries, int smem_optin, ScanLayout* out, bool packed = false) {
     const int cell_modes[2] = {n_entries < 65536 ? 0 : 1, 2};
     for (int min_w : {16, 8, 1})
         for (int cm : cell_modes)
             for (int es = 1; es >= 0; --es) {
                 if (es && cm == 2) continue;
                 for (int w = kMaxWarps; w >= min_w; --w) {
-                    const ScanLayout l = make_layout(qlen, L, n_entries, w, cm, es);
+                    const ScanLayout l = make_layout(qlen, L, n_entries, w, cm, es, packed);
                     if (l.total <= smem_optin) {
                         *out = l;
                         return true;
@@ -806,9 +898,9 @@ cudaError_t launch(bp_engine* e, const ScanArgs& a, const ScanLayout& lay) {
     return cudaGetLastError();
 }
 
-template <typename CellT, bool kCellsSmem, bool kDefer>
+template <typename CellT, bool kCellsSmem, bool kDefer, bool kPacked>
 cudaError_t launch_batch(bp_engine* e, cudaStream_t stream, const BatchArgs& b, const ScanLayout& lay, int grid) {
-    auto kern = scan_batch_kernel<CellT, kCellsSmem, kDefer>;
+    auto kern = scan_batch_kernel<CellT, kCellsSmem, kDefer, kPacked>;
     // the largest allowed size, not this launch's: launches of one instance
     // with different layouts (batch classes, captured graph nodes replayed
     // later) must all stay valid whatever order the attribute was set in
@@ -823,32 +915,41 @@ cudaError_t launch_batch(bp_engine* e, cudaStream_t stream, const BatchArgs& b, 
 
 static_assert(sizeof(BatchCtl) <= 512, "batched control block must fit its shared-memory slot");
 static_assert(sizeof(Task) == 16, "task layout");
+static_assert(kMaxMembers == BP_MAX_PACK_MEMBERS, "pack size limit");
 
 int bp_diag_len(int qlen, int window) {
     const long long n = ((long long)qlen + window + 31) / 32 * 32;
     return (int)(n < 128 ? 128 : (n > (1LL << 30) ? (1LL << 30) : n));
 }
 
-cudaError_t bp_launch_scan_batch(bp_engine* e, cudaStream_t stream, const BatchArgs& b, int32_t max_qlen,
-                                 int32_t max_diag_len, int64_t max_entries, int grid, int max_warps) {
-    ScanLayout lay;
-    if (!choose_layout(max_qlen, max_diag_len, max_entries, e->smem_optin, &lay)) return cudaErrorInvalidValue;
-    if (max_warps > 0 && lay.warps > max_warps) {
-        lay = make_layout(max_qlen, max_diag_len, max_entries, max_warps, lay.cells_mode, lay.entries_smem);
+template <bool kPacked>
+cudaError_t launch_batch_layout(bp_engine* e, cudaStream_t stream, const BatchArgs& b, const ScanLayout& lay,
+                                int grid, bool defer) {
+    if (defer) {
+        if (lay.cells_mode == 0) return launch_batch<uint16_t, true, true, kPacked>(e, stream, b, lay, grid);
+        if (lay.cells_mode == 1) return launch_batch<uint32_t, true, true, kPacked>(e, stream, b, lay, grid);
+        return launch_batch<uint32_t, false, true, kPacked>(e, stream, b, lay, grid);
     }
-    if (max_qlen >= kDeferMinQlen) {
-        if (lay.cells_mode == 0) return launch_batch<uint16_t, true, true>(e, stream, b, lay, grid);
-        if (lay.cells_mode == 1) return launch_batch<uint32_t, true, true>(e, stream, b, lay, grid);
-        return launch_batch<uint32_t, false, true>(e, stream, b, lay, grid);
-    }
-    if (lay.cells_mode == 0) return launch_batch<uint16_t, true, false>(e, stream, b, lay, grid);
-    if (lay.cells_mode == 1) return launch_batch<uint32_t, true, false>(e, stream, b, lay, grid);
-    return launch_batch<uint32_t, false, false>(e, stream, b, lay, grid);
+    if (lay.cells_mode == 0) return launch_batch<uint16_t, true, false, kPacked>(e, stream, b, lay, grid);
+    if (lay.cells_mode == 1) return launch_batch<uint32_t, true, false, kPacked>(e, stream, b, lay, grid);
+    return launch_batch<uint32_t, false, false, kPacked>(e, stream, b, lay, grid);
 }
 
-int bp_scan_warps(int32_t qlen, int32_t diag_len, int64_t n_entries, int smem_optin) {
+cudaError_t bp_launch_scan_batch(bp_engine* e, cudaStream_t stream, const BatchArgs& b, int32_t max_qlen,
+                                 int32_t max_diag_len, int64_t max_entries, int grid, int max_warps, bool packed) {
+    ScanLayout lay;
+    if (!choose_layout(max_qlen, max_diag_len, max_entries, e->smem_optin, &lay, packed)) return cudaErrorInvalidValue;
+    if (max_warps > 0 && lay.warps > max_warps) {
+        lay = make_layout(max_qlen, max_diag_len, max_entries, max_warps, lay.cells_mode, lay.entries_smem, packed);
+    }
+    const bool defer = max_qlen >= kDeferMinQlen;
+    return packed ? launch_batch_layout<true>(e, stream, b, lay, grid, defer)
+                  : launch_batch_layout<false>(e, stream, b, lay, grid, defer);
+}
+
+int bp_scan_warps(int32_t qlen, int32_t diag_len, int64_t n_entries, int smem_optin, bool packed) {
     ScanLayout l;
-    return choose_layout(qlen, diag_len, n_entries, smem_optin, &l) ? l.warps : 0;
+    return choose_layout(qlen, diag_len, n_entries, smem_optin, &l, packed) ? l.warps : 0;
 }
 
 bool bp_scan_defers(int32_t qlen) { return qlen >= kDeferMinQlen; }

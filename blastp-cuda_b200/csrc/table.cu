@@ -101,6 +101,28 @@ table_scan(const uint32_t* __restrict__ counts, uint32_t* __restrict__ cells) {
     }
 }
 
+// Cells of a packed table: the members' counts summed per cell.
+__global__ void pack_count(const PackSrc* __restrict__ src, int n, uint32_t* __restrict__ counts) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= BP_NC) return;
+    uint32_t s = 0;
+    for (int m = 0; m < n; ++m) s += src[m].cells[c + 1] - src[m].cells[c];
+    counts[c] = s;
+}
+
+// Entries of a packed table: per cell, each member's entries in member order
+// (so offsets stay ascending), shifted to the member's packed offset.
+__global__ void pack_fill(const PackSrc* __restrict__ src, int n, const uint32_t* __restrict__ cells,
+                          uint16_t* __restrict__ entries) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= BP_NC) return;
+    uint32_t pos = cells[c];
+    for (int m = 0; m < n; ++m) {
+        const uint32_t lo = src[m].cells[c], hi = src[m].cells[c + 1];
+        for (uint32_t i = lo; i < hi; ++i) entries[pos++] = (uint16_t)(src[m].entries[i] + src[m].off);
+    }
+}
+
 }  // namespace
 
 // pass 0: count + scan (the host then reads cells[BP_NC] to size the
@@ -133,4 +155,14 @@ cudaError_t bp_launch_table_build(bp_engine* e, const uint8_t* d_q, int32_t qlen
 int bp_cell_to_code15(int cell) {
     const int r0 = cell / 729 + 1, r1 = (cell / 27) % 27 + 1, r2 = cell % 27 + 1;
     return (r0 << 10) | (r1 << 5) | r2;
+}
+
+cudaError_t bp_launch_pack_table(bp_engine* e, cudaStream_t stream, const PackSrc* d_src, int n_members,
+                                 uint32_t* d_counts_tmp, uint32_t* d_cells, uint16_t* d_entries) {
+    const int grid = (BP_NC + 255) / 256;
+    pack_count<<<grid, 256, 0, stream>>>(d_src, n_members, d_counts_tmp);
+    table_scan<<<1, 1024, 0, stream>>>(d_counts_tmp, d_cells);
+    pack_fill<<<grid, 256, 0, stream>>>(d_src, n_members, d_cells, d_entries);
+    e->launches += 3;
+    return cudaGetLastError();
 }

@@ -152,6 +152,10 @@ typedef struct {
     const float* item_costs;    /* BP_SCHED_COSTS: predicted cost of item q*n_chunks + c */
     int32_t subject_first;      /* subjects [subject_first, subject_first + subject_count) */
     int32_t subject_count;      /* (< 0: to the end of the database) */
+    int32_t pack_residues;      /* > 0: queries of at most half this length share tables of up to
+                                   this many offsets (32 queries at most), so one word scan of a
+                                   subject serves all of them; 0: every query alone.
+                                   Default 512. */
 } bp_batch_options;
 
 void bp_batch_options_default(bp_batch_options* o);
@@ -221,12 +225,14 @@ bp_status bp_batch_predict_costs(bp_engine* e, bp_mlp* model, const float* weigh
                                  int32_t n_chunks, float planted_density, float* costs);
 
 /* ---- autotuner -------------------------------------------------------------
- * Times candidate batch configurations (subject-chunk size, warps per CTA,
- * schedule) on the first sample_subjects subjects with the whole query set
- * and returns the fastest. */
+ * Times candidate batch configurations on the first sample_subjects subjects
+ * with the whole query set and returns the fastest: first every subject-chunk
+ * size with every packing size (dynamic schedule, all warps), then, at the
+ * best of those, the other schedules and the warp caps. */
 typedef struct {
     int32_t chunk_residues, schedule, max_warps;
     float ms;                   /* best scan time of the candidate on the sample */
+    int32_t pack_residues;
 } bp_autotune_trial;
 
 typedef struct {
@@ -240,6 +246,8 @@ typedef struct {
     float planted_density;
     int32_t sample_subjects;    /* <= 0: 1/16 of the database */
     int32_t reps;               /* timed runs per candidate, best kept */
+    const int32_t* pack_sizes;  /* NULL: {0, 512, 1024} (bp_batch_options.pack_residues) */
+    int32_t n_pack_sizes;
 } bp_autotune_options;
 
 void bp_autotune_options_default(bp_autotune_options* o);

@@ -175,3 +175,37 @@ def test_autotune_picks_a_measured_candidate(engine, workload, singles):
     b = engine.search_batch(d, hs, **best)
     _check(b, singles, "autotuned")
     b.close()
+
+
+@pytest.mark.parametrize("pack", [256, 2048, 8000])
+@pytest.mark.parametrize("schedule", [SCHED_DYNAMIC, SCHED_COSTS])
+def test_packed_tables(engine, workload, singles, pack, schedule):
+    # short queries share packed tables; every query's result stays its own
+    qs, db = workload
+    d = engine.database(db.residues, db.offsets)
+    hs = [engine.query(q) for q in qs]
+    costs = None
+    if schedule == SCHED_COSTS:
+        costs = np.random.default_rng(pack).random(len(qs) * (len(engine.plan_chunks(d, 1 << 16)) - 1))
+    b = engine.search_batch(d, hs, chunk_residues=1 << 16, schedule=schedule, item_costs=costs,
+                            pack_residues=pack)
+    _check(b, singles, "pack %d sched %d" % (pack, schedule))
+    b.run()
+    _check(b, singles, "pack %d sched %d replay" % (pack, schedule))
+    b.close()
+
+
+def test_many_short_queries_packed(engine, matrix):
+    # 70 short queries (more than one full pack of 32), a subject range, and
+    # per-query parameters: packed results equal each query searched alone
+    rng = np.random.default_rng(31)
+    qs = [synth.residues(rng, int(n)) for n in rng.integers(3, 120, size=70)]
+    db = synth.make_database(rng, 5000, qs, 0.02, (30, 100), (0.35, 0.6), matrix)
+    d = engine.database(db.residues, db.offsets)
+    params = [default_params(x_dropoff=12 + (i % 3) * 4, cutoff_score=35 + (i % 4) * 3) for i in range(len(qs))]
+    hs = [engine.query(q, p) for q, p in zip(qs, params)]
+    b = engine.search_batch(d, hs, chunk_residues=1 << 15, pack_residues=3000, first=100, count=4500)
+    for i, h in enumerate(hs):
+        s = engine.search(d, h, 100, 4500).fetch()
+        assert_same(b.fetch(i), (s.counters, s.hsp_off, s.hsps_as_array()), "short query %d" % i)
+    b.close()
