@@ -83,6 +83,10 @@ SIGNATURES = {
     "bp_db_create": (ctypes.c_int, [P, P, i64, P, i32, P]),
     "bp_db_create_device": (ctypes.c_int, [P, P, i64, P, i32, P]),
     "bp_db_destroy": (None, [P]),
+    "bp_dbfile_write": (ctypes.c_int, [ctypes.c_char_p, P, i64, P, i32, i64, i32]),
+    "bp_dbfile_info": (ctypes.c_int, [ctypes.c_char_p, P, P, P, P]),
+    "bp_dbfile_read_host": (ctypes.c_int, [ctypes.c_char_p, P, P, P]),
+    "bp_db_open": (ctypes.c_int, [P, ctypes.c_char_p, P]),
     "bp_db_subjects": (i32, [P]),
     "bp_db_residues": (i64, [P]),
     "bp_query_create": (ctypes.c_int, [P, P, i32, P, P]),

@@ -83,6 +83,10 @@ class Engine:
     def database(self, residues: np.ndarray, offsets: np.ndarray) -> "Database":
         return Database(self, residues, offsets)
 
+    def open_database(self, path) -> "Database":
+        """A database file streamed into HBM (bp_db_open)."""
+        return Database(self, path=path)
+
     def query(self, residues: np.ndarray, params: BpParams | None = None) -> "Query":
         return Query(self, residues, params or default_params())
 
@@ -219,16 +223,45 @@ class Engine:
         return Result(counters, hoff, hsps[:nh.value])
 
 
+def write_database_file(path, residues, offsets, volume_residues: int = 0, sort_by_length: bool = False):
+    """Writes the subjects to a database file (bp_dbfile_write); no GPU needed."""
+    res = np.ascontiguousarray(residues, dtype=np.uint8)
+    off = np.ascontiguousarray(offsets, dtype=np.int64)
+    check(lib().bp_dbfile_write(str(path).encode(), _p(res), len(res), _p(off), len(off) - 1, volume_residues,
+                                int(bool(sort_by_length))))
+
+
+def read_database_file(path):
+    """(residues, offsets, oids, n_volumes) of a database file, in stored order;
+    oids[i] is the original index of stored subject i.  No GPU needed."""
+    n = ctypes.c_int32(0)
+    r = ctypes.c_int64(0)
+    v = ctypes.c_int32(0)
+    srt = ctypes.c_int32(0)
+    check(lib().bp_dbfile_info(str(path).encode(), ctypes.byref(n), ctypes.byref(r), ctypes.byref(v),
+                               ctypes.byref(srt)))
+    res = np.zeros(r.value, dtype=np.uint8)
+    off = np.zeros(n.value + 1, dtype=np.int64)
+    oids = np.zeros(n.value, dtype=np.int32)
+    check(lib().bp_dbfile_read_host(str(path).encode(), _p(res), _p(off), _p(oids)))
+    return res, off, oids, v.value
+
+
 class Database:
-    def __init__(self, engine: Engine, residues, offsets):
-        res = np.ascontiguousarray(residues, dtype=np.uint8)
-        off = np.ascontiguousarray(offsets, dtype=np.int64)
+    def __init__(self, engine: Engine, residues=None, offsets=None, path=None):
         h = ctypes.c_void_p()
-        check(lib().bp_db_create(engine.h, _p(res), len(res), _p(off), len(off) - 1, ctypes.byref(h)), engine.h)
+        if path is not None:
+            check(lib().bp_db_open(engine.h, str(path).encode(), ctypes.byref(h)), engine.h)
+            self.n_subjects = int(lib().bp_db_subjects(h))
+            self.n_residues = int(lib().bp_db_residues(h))
+        else:
+            res = np.ascontiguousarray(residues, dtype=np.uint8)
+            off = np.ascontiguousarray(offsets, dtype=np.int64)
+            check(lib().bp_db_create(engine.h, _p(res), len(res), _p(off), len(off) - 1, ctypes.byref(h)), engine.h)
+            self.n_subjects = len(off) - 1
+            self.n_residues = len(res)
         self.h = h
         self.engine = engine
-        self.n_subjects = len(off) - 1
-        self.n_residues = len(res)
 
     def close(self):
         if self.h:

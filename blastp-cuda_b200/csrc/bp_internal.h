@@ -165,6 +165,12 @@ struct BatchArgs {
 };
 
 // ---- host helpers ---------------------------------------------------------
+// Database allocation (residues + 32 bytes of zero padding, offsets), and
+// the finishing step: padding written, residue codes checked on the device.
+extern "C" {
+bp_status bp_db_alloc(bp_engine* e, int64_t n_residues, int32_t n_subjects, bp_db** out);
+bp_status bp_db_finish(bp_engine* e, bp_db* db);
+}
 bp_status bp_set_cuda_error(bp_engine* e, cudaError_t err, const char* what);
 bp_status bp_set_error(bp_engine* e, bp_status s, const std::string& msg);
 void bp_fill_matrix28(int8_t out[28 * 28]);

@@ -264,7 +264,7 @@ bp_status bp_engine_synchronize(bp_engine* e) {
     return BP_OK;
 }
 
-static bp_status db_alloc(bp_engine* e, int64_t n_residues, int32_t n_subjects, bp_db** out) {
+bp_status bp_db_alloc(bp_engine* e, int64_t n_residues, int32_t n_subjects, bp_db** out) {
     bp_db* db = new bp_db();
     db->e = e;
     db->n = n_subjects;
@@ -280,7 +280,7 @@ static bp_status db_alloc(bp_engine* e, int64_t n_residues, int32_t n_subjects, 
 }
 
 // Zero padding after the residues, then the residue-code check on the device.
-static bp_status db_finish(bp_engine* e, bp_db* db) {
+bp_status bp_db_finish(bp_engine* e, bp_db* db) {
     const size_t padded = (size_t)((db->nres + 15) & ~15LL) + 32;
     CK(cudaMemsetAsync(db->d_res + db->nres, 0, padded - (size_t)db->nres, e->stream), "pad database");
     CK(cudaMemsetAsync(e->d_counts + 3, 0, sizeof(uint32_t), e->stream), "memset(check)");
@@ -308,7 +308,7 @@ bp_status bp_db_create(bp_engine* e, const uint8_t* residues, int64_t n_residues
             return bp_set_error(e, BP_ERR_INVALID, "bp_db_create: offsets must be non-decreasing, subjects < 2^29");
     CK(cudaSetDevice(e->device), "cudaSetDevice");
     bp_db* db = nullptr;
-    bp_status st = db_alloc(e, n_residues, n_subjects, &db);
+    bp_status st = bp_db_alloc(e, n_residues, n_subjects, &db);
     if (st != BP_OK) return st;
     cudaError_t err = cudaMemcpyAsync(db->d_res, residues, (size_t)n_residues, cudaMemcpyHostToDevice, e->stream);
     if (err == cudaSuccess)
@@ -318,7 +318,7 @@ bp_status bp_db_create(bp_engine* e, const uint8_t* residues, int64_t n_residues
         bp_db_destroy(db);
         return bp_set_cuda_error(e, err, "database upload");
     }
-    st = db_finish(e, db);
+    st = bp_db_finish(e, db);
     if (st != BP_OK) {
         bp_db_destroy(db);
         return st;
@@ -342,7 +342,7 @@ bp_status bp_db_create_device(bp_engine* e, const uint8_t* d_residues, int64_t n
         if (off[i + 1] < off[i] || off[i + 1] - off[i] > (1 << 29))
             return bp_set_error(e, BP_ERR_INVALID, "bp_db_create_device: offsets must be non-decreasing");
     bp_db* db = nullptr;
-    bp_status st = db_alloc(e, n_residues, n_subjects, &db);
+    bp_status st = bp_db_alloc(e, n_residues, n_subjects, &db);
     if (st != BP_OK) return st;
     cudaError_t err =
         cudaMemcpyAsync(db->d_res, d_residues, (size_t)n_residues, cudaMemcpyDeviceToDevice, e->stream);
@@ -352,7 +352,7 @@ bp_status bp_db_create_device(bp_engine* e, const uint8_t* d_residues, int64_t n
         bp_db_destroy(db);
         return bp_set_cuda_error(e, err, "database copy");
     }
-    st = db_finish(e, db);
+    st = bp_db_finish(e, db);
     if (st != BP_OK) {
         bp_db_destroy(db);
         return st;

@@ -97,6 +97,22 @@ void bp_db_destroy(bp_db* db);
 int32_t bp_db_subjects(const bp_db* db);
 int64_t bp_db_residues(const bp_db* db);
 
+/* Database file: the subjects on disk in volumes of at most volume_residues
+ * residues (<= 0: 1 GiB), optionally stored longest first (an oid map then
+ * gives every stored subject's original index).  Replaces the reference's
+ * ".gpu" file (functions.cpp:364-613, 4 GB volume cap at :481-485).
+ * bp_dbfile_info / bp_dbfile_read_host need no GPU; bp_db_open maps the file
+ * and streams it into HBM through two pinned staging buffers, so the host
+ * copy of one part overlaps the transfer of the previous one. */
+bp_status bp_dbfile_write(const char* path, const uint8_t* residues, int64_t n_residues, const int64_t* offsets,
+                          int32_t n_subjects, int64_t volume_residues, int32_t sort_by_length);
+bp_status bp_dbfile_info(const char* path, int32_t* n_subjects, int64_t* n_residues, int32_t* n_volumes,
+                         int32_t* sorted);
+/* residues [n_residues], offsets [n_subjects+1] (stored order), oids
+ * [n_subjects] (original index of each stored subject); any may be NULL. */
+bp_status bp_dbfile_read_host(const char* path, uint8_t* residues, int64_t* offsets, int32_t* oids);
+bp_status bp_db_open(bp_engine* e, const char* path, bp_db** out);
+
 /* Query: copies the residues to the device and builds the neighbour-word
  * table there (CSR keyed by the packed 3-letter code, plus presence bitmap). */
 bp_status bp_query_create(bp_engine* e, const uint8_t* residues, int32_t length,
