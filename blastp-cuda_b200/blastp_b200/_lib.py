@@ -124,6 +124,8 @@ SIGNATURES = {
     "bp_mlp_predict": (ctypes.c_int, [P, P, i32, P]),
     "bp_batch_predict_costs": (ctypes.c_int, [P, P, P, P, P, i32, P, i32, ctypes.c_float, P]),
     "bp_autotune_options_default": (None, [P]),
+    "bp_cosched_split_costs": (i32, [P, i32, ctypes.c_double]),
+    "bp_cosched_split": (ctypes.c_int, [P, P, P, P, P, i32, ctypes.c_float, ctypes.c_double, P]),
     "bp_batch_autotune": (ctypes.c_int, [P, P, P, i32, P, P, P, i32, P]),
     "bp_server_options_default": (None, [P]),
     "bp_server_create": (ctypes.c_int, [P, P, P, P]),

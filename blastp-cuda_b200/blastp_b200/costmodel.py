@@ -160,6 +160,28 @@ def train(engine: Engine, matrix28, seeds=range(50), holdout: int = 10, epochs: 
     return model, report, curve
 
 
+def cosched_split_chunk(chunk_costs, cpu_factor: float) -> int:
+    """Chunk index splitting device [0, k) and CPU [k, n) work so both finish
+    together (bp_cosched_split_costs; no GPU needed)."""
+    import ctypes
+    from ._lib import lib
+    c = np.ascontiguousarray(chunk_costs, dtype=np.float64)
+    return int(lib().bp_cosched_split_costs(c.ctypes.data if len(c) else None, len(c), float(cpu_factor)))
+
+
+def cosched_split(engine: Engine, model: "CostModel", db, queries, cpu_factor: float,
+                  planted_density: float = 0.0) -> int:
+    """First subject of the CPU's share (bp_cosched_split)."""
+    import ctypes
+    from ._lib import check, lib
+    w = np.ascontiguousarray(model.weights, dtype=np.float32)
+    arr = (ctypes.c_void_p * len(queries))(*[q.h.value for q in queries])
+    out = ctypes.c_int32(0)
+    check(lib().bp_cosched_split(engine.h, model.mlp.h, w.ctypes.data, db.h, arr, len(queries), planted_density,
+                                 float(cpu_factor), ctypes.byref(out)), engine.h)
+    return int(out.value)
+
+
 def makespan(costs: np.ndarray, queue_of_item: np.ndarray) -> float:
     """Largest per-queue sum of `costs` under an item -> queue assignment."""
     q = queue_of_item[queue_of_item >= 0]
@@ -176,7 +198,7 @@ def actual_item_costs(weights, residues_per_chunk, counts_per_item):
 
 
 __all__ = ["CostModel", "train", "training_workload", "log_counts", "fit_cost_weights", "relative_error",
-           "makespan", "actual_item_costs", "chunk_sums", "MODEL_PATH", "TRAIN_CHUNK_RESIDUES"]
+           "makespan", "actual_item_costs", "cosched_split_chunk", "cosched_split", "chunk_sums", "MODEL_PATH", "TRAIN_CHUNK_RESIDUES"]
 
 
 def main(argv=None):

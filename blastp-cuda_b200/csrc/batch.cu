@@ -856,3 +856,57 @@ bp_status bp_batch_autotune(bp_engine* e, const bp_db* db, const bp_query* const
 }
 
 }  // extern "C"
+
+// ---- GPU/CPU co-scheduling -------------------------------------------------
+
+extern "C" {
+
+// The chunk index k that balances the device's share [0, k) against the CPU's
+// share [k, n): minimises max(sum_{c<k} cost_c, cpu_factor * sum_{c>=k} cost_c),
+// costs being device time per chunk and cpu_factor the CPU's time per unit of
+// device time.  Replaces the reference's fixed GPU fraction of the OIDs
+// (functions.cpp:125-149, :1059).
+int32_t bp_cosched_split_costs(const double* chunk_costs, int32_t n_chunks, double cpu_factor) {
+    if (!chunk_costs || n_chunks <= 0) return 0;
+    if (!(cpu_factor > 0)) return n_chunks;                 // no CPU share
+    double total = 0;
+    for (int32_t c = 0; c < n_chunks; ++c) total += std::max(0.0, chunk_costs[c]);
+    double gpu = 0, best = 1e300;
+    int32_t best_k = n_chunks;
+    for (int32_t k = 0; k <= n_chunks; ++k) {
+        const double m = std::max(gpu, cpu_factor * (total - gpu));
+        if (m < best) {
+            best = m;
+            best_k = k;
+        }
+        if (k < n_chunks) gpu += std::max(0.0, chunk_costs[k]);
+    }
+    return best_k;
+}
+
+// The first subject the CPU should take when the device searches subjects
+// [0, split) and the CPU the rest, from the cost model's predictions for these
+// queries over 64Ki-residue chunks.
+bp_status bp_cosched_split(bp_engine* e, bp_mlp* model, const float* weights, const bp_db* db,
+                           const bp_query* const* queries, int32_t n_queries, float planted_density, double cpu_factor,
+                           int32_t* split_subject) {
+    if (!e || !model || !weights || !db || !queries || n_queries < 1 || !split_subject) return BP_ERR_INVALID;
+    std::vector<int32_t> first;
+    plan_direct(db, 0, db->n, kBaseChunk, first);
+    const int32_t nc = (int32_t)first.size() - 1;
+    if (nc == 0) {
+        *split_subject = 0;
+        return BP_OK;
+    }
+    std::vector<float> costs((size_t)n_queries * nc);
+    bp_status st = bp_batch_predict_costs(e, model, weights, db, queries, n_queries, first.data(), nc,
+                                          planted_density, costs.data());
+    if (st != BP_OK) return st;
+    std::vector<double> per_chunk(nc, 0.0);
+    for (int32_t q = 0; q < n_queries; ++q)
+        for (int32_t c = 0; c < nc; ++c) per_chunk[c] += costs[(size_t)q * nc + c];
+    *split_subject = first[bp_cosched_split_costs(per_chunk.data(), nc, cpu_factor)];
+    return BP_OK;
+}
+
+}  // extern "C"

@@ -240,6 +240,17 @@ bp_status bp_batch_predict_costs(bp_engine* e, bp_mlp* model, const float* weigh
                                  const bp_query* const* queries, int32_t n_queries, const int32_t* chunk_first,
                                  int32_t n_chunks, float planted_density, float* costs);
 
+/* ---- GPU/CPU co-scheduling -------------------------------------------------
+ * Splits the subjects between the device ([0, split)) and a CPU search of
+ * the rest so both finish together, from predicted device time per chunk and
+ * the CPU's time per unit of device time (cpu_factor, measured by the
+ * caller).  Replaces the reference's fixed GPU share of the OIDs
+ * (functions.cpp:125-149, :1059).  bp_cosched_split_costs needs no GPU. */
+int32_t bp_cosched_split_costs(const double* chunk_costs, int32_t n_chunks, double cpu_factor);
+bp_status bp_cosched_split(bp_engine* e, bp_mlp* model, const float* weights, const bp_db* db,
+                           const bp_query* const* queries, int32_t n_queries, float planted_density, double cpu_factor,
+                           int32_t* split_subject);
+
 /* ---- autotuner -------------------------------------------------------------
  * Times candidate batch configurations on the first sample_subjects subjects
  * with the whole query set and returns the fastest: first every subject-chunk

@@ -39,3 +39,16 @@ def test_relative_error_and_cost_weights():
     timing = np.concatenate([A, (A @ w_true)[:, None]], axis=1)
     w = costmodel.fit_cost_weights(timing)
     assert np.allclose(w, w_true, rtol=1e-6)
+
+
+def test_cosched_split_balances_device_and_cpu():
+    rng = np.random.default_rng(4)
+    costs = rng.uniform(0.5, 2.0, size=400)
+    for f in (0.5, 4.0, 40.0):
+        k = costmodel.cosched_split_chunk(costs, f)
+        gpu, cpu = costs[:k].sum(), f * costs[k:].sum()
+        best = min(max(costs[:j].sum(), f * costs[j:].sum()) for j in range(401))
+        assert max(gpu, cpu) == best
+        assert abs(gpu - cpu) <= max(costs) * max(1.0, f)
+    assert costmodel.cosched_split_chunk(costs, 0.0) == 400      # no CPU share
+    assert costmodel.cosched_split_chunk([], 3.0) == 0

@@ -134,3 +134,16 @@ def test_library_costs_match_python_costs(engine, matrix):
     best, trials = engine.autotune(d, hq, model=model, planted_density=0.01, sample_subjects=1000,
                                    chunk_sizes=[1 << 15], warp_caps=[0], reps=1)
     assert {t["schedule"] for t in trials} == {SCHED_DYNAMIC, SCHED_STATIC, SCHED_COSTS}
+
+
+def test_cosched_split_from_model(engine, matrix):
+    model = costmodel.CostModel.load(engine)
+    rng = np.random.default_rng(19)
+    qs = [synth.residues(rng, int(n)) for n in (80, 600)]
+    db = synth.make_database(rng, 20_000, qs, 0.005, (60, 150), (0.3, 0.5), matrix)
+    d = engine.database(db.residues, db.offsets)
+    hq = [engine.query(q) for q in qs]
+    splits = [costmodel.cosched_split(engine, model, d, hq, f, 0.005) for f in (0.1, 1.0, 10.0, 100.0)]
+    assert all(0 <= s <= 20_000 for s in splits)
+    assert splits == sorted(splits)                 # a slower CPU leaves more to the device
+    assert 8_000 <= splits[1] <= 12_000             # equal speeds: about half the residues each
