@@ -47,7 +47,18 @@ struct bp_engine {
     uint32_t* h_pool = nullptr;
     std::vector<int> pool_free;
     std::mutex pool_mu;
+    struct HostPath* host_path = nullptr;   // buffers and copy stream of bp_blastp_host
 };
+
+// Frees bp_blastp_host's buffers (engine destruction).
+void bp_host_path_free(bp_engine* e);
+extern "C" bp_status bp_blastp_host_staged(bp_engine* e, const uint8_t* query, int32_t qlen, const bp_params* p,
+                                           const uint8_t* residues, int64_t n_residues, const int64_t* offsets,
+                                           int32_t n_subjects, int32_t* counters, int64_t* hsp_off, bp_hsp* hsps,
+                                           int64_t hsp_cap, int64_t* n_hsps);
+// Sets *bad (device word) when any of n residues is >= 28.
+cudaError_t bp_launch_check_residues(bp_engine* e, cudaStream_t stream, const uint8_t* d_res, int64_t n,
+                                     uint32_t* d_bad);
 
 // A pinned 4-word slot from the engine's pool (or a fresh pinned block when
 // the pool is exhausted); returned with bp_pinned_put.
@@ -115,6 +126,7 @@ struct ScanArgs {
     uint32_t* rec_count;
     uint32_t* cursor;           // subject cursor (chunks of 32)
     uint32_t* error;            // set when a bounded wait runs out
+    int32_t oid_base;           // plain kernel: counters and records of subject i go to oid_base + i
     // packed tables (batched kernel): per query {id, offset, length, x-drop,
     // cutoff}, the query of every packed offset, and the segment stride
     const int32_t* members;

@@ -35,11 +35,15 @@ bp_status bp_set_error(bp_engine* e, bp_status s, const std::string& msg) {
 namespace {
 
 // Sets *bad when any residue code is >= 28 (16 bytes per thread per step).
+// `res` may start anywhere: the bytes before its first 16-byte boundary and
+// after its last one are checked one by one, the rest with 16-byte loads.
 __global__ void check_residues(const uint8_t* __restrict__ res, int64_t n, uint32_t* bad) {
-    const int64_t n16 = n / 16;
+    const int64_t head = std::min<int64_t>(n, (int64_t)((16 - ((uintptr_t)res & 15)) & 15));
+    const uint8_t* body = res + head;                       // 16-byte aligned
+    const int64_t n16 = (n - head) / 16;
     uint32_t b = 0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n16; i += (int64_t)gridDim.x * blockDim.x) {
-        const uint4 v = reinterpret_cast<const uint4*>(res)[i];
+        const uint4 v = reinterpret_cast<const uint4*>(body)[i];
         const uint32_t w[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
@@ -48,8 +52,10 @@ __global__ void check_residues(const uint8_t* __restrict__ res, int64_t n, uint3
             b |= (x | ((x & 0x7f7f7f7fu) + 0x64646464u)) & 0x80808080u;
         }
     }
-    if (blockIdx.x == 0)
-        for (int64_t i = n16 * 16 + threadIdx.x; i < n; i += blockDim.x) b |= res[i] >= BP_ALPHABET;
+    if (blockIdx.x == 0) {
+        for (int64_t i = threadIdx.x; i < head; i += blockDim.x) b |= res[i] >= BP_ALPHABET;
+        for (int64_t i = head + n16 * 16 + threadIdx.x; i < n; i += blockDim.x) b |= res[i] >= BP_ALPHABET;
+    }
     if (b) atomicOr(bad, 1u);
 }
 
@@ -67,6 +73,15 @@ cudaError_t grow(T** p, size_t* cap_elems, size_t need) {
 constexpr int kPoolSlots = 1024;
 
 }  // namespace
+
+cudaError_t bp_launch_check_residues(bp_engine* e, cudaStream_t stream, const uint8_t* d_res, int64_t n,
+                                     uint32_t* d_bad) {
+    if (n <= 0) return cudaSuccess;
+    const int64_t blocks = std::min<int64_t>((int64_t)e->sm_count * 4, (n / 16 + 255) / 256 + 1);
+    check_residues<<<(unsigned)blocks, 256, 0, stream>>>(d_res, n, d_bad);
+    e->launches += 1;
+    return cudaGetLastError();
+}
 
 uint32_t* bp_pinned_get(bp_engine* e) {
     {
@@ -121,7 +136,7 @@ bp_status bp_run_search(bp_engine* e, bp_result* r) {
     }
     CK(cudaMemsetAsync(e->d_counts, 0, 4 * sizeof(uint32_t), e->stream), "memset(counts)");
 
-    ScanArgs a;
+    ScanArgs a{};
     a.db = db->d_res;
     a.db_off = db->d_off;
     a.first = r->first;
@@ -241,6 +256,7 @@ void bp_engine_destroy(bp_engine* e) {
     if (!e) return;
     cudaSetDevice(e->device);
     if (e->stream) cudaStreamSynchronize(e->stream);
+    bp_host_path_free(e);
     cudaFree(e->d_matrix);
     cudaFree(e->d_recs);
     cudaFree(e->d_counts);
@@ -569,9 +585,12 @@ void bp_result_destroy(bp_result* r) {
     delete r;
 }
 
-bp_status bp_blastp_host(bp_engine* e, const uint8_t* query, int32_t qlen, const bp_params* p,
-                         const uint8_t* residues, int64_t n_residues, const int64_t* offsets, int32_t n_subjects,
-                         int32_t* counters, int64_t* hsp_off, bp_hsp* hsps, int64_t hsp_cap, int64_t* n_hsps) {
+// The unpipelined form: database upload, then the search (bp_blastp_host
+// falls back to it when the pipelined search's record buffer overflows).
+bp_status bp_blastp_host_staged(bp_engine* e, const uint8_t* query, int32_t qlen, const bp_params* p,
+                                const uint8_t* residues, int64_t n_residues, const int64_t* offsets,
+                                int32_t n_subjects, int32_t* counters, int64_t* hsp_off, bp_hsp* hsps,
+                                int64_t hsp_cap, int64_t* n_hsps) {
     if (!e) return BP_ERR_INVALID;
     bp_db* db = nullptr;
     bp_query* q = nullptr;

@@ -1,0 +1,225 @@
+// bp_blastp_host: one search from host buffers to host buffers, with the
+// database upload overlapped with the scan.
+//
+// The reference copies the whole database to the device and only then
+// launches its kernel (gpu_blastp.cu:139-210).  Here the subjects are cut
+// into chunks of about 64 MiB of residues; a copy stream uploads them one
+// after the other, each followed by an event, and the engine stream checks
+// and scans every chunk as soon as its event has fired, so the transfer of
+// chunk k+1 runs under the scan of chunk k.  The query's table is built on
+// the engine stream while the first chunk is in flight.  All chunks write
+// one set of per-subject counters and one record buffer (subject index =
+// chunk start + index in the chunk), ordered once at the end.  Device
+// buffers are grow-only and kept by the engine, so repeated calls allocate
+// nothing once warm.
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "bp_internal.h"
+
+#define CKH(call, what)                                                   \
+    do {                                                                  \
+        cudaError_t _err = (call);                                        \
+        if (_err != cudaSuccess) return bp_set_cuda_error(e, _err, what); \
+    } while (0)
+
+struct HostPath {
+    cudaStream_t copy = nullptr;
+    std::vector<cudaEvent_t> ready;     // one per chunk slot
+    uint8_t* d_res = nullptr;
+    size_t res_cap = 0;
+    int64_t* d_off = nullptr;
+    size_t off_cap = 0;
+    int32_t* d_counters = nullptr;
+    int64_t* d_hsp_off = nullptr;
+    size_t subj_cap = 0;
+    uint32_t* d_words = nullptr;        // [0] records, [1] bad residue, [2..] chunk cursors
+    size_t words_cap = 0;
+    uint32_t* h_words = nullptr;        // pinned read-back
+};
+
+namespace {
+
+constexpr int64_t kChunkResidues = (int64_t)64 << 20;
+
+template <class T>
+cudaError_t grow_buf(T** p, size_t* cap, size_t need) {
+    if (*p && *cap >= need) return cudaSuccess;
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    const size_t n = std::max(need, *cap + *cap / 2);
+    cudaError_t err = cudaMalloc((void**)p, n * sizeof(T));
+    *cap = err == cudaSuccess ? n : 0;
+    return err;
+}
+
+}  // namespace
+
+void bp_host_path_free(bp_engine* e) {
+    HostPath* h = e->host_path;
+    if (!h) return;
+    if (h->copy) cudaStreamSynchronize(h->copy);
+    for (cudaEvent_t ev : h->ready) cudaEventDestroy(ev);
+    if (h->copy) cudaStreamDestroy(h->copy);
+    cudaFree(h->d_res);
+    cudaFree(h->d_off);
+    cudaFree(h->d_counters);
+    cudaFree(h->d_hsp_off);
+    cudaFree(h->d_words);
+    if (h->h_words) cudaFreeHost(h->h_words);
+    delete h;
+    e->host_path = nullptr;
+}
+
+extern "C" bp_status bp_blastp_host(bp_engine* e, const uint8_t* query, int32_t qlen, const bp_params* p,
+                                    const uint8_t* residues, int64_t n_residues, const int64_t* offsets,
+                                    int32_t n_subjects, int32_t* counters, int64_t* hsp_off, bp_hsp* hsps,
+                                    int64_t hsp_cap, int64_t* n_hsps) {
+    if (!e || !offsets || n_subjects < 0 || n_residues < 0 || (n_residues > 0 && !residues) || !p ||
+        (qlen > 0 && !query) || qlen < 0)
+        return bp_set_error(e, BP_ERR_INVALID, "bp_blastp_host: bad argument");
+    if (offsets[0] != 0 || offsets[n_subjects] != n_residues)
+        return bp_set_error(e, BP_ERR_INVALID, "bp_blastp_host: offsets must run from 0 to n_residues");
+    for (int32_t i = 0; i < n_subjects; ++i)
+        if (offsets[i + 1] < offsets[i] || offsets[i + 1] - offsets[i] > (1 << 29))
+            return bp_set_error(e, BP_ERR_INVALID, "bp_blastp_host: offsets must be non-decreasing, subjects < 2^29");
+    CKH(cudaSetDevice(e->device), "cudaSetDevice");
+    // chunks of whole subjects, about kChunkResidues residues each
+    std::vector<int32_t> cf(1, 0);
+    while (cf.back() < n_subjects) {
+        const int32_t s = cf.back();
+        const int64_t limit = offsets[s] + kChunkResidues;
+        int32_t t = (int32_t)(std::upper_bound(offsets + s + 1, offsets + n_subjects + 1, limit) - offsets) - 1;
+        cf.push_back(std::max(t, s + 1));
+    }
+    const int n_chunks = (int)cf.size() - 1;
+    if (!e->host_path) e->host_path = new HostPath();
+    HostPath* h = e->host_path;
+    if (!h->copy) CKH(cudaStreamCreateWithFlags(&h->copy, cudaStreamNonBlocking), "cudaStreamCreate");
+    if (!h->h_words) CKH(cudaMallocHost((void**)&h->h_words, 4 * sizeof(uint32_t)), "cudaMallocHost");
+    while ((int)h->ready.size() < n_chunks) {
+        cudaEvent_t ev = nullptr;
+        CKH(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreate");
+        h->ready.push_back(ev);
+    }
+    const size_t res_bytes = (size_t)((n_residues + 15) & ~15LL) + 32;
+    CKH(grow_buf(&h->d_res, &h->res_cap, res_bytes), "cudaMalloc(database)");
+    CKH(grow_buf(&h->d_off, &h->off_cap, (size_t)n_subjects + 1), "cudaMalloc(offsets)");
+    if (h->subj_cap < (size_t)n_subjects + 1) {
+        cudaFree(h->d_counters);
+        cudaFree(h->d_hsp_off);
+        h->d_counters = nullptr;
+        h->d_hsp_off = nullptr;
+        h->subj_cap = 0;
+        const size_t n = (size_t)n_subjects + 1;
+        CKH(cudaMalloc((void**)&h->d_counters, n * 3 * sizeof(int32_t)), "cudaMalloc(counters)");
+        CKH(cudaMalloc((void**)&h->d_hsp_off, n * sizeof(int64_t)), "cudaMalloc(offsets)");
+        h->subj_cap = n;
+    }
+    CKH(grow_buf(&h->d_words, &h->words_cap, (size_t)n_chunks + 2), "cudaMalloc(words)");
+    // the query table first (it synchronises the engine stream), then the
+    // engine's record scratch
+    bp_query* q = nullptr;
+    bp_status st = bp_query_create(e, query, qlen, p, &q);
+    if (st != BP_OK) return st;
+    if (!bp_scan_fits(q->qlen, q->diag_len, q->n_entries, e->smem_optin)) {
+        bp_query_destroy(q);
+        return bp_set_error(e, BP_ERR_TOO_LARGE, "bp_blastp_host: query too long for the diagonal array");
+    }
+    uint32_t cap = std::max<uint32_t>(e->rec_cap, 65536);
+    size_t rc = e->rec_cap;
+    CKH(grow_buf(&e->d_recs, &rc, cap), "cudaMalloc(records)");
+    e->rec_cap = (uint32_t)rc;
+    size_t fc = (size_t)e->fill_cap;
+    CKH(grow_buf(&e->d_fill, &fc, (size_t)std::max(n_subjects, 1)), "cudaMalloc(fill)");
+    e->fill_cap = (int32_t)fc;
+    size_t bc = (size_t)e->blocksum_cap;
+    CKH(grow_buf(&e->d_blocksums, &bc, (size_t)bp_order_blocksums_needed(n_subjects)), "cudaMalloc(sums)");
+    e->blocksum_cap = (int32_t)bc;
+    // chunk k's upload is queued on the copy stream, its check and scan on the
+    // engine stream behind the chunk's event: from pinned memory every copy
+    // is queued at once and the scans follow the copies; from pageable memory
+    // each copy call returns once staged, while the scans already queued run
+    CKH(cudaMemsetAsync(h->d_words, 0, ((size_t)n_chunks + 2) * sizeof(uint32_t), e->stream), "memset");
+    CKH(cudaMemsetAsync(h->d_res + n_residues, 0, res_bytes - (size_t)n_residues, h->copy), "memset(pad)");
+    CKH(cudaMemcpyAsync(h->d_off, offsets, ((size_t)n_subjects + 1) * 8, cudaMemcpyHostToDevice, h->copy),
+        "upload offsets");
+    CKH(cudaEventRecord(e->ev_scan0, e->stream), "cudaEventRecord");
+    for (int k = 0; k < n_chunks; ++k) {
+        const int64_t lo = offsets[cf[k]], hi = offsets[cf[k + 1]];
+        if (hi > lo)
+            CKH(cudaMemcpyAsync(h->d_res + lo, residues + lo, (size_t)(hi - lo), cudaMemcpyHostToDevice, h->copy),
+                "upload residues");
+        CKH(cudaEventRecord(h->ready[k], h->copy), "cudaEventRecord");
+        CKH(cudaStreamWaitEvent(e->stream, h->ready[k], 0), "cudaStreamWaitEvent");
+        CKH(bp_launch_check_residues(e, e->stream, h->d_res + lo, hi - lo, h->d_words + 1), "residue check");
+        ScanArgs a{};
+        a.db = h->d_res;
+        a.db_off = h->d_off;
+        a.first = cf[k];
+        a.n = cf[k + 1] - cf[k];
+        a.query = q->d_q;
+        a.qlen = q->qlen;
+        a.cells = q->d_cells;
+        a.entries = q->d_entries;
+        a.n_entries = (int32_t)q->n_entries;
+        a.ctx = q->d_ctx;
+        a.n_ctx = q->n_ctx;
+        a.matrix = e->d_matrix;
+        a.window = q->p.window;
+        a.diag_len = q->diag_len;
+        a.counters = h->d_counters;
+        a.recs = e->d_recs;
+        a.rec_cap = e->rec_cap;
+        a.rec_count = h->d_words;
+        a.cursor = h->d_words + 2 + k;
+        a.error = h->d_words + 1;
+        a.oid_base = cf[k];
+        CKH(bp_launch_scan(e, a), "scan kernel launch");
+    }
+    CKH(cudaEventRecord(e->ev_scan1, e->stream), "cudaEventRecord");
+    // records written and the residue check, then outputs sized by the records
+    CKH(cudaMemcpyAsync(h->h_words, h->d_words, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, e->stream),
+        "read counts");
+    CKH(cudaStreamSynchronize(e->stream), "pipelined search");
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, e->ev_scan0, e->ev_scan1) == cudaSuccess) e->last_scan_ms = ms;
+    cudaGetLastError();
+    const uint32_t recs = h->h_words[0];
+    if (h->h_words[1]) {
+        bp_query_destroy(q);
+        return bp_set_error(e, BP_ERR_INVALID, "bp_blastp_host: residue code >= 28");
+    }
+    if (recs > e->rec_cap) {
+        // more HSPs than the record buffer held: the unpipelined path grows and re-runs
+        bp_query_destroy(q);
+        return bp_blastp_host_staged(e, query, qlen, p, residues, n_residues, offsets, n_subjects, counters, hsp_off,
+                                     hsps, hsp_cap, n_hsps);
+    }
+    bp_hsp* d_hsps = nullptr;
+    int32_t* d_keys = nullptr;
+    CKH(cudaMallocAsync((void**)&d_hsps, (size_t)std::max<uint32_t>(recs, 1) * sizeof(bp_hsp), e->stream),
+        "cudaMallocAsync(hsps)");
+    CKH(cudaMallocAsync((void**)&d_keys, (size_t)std::max<uint32_t>(recs, 1) * sizeof(int32_t), e->stream),
+        "cudaMallocAsync(keys)");
+    CKH(bp_launch_order(e, n_subjects, h->d_counters, h->d_hsp_off, e->d_recs, e->rec_cap, h->d_words, e->d_fill,
+                        d_hsps, d_keys, e->d_blocksums),
+        "order kernels launch");
+    if (n_hsps) *n_hsps = recs;
+    cudaError_t err = cudaSuccess;
+    if (counters && n_subjects > 0)
+        err = cudaMemcpyAsync(counters, h->d_counters, (size_t)n_subjects * 12, cudaMemcpyDeviceToHost, e->stream);
+    if (err == cudaSuccess && hsp_off)
+        err = cudaMemcpyAsync(hsp_off, h->d_hsp_off, ((size_t)n_subjects + 1) * 8, cudaMemcpyDeviceToHost, e->stream);
+    if (hsps && (int64_t)recs > hsp_cap) st = bp_set_error(e, BP_ERR_TOO_LARGE, "bp_blastp_host: hsp_cap too small");
+    else if (err == cudaSuccess && hsps && recs > 0)
+        err = cudaMemcpyAsync(hsps, d_hsps, (size_t)recs * sizeof(bp_hsp), cudaMemcpyDeviceToHost, e->stream);
+    cudaFreeAsync(d_hsps, e->stream);
+    cudaFreeAsync(d_keys, e->stream);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
+    bp_query_destroy(q);
+    if (err != cudaSuccess) return bp_set_cuda_error(e, err, "bp_blastp_host: results");
+    return st;
+}

@@ -168,7 +168,7 @@ extern "C" bp_status bp_search_noalloc(const uint8_t* d_query, int32_t qlen, con
     err = bp_launch_table_build(&e, d_query, qlen, p->threshold, cells, entries, tmp, 1);
 
     const uint32_t cap = (uint32_t)(hsp_cap < kMaxRecords ? hsp_cap : kMaxRecords);
-    ScanArgs a;
+    ScanArgs a{};
     a.db = d_residues;
     a.db_off = d_offsets;
     a.first = 0;

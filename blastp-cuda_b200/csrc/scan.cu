@@ -678,7 +678,7 @@ scan_kernel(ScanArgs a, ScanLayout lay) {
             oid3 = (int)atomicAdd(a.cursor, 1u);
         }
         scan_subject<CellT, kDefer, false>(a, m, qs, cells, entries, wr.diag, wr.lane_pos, wr.tasks, wr.blocked,
-                                           wr.wcnt, cur, a.db + cs, (int)(ce - cs), base, lane);
+                                           wr.wcnt, a.oid_base + cur, a.db + cs, (int)(ce - cs), base, lane);
         int nxt = 0;
         long long ns = 0, ne = 0;
         if (lane == 0) {

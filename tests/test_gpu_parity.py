@@ -168,3 +168,28 @@ def test_shape2_full_size(engine, matrix):
     found = set(owner.tolist())
     planted = w.db.plants[w.db.plants[:, 4] >= 100][:, 0]
     assert np.mean([p in found for p in planted]) > 0.9
+
+
+def test_host_path_overlapped_chunks(engine, matrix):
+    # ~144M residues: the host-to-host call uploads three chunks under the
+    # scans of the earlier ones; results equal the resident-database search,
+    # from pinned and from pageable host memory, and on a repeated call
+    import torch
+    w = synth.shape2(matrix, n_subjects=400_000)
+    q = w.queries[0]
+    ref = gpu_search(engine, q, w.db.residues, w.db.offsets)
+    got = engine.blastp_host(q, default_params(), w.db.residues, w.db.offsets)
+    assert_same(got, (ref.counters, ref.hsp_off, ref.hsps_as_array()), "pageable")
+    pin = torch.empty(len(w.db.residues), dtype=torch.uint8, pin_memory=True)
+    pin.numpy()[:] = w.db.residues
+    got = engine.blastp_host(q, default_params(), pin.numpy(), w.db.offsets)
+    assert_same(got, (ref.counters, ref.hsp_off, ref.hsps_as_array()), "pinned")
+    got = engine.blastp_host(q, default_params(), pin.numpy(), w.db.offsets)
+    assert_same(got, (ref.counters, ref.hsp_off, ref.hsps_as_array()), "pinned, again")
+
+
+def test_host_path_rejects_bad_residues(engine):
+    res = np.ones(1000, dtype=np.uint8)
+    res[777] = 50
+    with pytest.raises(BpError):
+        engine.blastp_host(enc("WCWHEAL"), default_params(), res, np.array([0, 500, 1000], np.int64))
