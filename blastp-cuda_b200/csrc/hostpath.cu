@@ -3,7 +3,7 @@
 //
 // The reference copies the whole database to the device and only then
 // launches its kernel (gpu_blastp.cu:139-210).  Here the subjects are cut
-// into chunks of about 64 MiB of residues; a copy stream uploads them one
+// into chunks (8, 16, 32, then 64 MiB of residues); a copy stream uploads them one
 // after the other, each followed by an event, and the engine stream checks
 // and scans every chunk as soon as its event has fired, so the transfer of
 // chunk k+1 runs under the scan of chunk k.  The query's table is built on
@@ -86,11 +86,14 @@ extern "C" bp_status bp_blastp_host(bp_engine* e, const uint8_t* query, int32_t 
         if (offsets[i + 1] < offsets[i] || offsets[i + 1] - offsets[i] > (1 << 29))
             return bp_set_error(e, BP_ERR_INVALID, "bp_blastp_host: offsets must be non-decreasing, subjects < 2^29");
     CKH(cudaSetDevice(e->device), "cudaSetDevice");
-    // chunks of whole subjects, about kChunkResidues residues each
+    // chunks of whole subjects: 8 MiB, 16, 32, then 64 MiB of residues, so
+    // the first scan starts after a short upload
     std::vector<int32_t> cf(1, 0);
+    int64_t chunk = kChunkResidues / 8;
     while (cf.back() < n_subjects) {
         const int32_t s = cf.back();
-        const int64_t limit = offsets[s] + kChunkResidues;
+        const int64_t limit = offsets[s] + chunk;
+        chunk = std::min(kChunkResidues, chunk * 2);
         int32_t t = (int32_t)(std::upper_bound(offsets + s + 1, offsets + n_subjects + 1, limit) - offsets) - 1;
         cf.push_back(std::max(t, s + 1));
     }
