@@ -122,12 +122,35 @@ extern "C" bp_status bp_blastp_host(bp_engine* e, const uint8_t* query, int32_t 
         h->subj_cap = n;
     }
     CKH(grow_buf(&h->d_words, &h->words_cap, (size_t)n_chunks + 2), "cudaMalloc(words)");
-    // the query table first (it synchronises the engine stream), then the
-    // engine's record scratch
+    // uploads: from pinned memory every chunk is queued now, so the transfers
+    // start under the table build; from pageable memory each copy call returns
+    // only once staged, so those copies are interleaved with the scans below
+    cudaPointerAttributes pa;
+    const bool pinned = cudaPointerGetAttributes(&pa, residues) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+    auto upload = [&](int k) -> cudaError_t {
+        const int64_t lo = offsets[cf[k]], hi = offsets[cf[k + 1]];
+        cudaError_t err = cudaSuccess;
+        if (hi > lo)
+            err = cudaMemcpyAsync(h->d_res + lo, residues + lo, (size_t)(hi - lo), cudaMemcpyHostToDevice, h->copy);
+        if (err == cudaSuccess) err = cudaEventRecord(h->ready[k], h->copy);
+        return err;
+    };
+    CKH(cudaMemsetAsync(h->d_res + n_residues, 0, res_bytes - (size_t)n_residues, h->copy), "memset(pad)");
+    CKH(cudaMemcpyAsync(h->d_off, offsets, ((size_t)n_subjects + 1) * 8, cudaMemcpyHostToDevice, h->copy),
+        "upload offsets");
+    if (pinned)
+        for (int k = 0; k < n_chunks; ++k) CKH(upload(k), "upload residues");
+    // the query table (it synchronises the engine stream), then the engine's
+    // record scratch
     bp_query* q = nullptr;
     bp_status st = bp_query_create(e, query, qlen, p, &q);
-    if (st != BP_OK) return st;
+    if (st != BP_OK) {
+        cudaStreamSynchronize(h->copy);
+        return st;
+    }
     if (!bp_scan_fits(q->qlen, q->diag_len, q->n_entries, e->smem_optin)) {
+        cudaStreamSynchronize(h->copy);
         bp_query_destroy(q);
         return bp_set_error(e, BP_ERR_TOO_LARGE, "bp_blastp_host: query too long for the diagonal array");
     }
@@ -141,21 +164,12 @@ extern "C" bp_status bp_blastp_host(bp_engine* e, const uint8_t* query, int32_t 
     size_t bc = (size_t)e->blocksum_cap;
     CKH(grow_buf(&e->d_blocksums, &bc, (size_t)bp_order_blocksums_needed(n_subjects)), "cudaMalloc(sums)");
     e->blocksum_cap = (int32_t)bc;
-    // chunk k's upload is queued on the copy stream, its check and scan on the
-    // engine stream behind the chunk's event: from pinned memory every copy
-    // is queued at once and the scans follow the copies; from pageable memory
-    // each copy call returns once staged, while the scans already queued run
+    // chunk k's check and scan run on the engine stream behind its event
     CKH(cudaMemsetAsync(h->d_words, 0, ((size_t)n_chunks + 2) * sizeof(uint32_t), e->stream), "memset");
-    CKH(cudaMemsetAsync(h->d_res + n_residues, 0, res_bytes - (size_t)n_residues, h->copy), "memset(pad)");
-    CKH(cudaMemcpyAsync(h->d_off, offsets, ((size_t)n_subjects + 1) * 8, cudaMemcpyHostToDevice, h->copy),
-        "upload offsets");
     CKH(cudaEventRecord(e->ev_scan0, e->stream), "cudaEventRecord");
     for (int k = 0; k < n_chunks; ++k) {
         const int64_t lo = offsets[cf[k]], hi = offsets[cf[k + 1]];
-        if (hi > lo)
-            CKH(cudaMemcpyAsync(h->d_res + lo, residues + lo, (size_t)(hi - lo), cudaMemcpyHostToDevice, h->copy),
-                "upload residues");
-        CKH(cudaEventRecord(h->ready[k], h->copy), "cudaEventRecord");
+        if (!pinned) CKH(upload(k), "upload residues");
         CKH(cudaStreamWaitEvent(e->stream, h->ready[k], 0), "cudaStreamWaitEvent");
         CKH(bp_launch_check_residues(e, e->stream, h->d_res + lo, hi - lo, h->d_words + 1), "residue check");
         ScanArgs a{};
