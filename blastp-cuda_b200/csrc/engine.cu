@@ -38,7 +38,8 @@ namespace {
 // `res` may start anywhere: the bytes before its first 16-byte boundary and
 // after its last one are checked one by one, the rest with 16-byte loads.
 __global__ void check_residues(const uint8_t* __restrict__ res, int64_t n, uint32_t* bad) {
-    const int64_t head = std::min<int64_t>(n, (int64_t)((16 - ((uintptr_t)res & 15)) & 15));
+    const int64_t lead = (int64_t)((16 - ((uintptr_t)res & 15)) & 15);
+    const int64_t head = lead < n ? lead : n;
     const uint8_t* body = res + head;                       // 16-byte aligned
     const int64_t n16 = (n - head) / 16;
     uint32_t b = 0;

@@ -145,40 +145,47 @@ __device__ __forceinline__ void warp_xdrop(const int8_t* m, const uint8_t* __res
 
 // The same walk by one lane, letter by letter as in the reference's loops
 // (gpu_blastp_kernel.cu:435-481, :503-549); residues are fetched four
-// letters ahead so the loads overlap the dependent score chain.
+// letters at a time so the loads overlap the dependent score chain, and only
+// the last, partial group of four checks the walk's end.
 template <bool kRight>
 __device__ __forceinline__ void lane_xdrop(const int8_t* m, const uint8_t* __restrict__ subj, const uint8_t* qry,
                                            int s0, int q0, int n, int start, int xdrop, int& best, int& best_i,
                                            int& stop_i) {
+    constexpr int D = kRight ? 1 : -1;
+    const uint8_t* qp = qry + q0;
+    const uint8_t* sp = subj + s0;
     int run = start;
     best = start;
     best_i = -1;
     stop_i = n;
-    for (int i0 = 0; i0 < n; i0 += 4) {
+    int i0 = 0;
+    for (; i0 + 4 <= n; i0 += 4) {
         int sc[4];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const int i = i0 + k;
-            sc[k] = i < n ? (kRight ? msc(m, qry[q0 + i], __ldg(subj + s0 + i))
-                                    : msc(m, qry[q0 - i], __ldg(subj + s0 - i)))
-                          : 0;
-        }
-        bool stop = false;
+        for (int k = 0; k < 4; ++k) sc[k] = msc(m, qp[D * (i0 + k)], __ldg(sp + D * (i0 + k)));
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-            if (!stop && i0 + k < n) {
-                run += sc[k];
-                if (run > best) {
-                    best = run;
-                    best_i = i0 + k;
-                }
-                if (best - run >= xdrop || (kRight && run <= 0)) {
-                    stop = true;
-                    stop_i = i0 + k;
-                }
+            run += sc[k];
+            if (run > best) {
+                best = run;
+                best_i = i0 + k;
+            }
+            if (best - run >= xdrop || (kRight && run <= 0)) {
+                stop_i = i0 + k;
+                return;
             }
         }
-        if (stop) break;
+    }
+    for (; i0 < n; ++i0) {
+        run += msc(m, qp[D * i0], __ldg(sp + D * i0));
+        if (run > best) {
+            best = run;
+            best_i = i0;
+        }
+        if (best - run >= xdrop || (kRight && run <= 0)) {
+            stop_i = i0;
+            return;
+        }
     }
 }
 
