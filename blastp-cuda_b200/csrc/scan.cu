@@ -44,8 +44,6 @@ extern __shared__ __align__(128) uint8_t bp_smem[];
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
-constexpr uint32_t kFlag = 0x80000000u;     // diagonal: an extension reached past this point
-constexpr uint32_t kPend = 0x40000000u;     // diagonal: an extension waits in the task queue
 constexpr int kP = 4;                       // word positions per lane per window
 constexpr int kMaxWarps = 32;
 constexpr int kTaskCap = 64;                // queued extensions per warp
@@ -56,6 +54,26 @@ constexpr int kLaneWalkMin = 6;             // from this many queued extensions 
 // for the queue, and extend each pair at once with the whole warp.
 constexpr int kDeferMinQlen = 320;
 constexpr int kMaxMembers = 32;             // queries per packed table (BP_MAX_PACK_MEMBERS)
+// Diagonal arrays of at most this many entries use 16-bit entries.
+constexpr int kNarrowMaxL = 8192;
+
+// One diagonal entry: a stamp (position + the warp's running offset) and two
+// flags -- an extension reached past this point, or an extension waits in
+// the task queue.  Stamps stay below kMax: the offset is rebased when the
+// next window could produce a larger one.  16-bit entries halve the per-warp
+// arrays, so long queries keep more warps (and their tables) on chip.
+template <typename DiagT>
+struct DiagBits;
+template <>
+struct DiagBits<uint32_t> {
+    static constexpr uint32_t kFlag = 0x80000000u, kPend = 0x40000000u, kStamp = 0x3fffffffu;
+    static constexpr int kMax = 1 << 30;
+};
+template <>
+struct DiagBits<uint16_t> {
+    static constexpr uint32_t kFlag = 0x8000u, kPend = 0x4000u, kStamp = 0x3fffu;
+    static constexpr int kMax = 1 << 14;
+};
 
 }  // namespace
 
@@ -261,11 +279,12 @@ __device__ __forceinline__ void load_window(const uint8_t* __restrict__ sub, int
 }
 
 // One warp's view of the subject it is scanning.
+template <typename DiagT>
 struct WarpScan {
     const ScanArgs* a;
     const int8_t* m;
     const uint8_t* qs;
-    uint32_t* diag;
+    DiagT* diag;
     Task* tasks;
     Task* blocked;
     const uint8_t* sub;
@@ -283,8 +302,8 @@ struct Member {
     int k, q_lo, q_hi, xdrop, cutoff;
 };
 
-template <bool kPacked>
-__device__ __forceinline__ Member member_at(const WarpScan& w, int hq) {
+template <bool kPacked, class W>
+__device__ __forceinline__ Member member_at(const W& w, int hq) {
     const ScanArgs& a = *w.a;
     Member r;
     if (kPacked) {
@@ -306,8 +325,8 @@ __device__ __forceinline__ Member member_at(const WarpScan& w, int hq) {
 
 // Appends the reported HSPs of this round (one candidate per lane).  Packed:
 // the record goes to its query's segment, with query offsets relative to it.
-template <bool kPacked>
-__device__ __forceinline__ void emit(WarpScan& w, bool found, int key, int hs, int hq, const ExtOut& x) {
+template <bool kPacked, class W>
+__device__ __forceinline__ void emit(W& w, bool found, int key, int hs, int hq, const ExtOut& x) {
     const unsigned fm = __ballot_sync(kFull, found);
     if (!fm) return;
     uint32_t pos0 = 0;
@@ -339,8 +358,12 @@ __device__ __forceinline__ void emit(WarpScan& w, bool found, int key, int hs, i
     }
 }
 
-__device__ __forceinline__ uint32_t diag_after(const ExtOut& x, int hs, int base) {
-    return x.right_ext ? ((uint32_t)(x.s_last - (BP_WORD - 1) + base) | kFlag) : (uint32_t)(hs + base);
+// The diagonal's entry after an extension of the pair ending at hs: past the
+// right walk's last letter when it ran, else the hit itself.
+template <typename DiagT>
+__device__ __forceinline__ DiagT diag_after(const ExtOut& x, int hs, int base) {
+    return (DiagT)(x.right_ext ? ((uint32_t)(x.s_last - (BP_WORD - 1) + base) | DiagBits<DiagT>::kFlag)
+                               : (uint32_t)(hs + base));
 }
 
 // Applies up to 32 hits (one per lane, in hit-stream order by lane) to the
@@ -349,8 +372,9 @@ __device__ __forceinline__ uint32_t diag_after(const ExtOut& x, int hs, int base
 // pending, and a hit on a pending diagonal joins the blocked list (needs room
 // for 32 more tasks and 32 more blocked hits).  Otherwise each pair is
 // extended at once by the whole warp, one after the other.
-template <bool kDefer, bool kPacked>
-__device__ __forceinline__ void apply_hits(WarpScan& w, bool hv, int hs, int hq, int d, int key, bool count) {
+template <bool kDefer, bool kPacked, typename DiagT>
+__device__ __forceinline__ void apply_hits(WarpScan<DiagT>& w, bool hv, int hs, int hq, int d, int key, bool count) {
+    using B = DiagBits<DiagT>;
     const unsigned vmask = __ballot_sync(kFull, hv);
     if (!vmask) return;
     if (kPacked && count && hv) atomicAdd(&w.wcnt[3 * w.a->member_of[hq]], 1);   // word hits per query
@@ -368,14 +392,14 @@ __device__ __forceinline__ void apply_hits(WarpScan& w, bool hv, int hs, int hq,
             pending = false;
             const uint32_t v = w.diag[d];
             const int stamp = hs + w.base;
-            if (kDefer && (v & kPend)) {
+            if (kDefer && (v & B::kPend)) {
                 blk = true;
-            } else if (v & kFlag) {
+            } else if (v & B::kFlag) {
                 // an extension already covered this hit; the first hit past it restarts the diagonal
-                if (stamp >= (int)(v & ~kFlag)) w.diag[d] = (uint32_t)stamp;
+                if (stamp >= (int)(v & B::kStamp)) w.diag[d] = (DiagT)stamp;
             } else {
                 diff = hs - ((int)v - w.base);
-                if (diff >= window) w.diag[d] = (uint32_t)stamp;
+                if (diff >= window) w.diag[d] = (DiagT)stamp;
                 else if (diff >= BP_WORD) need = true;
             }
         }
@@ -386,7 +410,7 @@ __device__ __forceinline__ void apply_hits(WarpScan& w, bool hv, int hs, int hq,
             const unsigned nm = __ballot_sync(kFull, need);
             if (need) {
                 w.tasks[w.nt + __popc(nm & w.lt)] = Task{hs, key, d, (uint32_t)hq | ((uint32_t)diff << 16)};
-                w.diag[d] = kPend | (uint32_t)(hs + w.base);
+                w.diag[d] = (DiagT)(B::kPend | (uint32_t)(hs + w.base));
                 if (kPacked) atomicAdd(&w.wcnt[3 * w.a->member_of[hq] + 2], 1);
                 else ++w.ext;
             }
@@ -408,8 +432,7 @@ __device__ __forceinline__ void apply_hits(WarpScan& w, bool hv, int hs, int hq,
                     if (kPacked) atomicAdd(&w.wcnt[3 * mb.k + 2], 1);
                     else ++w.ext;
                     found = x.score >= mb.cutoff;
-                    w.diag[d] = x.right_ext ? ((uint32_t)(x.s_last - (BP_WORD - 1) + w.base) | kFlag)
-                                            : (uint32_t)(hs + w.base);
+                    w.diag[d] = diag_after<DiagT>(x, hs, w.base);
                 }
             }
             __syncwarp();
@@ -419,8 +442,8 @@ __device__ __forceinline__ void apply_hits(WarpScan& w, bool hv, int hs, int hq,
 }
 
 // Walks every queued extension and writes its outcome into its diagonal.
-template <bool kPacked>
-__device__ void flush_tasks(WarpScan& w) {
+template <bool kPacked, typename DiagT>
+__device__ void flush_tasks(WarpScan<DiagT>& w) {
     const int nt = w.nt;
     if (nt >= kLaneWalkMin) {
         for (int t0 = 0; t0 < nt; t0 += 32) {
@@ -435,7 +458,7 @@ __device__ void flush_tasks(WarpScan& w) {
                 x = extend_two_hit<false>(w.m, w.sub, w.slen, w.qs, mb.q_lo, mb.q_hi, tk.hs - diff + BP_WORD, tk.hs,
                                           hq, mb.xdrop, w.lane);
                 found = x.score >= mb.cutoff;
-                w.diag[tk.d] = diag_after(x, tk.hs, w.base);
+                w.diag[tk.d] = diag_after<DiagT>(x, tk.hs, w.base);
             }
             emit<kPacked>(w, found, tk.key, tk.hs, (int)(tk.hqx & 0xffffu), x);
         }
@@ -447,7 +470,7 @@ __device__ void flush_tasks(WarpScan& w) {
             const ExtOut x = extend_two_hit<true>(w.m, w.sub, w.slen, w.qs, mb.q_lo, mb.q_hi, tk.hs - diff + BP_WORD,
                                                   tk.hs, hq, mb.xdrop, w.lane);
             const bool found = w.lane == 0 && x.score >= mb.cutoff;
-            if (w.lane == 0) w.diag[tk.d] = diag_after(x, tk.hs, w.base);
+            if (w.lane == 0) w.diag[tk.d] = diag_after<DiagT>(x, tk.hs, w.base);
             emit<kPacked>(w, found, tk.key, tk.hs, hq, x);
         }
     }
@@ -458,8 +481,8 @@ __device__ void flush_tasks(WarpScan& w) {
 // Resolves the queued extensions, then replays the blocked hits once, in
 // order.  A replayed hit may queue a new extension (and block the hits after
 // it on its diagonal again); the blocked list is rewritten in place.
-template <bool kPacked>
-__device__ void resolve(WarpScan& w) {
+template <bool kPacked, typename DiagT>
+__device__ void resolve(WarpScan<DiagT>& w) {
     flush_tasks<kPacked>(w);
     const int n = w.nb;
     w.nb = 0;
@@ -476,18 +499,43 @@ __device__ void resolve(WarpScan& w) {
 
 // Scans one subject.  oid: the subject's counter/record segment; packed: its
 // index in the batch's subject range (each query's segment is derived).
-template <typename CellT, bool kDefer, bool kPacked>
+// Moves the stamp offset so that position s0 gets stamp `window`: every entry
+// moves down by delta = base + s0 - window with its flag, and an entry that
+// would go below zero -- a hit or an extension end more than `window` before
+// s0 -- becomes 0, which every later hit reads the same way (a diagonal whose
+// last event is out of reach).  Nothing may be pending.  All n entries are
+// swept, the batched kernel's longer arrays included, so no older stamp can
+// look recent after the move.
+template <typename DiagT>
+__device__ __forceinline__ void rebase_diag(DiagT* diag, int n, int delta, int lane) {
+    using B = DiagBits<DiagT>;
+    for (int i = lane; i < n; i += 32) {
+        const uint32_t v = diag[i];
+        const int st = (int)(v & B::kStamp);
+        diag[i] = st >= delta ? (DiagT)((uint32_t)(st - delta) | (v & B::kFlag)) : (DiagT)0;
+    }
+    __syncwarp();
+}
+
+// Scans one subject.  The stamps written while a window starting at s0 is
+// processed (hits, pending marks, extension ends) are at most
+// base + s0 + 128 + qlen (a hit lies before s0 + 128 and a right walk ends
+// within qlen letters of it), so the offset is reset when that bound could
+// reach DiagBits::kMax.  clear_len: entries of the warp's whole array.
+template <typename CellT, bool kDefer, bool kPacked, typename DiagT>
 __device__ void scan_subject(const ScanArgs& a, const int8_t* m, const uint8_t* qs, const CellT* cells,
-                             const uint16_t* entries, uint32_t* diag, uint32_t* lane_pos, Task* tasks,
+                             const uint16_t* entries, DiagT* diag, int clear_len, uint32_t* lane_pos, Task* tasks,
                              Task* blocked, int* wcnt, int oid, const uint8_t* __restrict__ sub, int slen, int& base,
                              int lane) {
+    using B = DiagBits<DiagT>;
     const int L = a.diag_len;
-    if (base + slen + a.window > (1 << 30)) {
-        for (int i = lane; i < L; i += 32) diag[i] = 0;
+    if (base + a.qlen + 129 >= B::kMax) {
+        // every entry is older than this subject: start the offset again
+        for (int i = lane; i < clear_len; i += 32) diag[i] = 0;
         __syncwarp();
         base = a.window;
     }
-    WarpScan w;
+    WarpScan<DiagT> w;
     w.a = &a;
     w.m = m;
     w.qs = qs;
@@ -514,6 +562,14 @@ __device__ void scan_subject(const ScanArgs& a, const int8_t* m, const uint8_t* 
     int r[kP + 2];
     load_window(sub, slen, lane * kP, r);
     for (int s0 = 0; s0 <= last_pos; s0 += 32 * kP) {
+        if (base + s0 + 129 + a.qlen >= B::kMax) {
+            // long subject: settle every queued extension, then move the offset
+            if (kDefer)
+                while (w.nt > 0 || w.nb > 0) resolve<kPacked>(w);
+            rebase_diag(diag, clear_len, base + s0 - a.window, lane);
+            base = a.window - s0;
+            w.base = base;
+        }
         int rn[kP + 2];
         load_window(sub, slen, s0 + 32 * kP + lane * kP, rn);    // next window, in flight meanwhile
         const int sl = s0 + lane * kP;
@@ -605,26 +661,29 @@ __device__ void scan_subject(const ScanArgs& a, const int8_t* m, const uint8_t* 
 
 // Per-warp regions: diagonal array, lane position table, task queue, blocked
 // list, and (packed layouts) per-member counters.
+template <typename DiagT>
 struct WarpRegions {
-    uint32_t* diag;
+    DiagT* diag;
     uint32_t* lane_pos;
     Task* tasks;
     Task* blocked;
     int* wcnt;
 };
 
-__device__ __forceinline__ WarpRegions warp_regions(const ScanLayout& lay, int warp, int lane) {
+template <typename DiagT>
+__device__ __forceinline__ WarpRegions<DiagT> warp_regions(const ScanLayout& lay, int warp, int lane) {
     uint8_t* wr = bp_smem + lay.off_warps + (size_t)warp * lay.warp_bytes;
-    WarpRegions r;
-    r.diag = reinterpret_cast<uint32_t*>(wr);
-    r.lane_pos = reinterpret_cast<uint32_t*>(wr + (size_t)lay.L * 4) + lane * kP * 2;
-    r.tasks = reinterpret_cast<Task*>(wr + (size_t)lay.L * 4 + 32 * kP * 2 * 4);
+    const size_t db = (size_t)lay.L * sizeof(DiagT);     // L is a multiple of 32: 16-byte aligned
+    WarpRegions<DiagT> r;
+    r.diag = reinterpret_cast<DiagT*>(wr);
+    r.lane_pos = reinterpret_cast<uint32_t*>(wr + db) + lane * kP * 2;
+    r.tasks = reinterpret_cast<Task*>(wr + db + 32 * kP * 2 * 4);
     r.blocked = r.tasks + kTaskCap;
     r.wcnt = reinterpret_cast<int*>(r.blocked + kBlkCap);
     return r;
 }
 
-template <typename CellT, bool kCellsSmem, bool kDefer>
+template <typename CellT, bool kCellsSmem, bool kDefer, typename DiagT>
 __global__ void __launch_bounds__(kMaxWarps * 32, 1)
 scan_kernel(ScanArgs a, ScanLayout lay) {
     uint8_t* sm = bp_smem;
@@ -645,7 +704,7 @@ scan_kernel(ScanArgs a, ScanLayout lay) {
     }
     for (int i = threadIdx.x; i < a.qlen; i += blockDim.x) qs[i] = a.query[i];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const WarpRegions wr = warp_regions(lay, warp, lane);
+    const WarpRegions<DiagT> wr = warp_regions<DiagT>(lay, warp, lane);
     for (int i = lane; i < lay.L; i += 32) wr.diag[i] = 0;
     __syncthreads();
 
@@ -684,8 +743,9 @@ scan_kernel(ScanArgs a, ScanLayout lay) {
             }
             oid3 = (int)atomicAdd(a.cursor, 1u);
         }
-        scan_subject<CellT, kDefer, false>(a, m, qs, cells, entries, wr.diag, wr.lane_pos, wr.tasks, wr.blocked,
-                                           wr.wcnt, a.oid_base + cur, a.db + cs, (int)(ce - cs), base, lane);
+        scan_subject<CellT, kDefer, false>(a, m, qs, cells, entries, wr.diag, lay.L, wr.lane_pos, wr.tasks,
+                                           wr.blocked, wr.wcnt, a.oid_base + cur, a.db + cs, (int)(ce - cs), base,
+                                           lane);
         int nxt = 0;
         long long ns = 0, ne = 0;
         if (lane == 0) {
@@ -719,7 +779,7 @@ struct BatchCtl {
 // (query, subject) pair sees exactly the plain kernel's sequence of events,
 // so every query's result is its single-query result; counters and records
 // are indexed by segment = query * n_subjects + subject.
-template <typename CellT, bool kCellsSmem, bool kDefer, bool kPacked>
+template <typename CellT, bool kCellsSmem, bool kDefer, bool kPacked, typename DiagT>
 __global__ void __launch_bounds__(kMaxWarps * 32, 1)
 scan_batch_kernel(BatchArgs b, ScanLayout lay) {
     uint8_t* sm = bp_smem;
@@ -728,7 +788,7 @@ scan_batch_kernel(BatchArgs b, ScanLayout lay) {
     BatchCtl* ctl = reinterpret_cast<BatchCtl*>(sm + lay.off_ctl);
     for (int i = threadIdx.x; i < 28 * BP_MROW; i += blockDim.x) m[i] = b.matrix[i];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const WarpRegions wr = warp_regions(lay, warp, lane);
+    const WarpRegions<DiagT> wr = warp_regions<DiagT>(lay, warp, lane);
     for (int i = lane; i < lay.L; i += 32) wr.diag[i] = 0;
     int base = b.window;   // diagonal stamp offset, carried across queries (stale stamps stay stale)
     int cur_q = -1;
@@ -817,16 +877,11 @@ scan_batch_kernel(BatchArgs b, ScanLayout lay) {
             if (s >= (unsigned)wi.count) break;
             const int oid = wi.first + (int)s;
             const long long so = b.db_off[oid], eo = b.db_off[oid + 1];
-            if (base + (int)(eo - so) + b.window > (1 << 30)) {
-                // the stamp offset is about to wrap: clear the whole array, since
-                // queries with a longer array than this one read past its end
-                for (int i = lane; i < lay.L; i += 32) wr.diag[i] = 0;
-                __syncwarp();
-                base = b.window;
-            }
-            scan_subject<CellT, kDefer, kPacked>(ctl->args, m, qs, cells, entries, wr.diag, wr.lane_pos, wr.tasks,
-                                                 wr.blocked, wr.wcnt, (int)(seg0 + oid - b.subject_first), b.db + so,
-                                                 (int)(eo - so), base, lane);
+            // (offset resets clear the launch's whole array, lay.L entries:
+            // queries with a longer array than this one read past its end)
+            scan_subject<CellT, kDefer, kPacked>(ctl->args, m, qs, cells, entries, wr.diag, lay.L, wr.lane_pos,
+                                                 wr.tasks, wr.blocked, wr.wcnt, (int)(seg0 + oid - b.subject_first),
+                                                 b.db + so, (int)(eo - so), base, lane);
         }
         __syncthreads();
     }
@@ -858,7 +913,8 @@ ScanLayout make_layout(int qlen, int L, int64_t n_entries, int warps, int cells_
         off = al(off + qlen, 16);
     }
     l.off_warps = (int)off;
-    const long long wb = al((long long)L * 4 + 32 * kP * 2 * 4 + (kTaskCap + kBlkCap) * (long long)sizeof(Task) +
+    const long long diag_bytes = (long long)L * (L <= kNarrowMaxL ? 2 : 4);
+    const long long wb = al(diag_bytes + 32 * kP * 2 * 4 + (kTaskCap + kBlkCap) * (long long)sizeof(Task) +
                                 (packed ? 3 * 4 * kMaxMembers : 0),
                             16);
     l.warp_bytes = (int)(wb > big ? big : wb);
@@ -889,9 +945,9 @@ bool choose_layout(int qlen, int L, int64_t n_entries, int smem_optin, ScanLayou
     return false;
 }
 
-template <typename CellT, bool kCellsSmem, bool kDefer>
+template <typename CellT, bool kCellsSmem, bool kDefer, typename DiagT>
 cudaError_t launch(bp_engine* e, const ScanArgs& a, const ScanLayout& lay) {
-    auto kern = scan_kernel<CellT, kCellsSmem, kDefer>;
+    auto kern = scan_kernel<CellT, kCellsSmem, kDefer, DiagT>;
     // the largest allowed size, not this launch's: launches of one instance
     // with different layouts (batch classes, captured graph nodes replayed
     // later) must all stay valid whatever order the attribute was set in
@@ -905,9 +961,9 @@ cudaError_t launch(bp_engine* e, const ScanArgs& a, const ScanLayout& lay) {
     return cudaGetLastError();
 }
 
-template <typename CellT, bool kCellsSmem, bool kDefer, bool kPacked>
+template <typename CellT, bool kCellsSmem, bool kDefer, bool kPacked, typename DiagT>
 cudaError_t launch_batch(bp_engine* e, cudaStream_t stream, const BatchArgs& b, const ScanLayout& lay, int grid) {
-    auto kern = scan_batch_kernel<CellT, kCellsSmem, kDefer, kPacked>;
+    auto kern = scan_batch_kernel<CellT, kCellsSmem, kDefer, kPacked, DiagT>;
     // the largest allowed size, not this launch's: launches of one instance
     // with different layouts (batch classes, captured graph nodes replayed
     // later) must all stay valid whatever order the attribute was set in
@@ -929,17 +985,27 @@ int bp_diag_len(int qlen, int window) {
     return (int)(n < 128 ? 128 : (n > (1LL << 30) ? (1LL << 30) : n));
 }
 
+// Diagonal arrays longer than kNarrowMaxL (query + window above about 8,000)
+// use 32-bit entries and always queue their extensions (the results are the
+// same either way).
 template <bool kPacked>
 cudaError_t launch_batch_layout(bp_engine* e, cudaStream_t stream, const BatchArgs& b, const ScanLayout& lay,
                                 int grid, bool defer) {
-    if (defer) {
-        if (lay.cells_mode == 0) return launch_batch<uint16_t, true, true, kPacked>(e, stream, b, lay, grid);
-        if (lay.cells_mode == 1) return launch_batch<uint32_t, true, true, kPacked>(e, stream, b, lay, grid);
-        return launch_batch<uint32_t, false, true, kPacked>(e, stream, b, lay, grid);
+    using N = uint16_t;
+    if (!kPacked && lay.L > kNarrowMaxL) {
+        if (lay.cells_mode == 0) return launch_batch<uint16_t, true, true, false, uint32_t>(e, stream, b, lay, grid);
+        if (lay.cells_mode == 1) return launch_batch<uint32_t, true, true, false, uint32_t>(e, stream, b, lay, grid);
+        return launch_batch<uint32_t, false, true, false, uint32_t>(e, stream, b, lay, grid);
     }
-    if (lay.cells_mode == 0) return launch_batch<uint16_t, true, false, kPacked>(e, stream, b, lay, grid);
-    if (lay.cells_mode == 1) return launch_batch<uint32_t, true, false, kPacked>(e, stream, b, lay, grid);
-    return launch_batch<uint32_t, false, false, kPacked>(e, stream, b, lay, grid);
+    if (lay.L > kNarrowMaxL) return cudaErrorInvalidValue;   // packed tables are short
+    if (defer) {
+        if (lay.cells_mode == 0) return launch_batch<uint16_t, true, true, kPacked, N>(e, stream, b, lay, grid);
+        if (lay.cells_mode == 1) return launch_batch<uint32_t, true, true, kPacked, N>(e, stream, b, lay, grid);
+        return launch_batch<uint32_t, false, true, kPacked, N>(e, stream, b, lay, grid);
+    }
+    if (lay.cells_mode == 0) return launch_batch<uint16_t, true, false, kPacked, N>(e, stream, b, lay, grid);
+    if (lay.cells_mode == 1) return launch_batch<uint32_t, true, false, kPacked, N>(e, stream, b, lay, grid);
+    return launch_batch<uint32_t, false, false, kPacked, N>(e, stream, b, lay, grid);
 }
 
 cudaError_t bp_launch_scan_batch(bp_engine* e, cudaStream_t stream, const BatchArgs& b, int32_t max_qlen,
@@ -969,12 +1035,20 @@ bool bp_scan_fits(int32_t qlen, int32_t diag_len, int64_t n_entries, int smem_op
 cudaError_t bp_launch_scan(bp_engine* e, const ScanArgs& a) {
     ScanLayout lay;
     if (!choose_layout(a.qlen, a.diag_len, a.n_entries, e->smem_optin, &lay)) return cudaErrorInvalidValue;
-    if (a.qlen >= kDeferMinQlen) {
-        if (lay.cells_mode == 0) return launch<uint16_t, true, true>(e, a, lay);
-        if (lay.cells_mode == 1) return launch<uint32_t, true, true>(e, a, lay);
-        return launch<uint32_t, false, true>(e, a, lay);
+    using N = uint16_t;
+    if (lay.L > kNarrowMaxL) {
+        // (32-bit arrays always queue their extensions: a query that is short
+        // but has a very large window gets the same results either way)
+        if (lay.cells_mode == 0) return launch<uint16_t, true, true, uint32_t>(e, a, lay);
+        if (lay.cells_mode == 1) return launch<uint32_t, true, true, uint32_t>(e, a, lay);
+        return launch<uint32_t, false, true, uint32_t>(e, a, lay);
     }
-    if (lay.cells_mode == 0) return launch<uint16_t, true, false>(e, a, lay);
-    if (lay.cells_mode == 1) return launch<uint32_t, true, false>(e, a, lay);
-    return launch<uint32_t, false, false>(e, a, lay);
+    if (a.qlen >= kDeferMinQlen) {
+        if (lay.cells_mode == 0) return launch<uint16_t, true, true, N>(e, a, lay);
+        if (lay.cells_mode == 1) return launch<uint32_t, true, true, N>(e, a, lay);
+        return launch<uint32_t, false, true, N>(e, a, lay);
+    }
+    if (lay.cells_mode == 0) return launch<uint16_t, true, false, N>(e, a, lay);
+    if (lay.cells_mode == 1) return launch<uint32_t, true, false, N>(e, a, lay);
+    return launch<uint32_t, false, false, N>(e, a, lay);
 }
