@@ -45,6 +45,10 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kP = 4;                       // word positions per lane per window
+// Per-lane position table row: kP hit counts and kP cell starts, padded to an
+// odd number of words so that the 32 lanes' rows start in 32 different banks
+// (rows read by the hit flattening, by owner lane, stay conflict-free too).
+constexpr int kRow = 2 * kP + 1;
 constexpr int kMaxWarps = 32;
 constexpr int kTaskCap = 64;                // queued extensions per warp
 constexpr int kBlkCap = 64;                 // hits waiting behind queued extensions, per warp
@@ -558,7 +562,7 @@ __device__ void scan_subject(const ScanArgs& a, const int8_t* m, const uint8_t* 
     int hits = 0, key_base = 0;
     int s0m = 0;                         // s0 mod L
     const int last_pos = slen - BP_WORD;
-    const uint32_t* my_row = lane_pos - lane * kP * 2;
+    const uint32_t* my_row = lane_pos - lane * kRow;
     int r[kP + 2];
     load_window(sub, slen, lane * kP, r);
     for (int s0 = 0; s0 <= last_pos; s0 += 32 * kP) {
@@ -607,7 +611,7 @@ __device__ void scan_subject(const ScanArgs& a, const int8_t* m, const uint8_t* 
             int hs = 0, hq = 0, d = 0;
             if (hv) {
                 const uint32_t local = j - (o_incl - o_cnt);
-                const uint32_t* op = my_row + lo * kP * 2;
+                const uint32_t* op = my_row + lo * kRow;
                 int p = 0;
 #pragma unroll
                 for (int t = 1; t < kP; ++t)
@@ -676,8 +680,8 @@ __device__ __forceinline__ WarpRegions<DiagT> warp_regions(const ScanLayout& lay
     const size_t db = (size_t)lay.L * sizeof(DiagT);     // L is a multiple of 32: 16-byte aligned
     WarpRegions<DiagT> r;
     r.diag = reinterpret_cast<DiagT*>(wr);
-    r.lane_pos = reinterpret_cast<uint32_t*>(wr + db) + lane * kP * 2;
-    r.tasks = reinterpret_cast<Task*>(wr + db + 32 * kP * 2 * 4);
+    r.lane_pos = reinterpret_cast<uint32_t*>(wr + db) + lane * kRow;
+    r.tasks = reinterpret_cast<Task*>(wr + db + 32 * kRow * 4);
     r.blocked = r.tasks + kTaskCap;
     r.wcnt = reinterpret_cast<int*>(r.blocked + kBlkCap);
     return r;
@@ -914,7 +918,7 @@ ScanLayout make_layout(int qlen, int L, int64_t n_entries, int warps, int cells_
     }
     l.off_warps = (int)off;
     const long long diag_bytes = (long long)L * (L <= kNarrowMaxL ? 2 : 4);
-    const long long wb = al(diag_bytes + 32 * kP * 2 * 4 + (kTaskCap + kBlkCap) * (long long)sizeof(Task) +
+    const long long wb = al(diag_bytes + 32 * kRow * 4 + (kTaskCap + kBlkCap) * (long long)sizeof(Task) +
                                 (packed ? 3 * 4 * kMaxMembers : 0),
                             16);
     l.warp_bytes = (int)(wb > big ? big : wb);
@@ -978,6 +982,8 @@ cudaError_t launch_batch(bp_engine* e, cudaStream_t stream, const BatchArgs& b, 
 
 static_assert(sizeof(BatchCtl) <= 512, "batched control block must fit its shared-memory slot");
 static_assert(sizeof(Task) == 16, "task layout");
+static_assert((32 * kRow * 4) % 16 == 0, "the task queue after the position table stays 16-byte aligned");
+static_assert(kRow % 2 == 1, "odd row stride: one bank per lane");
 static_assert(kMaxMembers == BP_MAX_PACK_MEMBERS, "pack size limit");
 
 int bp_diag_len(int qlen, int window) {
