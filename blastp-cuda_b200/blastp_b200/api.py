@@ -202,14 +202,23 @@ class Engine:
         return ({"chunk_residues": best.chunk_residues, "schedule": best.schedule, "max_warps": best.max_warps,
                  "pack_residues": best.pack_residues}, out)
 
-    def blastp_host(self, query, params, residues, offsets, hsp_cap=None):
-        """End-to-end: host buffers in, host buffers out (one C call)."""
+    def blastp_host(self, query, params, residues, offsets, hsp_cap=None, counters=None, hsp_off=None):
+        """End-to-end: host buffers in, host buffers out (one C call).
+        counters ([n, 3] int32) and hsp_off ([n + 1] int64) may be given, e.g.
+        views of pinned memory, into which each chunk's counters are copied
+        as soon as its scan ends."""
         q = np.ascontiguousarray(query, dtype=np.uint8)
         res = np.ascontiguousarray(residues, dtype=np.uint8)
         off = np.ascontiguousarray(offsets, dtype=np.int64)
         n = len(off) - 1
-        counters = np.zeros((n, 3), dtype=np.int32)
-        hoff = np.zeros(n + 1, dtype=np.int64)
+        if counters is None:
+            counters = np.zeros((n, 3), dtype=np.int32)
+        if hsp_off is None:
+            hsp_off = np.zeros(n + 1, dtype=np.int64)
+        if (counters.shape != (n, 3) or counters.dtype != np.int32 or not counters.flags.c_contiguous or
+                hsp_off.shape != (n + 1,) or hsp_off.dtype != np.int64 or not hsp_off.flags.c_contiguous):
+            raise ValueError("counters must be [n, 3] int32 and hsp_off [n + 1] int64, both contiguous")
+        hoff = hsp_off
         nh = ctypes.c_int64(0)
         cap = hsp_cap if hsp_cap is not None else max(4096, n // 2)
         hsps = np.zeros(cap, dtype=HSP_DTYPE)

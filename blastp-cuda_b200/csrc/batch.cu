@@ -160,6 +160,8 @@ bp_status enqueue(bp_batch* b) {
         a.recs = b->d_recs;
         a.rec_cap = b->cap;
         a.rec_count = b->d_counts;
+        a.long_ids = b->db->d_long;
+        a.long_min = b->db->long_min;
         if (a.n_items > 0)
             CKB(bp_launch_scan_batch(e, st, a, k.max_qlen, k.max_len, k.max_entries, k.grid, b->opt.max_warps,
                                      k.packed),
@@ -504,11 +506,11 @@ bp_status bp_search_batch(bp_engine* e, const bp_db* db, const bp_query* const* 
             for (int32_t qi : unit_queries[ui]) k.est += queries[qi]->hits_per_residue;
             for (int32_t c = 0; c < n_chunks; ++c) {
                 for (int32_t qi : unit_queries[ui]) item_pos[(size_t)qi * n_chunks + c] = (int32_t)items.size();
-                WorkItem w;
+                WorkItem w{};
                 w.qid = ui;
                 w.first = b->chunk_first[c];
                 w.count = b->chunk_first[c + 1] - b->chunk_first[c];
-                w.pad = 0;
+                bp_long_slice(db->h_long, w.first, w.count, &w.long_first, &w.n_long);
                 items.push_back(w);
             }
         }

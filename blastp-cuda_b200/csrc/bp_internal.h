@@ -57,6 +57,11 @@ extern "C" bp_status bp_blastp_host_staged(bp_engine* e, const uint8_t* query, i
                                            int32_t n_subjects, int32_t* counters, int64_t* hsp_off, bp_hsp* hsps,
                                            int64_t hsp_cap, int64_t* n_hsps);
 // Sets *bad (device word) when any of n residues is >= 28.
+// Subjects [first, first + n): a length outside [0, 2^29] sets *bad; the
+// indices of those of at least long_min residues are appended (in no
+// particular order) to out, their number added to *count.
+cudaError_t bp_launch_long_list(bp_engine* e, cudaStream_t stream, const int64_t* d_off, int32_t first, int32_t n,
+                                int32_t long_min, int32_t* out, int32_t* count, uint32_t* bad);
 cudaError_t bp_launch_check_residues(bp_engine* e, cudaStream_t stream, const uint8_t* d_res, int64_t n,
                                      uint32_t* d_bad);
 
@@ -72,6 +77,11 @@ struct bp_db {
     int32_t n = 0;
     int64_t nres = 0;
     std::vector<int64_t> h_off;          // host copy of the offsets (chunk planning)
+    // subjects of at least long_min residues (ascending indices), scanned
+    // first by every launch (see bp_long_subjects)
+    std::vector<int32_t> h_long;
+    int32_t* d_long = nullptr;
+    int32_t long_min = 0;
 };
 
 struct bp_query {
@@ -127,6 +137,14 @@ struct ScanArgs {
     uint32_t* cursor;           // subject cursor (chunks of 32)
     uint32_t* error;            // set when a bounded wait runs out
     int32_t oid_base;           // plain kernel: counters and records of subject i go to oid_base + i
+    // longest first: the range's subjects of at least long_min residues
+    // (absolute indices, ascending) are taken before the others, which then
+    // skip them; n_long = 0: plain index order
+    const int32_t* long_ids;
+    int32_t n_long;
+    int32_t long_min;
+    const int32_t* n_long_at;   // when set, n_long is read from here (a list built on the device)
+    const uint32_t* abort_if;   // when set and non-zero at launch, the kernel scans nothing
     // packed tables (batched kernel): per query {id, offset, length, x-drop,
     // cutoff}, the query of every packed offset, and the segment stride
     const int32_t* members;
@@ -153,7 +171,9 @@ struct BatchQuery {
 struct WorkItem {
     int32_t qid;            // query of the batch
     int32_t first, count;   // subjects [first, first+count)
-    int32_t pad;
+    int32_t long_first;     // its long subjects: BatchArgs::long_ids[long_first .. long_first + n_long)
+    int32_t n_long;
+    int32_t pad[3];
 };
 struct BatchArgs {
     const uint8_t* db;
@@ -174,6 +194,8 @@ struct BatchArgs {
     HspRec* recs;
     uint32_t rec_cap;
     uint32_t* rec_count;
+    const int32_t* long_ids;      // the database's long subjects (see WorkItem), and their threshold
+    int32_t long_min;
 };
 
 // ---- host helpers ---------------------------------------------------------
@@ -184,6 +206,14 @@ bp_status bp_db_alloc(bp_engine* e, int64_t n_residues, int32_t n_subjects, bp_d
 bp_status bp_db_finish(bp_engine* e, bp_db* db);
 }
 bp_status bp_set_cuda_error(bp_engine* e, cudaError_t err, const char* what);
+// Longest-first order: a persistent launch ends when its last warp finishes
+// its last subject, so subjects of at least twice the mean length (and at
+// least 64 residues) go first.  Returns the threshold and appends the
+// indices of [0, n) that reach it, ascending.
+int32_t bp_long_subjects(const int64_t* off, int32_t n, std::vector<int32_t>* out);
+int32_t bp_long_threshold(int64_t n_residues, int32_t n);
+// The part [*lo, *lo + *cnt) of a sorted index list inside [first, first + n).
+void bp_long_slice(const std::vector<int32_t>& ids, int32_t first, int32_t n, int32_t* lo, int32_t* cnt);
 bp_status bp_set_error(bp_engine* e, bp_status s, const std::string& msg);
 void bp_fill_matrix28(int8_t out[28 * 28]);
 // Expected word hits per subject residue of a table under the Robinson &

@@ -75,6 +75,36 @@ constexpr int kPoolSlots = 1024;
 
 }  // namespace
 
+__global__ void long_list(const int64_t* __restrict__ off, int32_t first, int32_t n, int32_t long_min,
+                          int32_t* __restrict__ out, int32_t* count, uint32_t* bad) {
+    uint32_t b = 0;
+    const int lane = threadIdx.x & 31;
+    for (int32_t i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
+        const int32_t i = i0 + threadIdx.x;
+        bool is_long = false;
+        if (i < n) {
+            const int64_t d = off[(int64_t)first + i + 1] - off[(int64_t)first + i];
+            b |= (d < 0 || d > (1 << 29)) ? 1u : 0u;
+            is_long = d >= long_min;
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, is_long);
+        int32_t pos = 0;
+        if (lane == 0 && m) pos = atomicAdd(count, __popc(m));
+        pos = __shfl_sync(0xffffffffu, pos, 0);
+        if (is_long) out[pos + __popc(m & ((1u << lane) - 1u))] = first + i;
+    }
+    if (b) atomicOr(bad, 1u);
+}
+
+cudaError_t bp_launch_long_list(bp_engine* e, cudaStream_t stream, const int64_t* d_off, int32_t first, int32_t n,
+                                int32_t long_min, int32_t* out, int32_t* count, uint32_t* bad) {
+    if (n <= 0) return cudaSuccess;
+    const int blocks = (int)std::min<int64_t>((int64_t)e->sm_count * 2, ((int64_t)n + 255) / 256);
+    long_list<<<blocks, 256, 0, stream>>>(d_off, first, n, long_min, out, count, bad);
+    e->launches += 1;
+    return cudaGetLastError();
+}
+
 cudaError_t bp_launch_check_residues(bp_engine* e, cudaStream_t stream, const uint8_t* d_res, int64_t n,
                                      uint32_t* d_bad) {
     if (n <= 0) return cudaSuccess;
@@ -158,6 +188,10 @@ bp_status bp_run_search(bp_engine* e, bp_result* r) {
     a.rec_count = e->d_counts;
     a.cursor = e->d_counts + 1;
     a.error = e->d_counts + 2;
+    int32_t long_lo = 0;
+    bp_long_slice(db->h_long, r->first, n, &long_lo, &a.n_long);
+    a.long_ids = db->d_long ? db->d_long + long_lo : nullptr;
+    a.long_min = db->long_min;
     CK(cudaEventRecord(e->ev_scan0, e->stream), "cudaEventRecord");
     if (n > 0) CK(bp_launch_scan(e, a), "scan kernel launch");
     CK(cudaEventRecord(e->ev_scan1, e->stream), "cudaEventRecord");
@@ -168,6 +202,27 @@ bp_status bp_run_search(bp_engine* e, bp_result* r) {
        "copy counts");
     r->n_hsps = -1;
     return BP_OK;
+}
+
+int32_t bp_long_threshold(int64_t n_residues, int32_t n) {
+    if (n <= 0) return 0;
+    const int64_t t = std::max<int64_t>(64, 2 * (n_residues / n));
+    return (int32_t)std::min<int64_t>(t, (int64_t)1 << 30);
+}
+
+int32_t bp_long_subjects(const int64_t* off, int32_t n, std::vector<int32_t>* out) {
+    if (n <= 0) return 0;
+    const int32_t long_min = bp_long_threshold(off[n] - off[0], n);
+    for (int32_t i = 0; i < n; ++i)
+        if (off[i + 1] - off[i] >= long_min) out->push_back(i);
+    return long_min;
+}
+
+void bp_long_slice(const std::vector<int32_t>& ids, int32_t first, int32_t n, int32_t* lo, int32_t* cnt) {
+    const auto a = std::lower_bound(ids.begin(), ids.end(), first);
+    const auto b = std::lower_bound(a, ids.end(), (int32_t)std::min<int64_t>((int64_t)first + n, INT32_MAX));
+    *lo = (int32_t)(a - ids.begin());
+    *cnt = (int32_t)(b - a);
 }
 
 extern "C" {
@@ -296,8 +351,17 @@ bp_status bp_db_alloc(bp_engine* e, int64_t n_residues, int32_t n_subjects, bp_d
     return BP_OK;
 }
 
-// Zero padding after the residues, then the residue-code check on the device.
+// Zero padding after the residues, the residue-code check on the device, and
+// the longest-first list (db->h_off must be set).
 bp_status bp_db_finish(bp_engine* e, bp_db* db) {
+    db->h_long.clear();
+    db->long_min = bp_long_subjects(db->h_off.data(), db->n, &db->h_long);
+    if (!db->h_long.empty()) {
+        CK(cudaMalloc((void**)&db->d_long, db->h_long.size() * sizeof(int32_t)), "cudaMalloc(long subjects)");
+        CK(cudaMemcpyAsync(db->d_long, db->h_long.data(), db->h_long.size() * sizeof(int32_t),
+                           cudaMemcpyHostToDevice, e->stream),
+           "upload long subjects");
+    }
     const size_t padded = (size_t)((db->nres + 15) & ~15LL) + 32;
     CK(cudaMemsetAsync(db->d_res + db->nres, 0, padded - (size_t)db->nres, e->stream), "pad database");
     CK(cudaMemsetAsync(e->d_counts + 3, 0, sizeof(uint32_t), e->stream), "memset(check)");
@@ -335,12 +399,12 @@ bp_status bp_db_create(bp_engine* e, const uint8_t* residues, int64_t n_residues
         bp_db_destroy(db);
         return bp_set_cuda_error(e, err, "database upload");
     }
+    db->h_off.assign(offsets, offsets + (size_t)n_subjects + 1);
     st = bp_db_finish(e, db);
     if (st != BP_OK) {
         bp_db_destroy(db);
         return st;
     }
-    db->h_off.assign(offsets, offsets + (size_t)n_subjects + 1);
     *out = db;
     return BP_OK;
 }
@@ -369,12 +433,12 @@ bp_status bp_db_create_device(bp_engine* e, const uint8_t* d_residues, int64_t n
         bp_db_destroy(db);
         return bp_set_cuda_error(e, err, "database copy");
     }
+    db->h_off.swap(off);
     st = bp_db_finish(e, db);
     if (st != BP_OK) {
         bp_db_destroy(db);
         return st;
     }
-    db->h_off.swap(off);
     *out = db;
     return BP_OK;
 }
@@ -383,6 +447,7 @@ void bp_db_destroy(bp_db* db) {
     if (!db) return;
     cudaFree(db->d_res);
     cudaFree(db->d_off);
+    cudaFree(db->d_long);
     delete db;
 }
 

@@ -6,12 +6,16 @@
 // into chunks (8, 16, 32, then 64 MiB of residues); a copy stream uploads them one
 // after the other, each followed by an event, and the engine stream checks
 // and scans every chunk as soon as its event has fired, so the transfer of
-// chunk k+1 runs under the scan of chunk k.  The query's table is built on
-// the engine stream while the first chunk is in flight.  All chunks write
-// one set of per-subject counters and one record buffer (subject index =
-// chunk start + index in the chunk), ordered once at the end.  Device
-// buffers are grow-only and kept by the engine, so repeated calls allocate
-// nothing once warm.
+// chunk k+1 runs under the scan of chunk k.  The host checks only the chunk
+// boundaries (they bound the copies); every subject's length is checked on
+// the device, chunk by chunk, by the kernel that also lists the chunk's long
+// subjects for the scan to take first, and a chunk whose check failed is not
+// scanned.  The query's table is built on the engine stream meanwhile.  All chunks write one set
+// of per-subject counters and one record buffer (subject index = chunk start
+// + index in the chunk), ordered once at the end; into pinned host memory
+// each chunk's counters go back as soon as its scan ends.  Device buffers are
+// grow-only and kept by the engine, so repeated calls allocate nothing once
+// warm.
 #include <string.h>
 
 #include <algorithm>
@@ -26,8 +30,10 @@
     } while (0)
 
 struct HostPath {
-    cudaStream_t copy = nullptr;
-    std::vector<cudaEvent_t> ready;     // one per chunk slot
+    cudaStream_t copy = nullptr;        // uploads
+    cudaStream_t back = nullptr;        // per-chunk counter read-back
+    std::vector<cudaEvent_t> ready;     // one per chunk slot: uploaded
+    std::vector<cudaEvent_t> scanned;   // one per chunk slot: scanned
     uint8_t* d_res = nullptr;
     size_t res_cap = 0;
     int64_t* d_off = nullptr;
@@ -35,14 +41,38 @@ struct HostPath {
     int32_t* d_counters = nullptr;
     int64_t* d_hsp_off = nullptr;
     size_t subj_cap = 0;
-    uint32_t* d_words = nullptr;        // [0] records, [1] bad residue, [2..] chunk cursors
+    // [0] records, [1] bad residue, [2] bad offsets, [3] unused,
+    // [4 .. 4 + chunks) chunk cursors, then the chunks' long-subject counts
+    uint32_t* d_words = nullptr;
     size_t words_cap = 0;
     uint32_t* h_words = nullptr;        // pinned read-back
+    int32_t* d_long = nullptr;          // chunk k's long subjects at d_long + its first subject
+    size_t long_cap = 0;
 };
 
 namespace {
 
 constexpr int64_t kChunkResidues = (int64_t)64 << 20;
+
+// First index t in [lo, hi] with off[t] > limit, for non-decreasing off; on
+// any other array still some index in [lo, hi] (the caller checks the
+// boundaries it gets before trusting them).
+int32_t first_above(const int64_t* off, int32_t lo, int32_t hi, int64_t limit) {
+    while (lo < hi) {
+        const int32_t mid = lo + (hi - lo) / 2;
+        if (off[mid] <= limit) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+
+bool is_pinned(const void* p) {
+    cudaPointerAttributes pa;
+    const bool pinned = p && cudaPointerGetAttributes(&pa, p) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+    return pinned;
+}
 
 template <class T>
 cudaError_t grow_buf(T** p, size_t* cap, size_t need) {
@@ -61,13 +91,17 @@ void bp_host_path_free(bp_engine* e) {
     HostPath* h = e->host_path;
     if (!h) return;
     if (h->copy) cudaStreamSynchronize(h->copy);
+    if (h->back) cudaStreamSynchronize(h->back);
     for (cudaEvent_t ev : h->ready) cudaEventDestroy(ev);
+    for (cudaEvent_t ev : h->scanned) cudaEventDestroy(ev);
     if (h->copy) cudaStreamDestroy(h->copy);
+    if (h->back) cudaStreamDestroy(h->back);
     cudaFree(h->d_res);
     cudaFree(h->d_off);
     cudaFree(h->d_counters);
     cudaFree(h->d_hsp_off);
     cudaFree(h->d_words);
+    cudaFree(h->d_long);
     if (h->h_words) cudaFreeHost(h->h_words);
     delete h;
     e->host_path = nullptr;
@@ -82,10 +116,6 @@ extern "C" bp_status bp_blastp_host(bp_engine* e, const uint8_t* query, int32_t 
         return bp_set_error(e, BP_ERR_INVALID, "bp_blastp_host: bad argument");
     if (offsets[0] != 0 || offsets[n_subjects] != n_residues)
         return bp_set_error(e, BP_ERR_INVALID, "bp_blastp_host: offsets must run from 0 to n_residues");
-    for (int32_t i = 0; i < n_subjects; ++i)
-        if (offsets[i + 1] < offsets[i] || offsets[i + 1] - offsets[i] > (1 << 29))
-            return bp_set_error(e, BP_ERR_INVALID, "bp_blastp_host: offsets must be non-decreasing, subjects < 2^29");
-    CKH(cudaSetDevice(e->device), "cudaSetDevice");
     // chunks of whole subjects: 8 MiB, 16, 32, then 64 MiB of residues, so
     // the first scan starts after a short upload
     std::vector<int32_t> cf(1, 0);
@@ -94,18 +124,27 @@ extern "C" bp_status bp_blastp_host(bp_engine* e, const uint8_t* query, int32_t 
         const int32_t s = cf.back();
         const int64_t limit = offsets[s] + chunk;
         chunk = std::min(kChunkResidues, chunk * 2);
-        int32_t t = (int32_t)(std::upper_bound(offsets + s + 1, offsets + n_subjects + 1, limit) - offsets) - 1;
+        const int32_t t = first_above(offsets, s + 1, n_subjects + 1, limit) - 1;
         cf.push_back(std::max(t, s + 1));
     }
     const int n_chunks = (int)cf.size() - 1;
+    // the chunk boundaries bound every copy: they must be in order and in
+    // range before anything is queued (every subject is checked on the device)
+    for (int k = 0; k < n_chunks; ++k)
+        if (offsets[cf[k]] < 0 || offsets[cf[k + 1]] < offsets[cf[k]] || offsets[cf[k + 1]] > n_residues)
+            return bp_set_error(e, BP_ERR_INVALID, "bp_blastp_host: offsets must be non-decreasing, subjects < 2^29");
+    CKH(cudaSetDevice(e->device), "cudaSetDevice");
     if (!e->host_path) e->host_path = new HostPath();
     HostPath* h = e->host_path;
     if (!h->copy) CKH(cudaStreamCreateWithFlags(&h->copy, cudaStreamNonBlocking), "cudaStreamCreate");
+    if (!h->back) CKH(cudaStreamCreateWithFlags(&h->back, cudaStreamNonBlocking), "cudaStreamCreate");
     if (!h->h_words) CKH(cudaMallocHost((void**)&h->h_words, 4 * sizeof(uint32_t)), "cudaMallocHost");
     while ((int)h->ready.size() < n_chunks) {
         cudaEvent_t ev = nullptr;
         CKH(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreate");
         h->ready.push_back(ev);
+        CKH(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreate");
+        h->scanned.push_back(ev);
     }
     const size_t res_bytes = (size_t)((n_residues + 15) & ~15LL) + 32;
     CKH(grow_buf(&h->d_res, &h->res_cap, res_bytes), "cudaMalloc(database)");
@@ -121,13 +160,13 @@ extern "C" bp_status bp_blastp_host(bp_engine* e, const uint8_t* query, int32_t 
         CKH(cudaMalloc((void**)&h->d_hsp_off, n * sizeof(int64_t)), "cudaMalloc(offsets)");
         h->subj_cap = n;
     }
-    CKH(grow_buf(&h->d_words, &h->words_cap, (size_t)n_chunks + 2), "cudaMalloc(words)");
+    CKH(grow_buf(&h->d_words, &h->words_cap, 4 + 2 * (size_t)n_chunks), "cudaMalloc(words)");
+    CKH(grow_buf(&h->d_long, &h->long_cap, (size_t)std::max(n_subjects, 1)), "cudaMalloc(long subjects)");
     // uploads: from pinned memory every chunk is queued now, so the transfers
     // start under the table build; from pageable memory each copy call returns
     // only once staged, so those copies are interleaved with the scans below
-    cudaPointerAttributes pa;
-    const bool pinned = cudaPointerGetAttributes(&pa, residues) == cudaSuccess && pa.type == cudaMemoryTypeHost;
-    cudaGetLastError();
+    const bool pinned = is_pinned(residues);
+    const bool counters_pinned = counters && n_subjects > 0 && is_pinned(counters);
     auto upload = [&](int k) -> cudaError_t {
         const int64_t lo = offsets[cf[k]], hi = offsets[cf[k + 1]];
         cudaError_t err = cudaSuccess;
@@ -141,6 +180,7 @@ extern "C" bp_status bp_blastp_host(bp_engine* e, const uint8_t* query, int32_t 
         "upload offsets");
     if (pinned)
         for (int k = 0; k < n_chunks; ++k) CKH(upload(k), "upload residues");
+    const int32_t long_min = bp_long_threshold(n_residues, n_subjects);
     // the query table (it synchronises the engine stream), then the engine's
     // record scratch
     bp_query* q = nullptr;
@@ -164,14 +204,21 @@ extern "C" bp_status bp_blastp_host(bp_engine* e, const uint8_t* query, int32_t 
     size_t bc = (size_t)e->blocksum_cap;
     CKH(grow_buf(&e->d_blocksums, &bc, (size_t)bp_order_blocksums_needed(n_subjects)), "cudaMalloc(sums)");
     e->blocksum_cap = (int32_t)bc;
-    // chunk k's check and scan run on the engine stream behind its event
-    CKH(cudaMemsetAsync(h->d_words, 0, ((size_t)n_chunks + 2) * sizeof(uint32_t), e->stream), "memset");
+    // chunk k's checks and scan run on the engine stream behind its event
+    uint32_t* bad_res = h->d_words + 1;
+    uint32_t* bad_off = h->d_words + 2;
+    uint32_t* cursors = h->d_words + 4;
+    int32_t* long_counts = (int32_t*)(h->d_words + 4 + n_chunks);
+    CKH(cudaMemsetAsync(h->d_words, 0, (4 + 2 * (size_t)n_chunks) * sizeof(uint32_t), e->stream), "memset");
     CKH(cudaEventRecord(e->ev_scan0, e->stream), "cudaEventRecord");
     for (int k = 0; k < n_chunks; ++k) {
         const int64_t lo = offsets[cf[k]], hi = offsets[cf[k + 1]];
         if (!pinned) CKH(upload(k), "upload residues");
         CKH(cudaStreamWaitEvent(e->stream, h->ready[k], 0), "cudaStreamWaitEvent");
-        CKH(bp_launch_check_residues(e, e->stream, h->d_res + lo, hi - lo, h->d_words + 1), "residue check");
+        CKH(bp_launch_check_residues(e, e->stream, h->d_res + lo, hi - lo, bad_res), "residue check");
+        CKH(bp_launch_long_list(e, e->stream, h->d_off, cf[k], cf[k + 1] - cf[k], long_min, h->d_long + cf[k],
+                                long_counts + k, bad_off),
+            "offsets check");
         ScanArgs a{};
         a.db = h->d_res;
         a.db_off = h->d_off;
@@ -191,26 +238,45 @@ extern "C" bp_status bp_blastp_host(bp_engine* e, const uint8_t* query, int32_t 
         a.recs = e->d_recs;
         a.rec_cap = e->rec_cap;
         a.rec_count = h->d_words;
-        a.cursor = h->d_words + 2 + k;
-        a.error = h->d_words + 1;
+        a.cursor = cursors + k;
+        a.error = bad_res;
         a.oid_base = cf[k];
+        a.long_ids = h->d_long + cf[k];
+        a.n_long_at = long_counts + k;
+        a.long_min = long_min;
+        a.abort_if = bad_off;
         CKH(bp_launch_scan(e, a), "scan kernel launch");
+        if (counters_pinned && cf[k + 1] > cf[k]) {
+            // this chunk's counters are final: back to the host under the next scans
+            CKH(cudaEventRecord(h->scanned[k], e->stream), "cudaEventRecord");
+            CKH(cudaStreamWaitEvent(h->back, h->scanned[k], 0), "cudaStreamWaitEvent");
+            CKH(cudaMemcpyAsync(counters + 3 * (int64_t)cf[k], h->d_counters + 3 * (int64_t)cf[k],
+                                (size_t)(cf[k + 1] - cf[k]) * 12, cudaMemcpyDeviceToHost, h->back),
+                "read counters");
+        }
     }
     CKH(cudaEventRecord(e->ev_scan1, e->stream), "cudaEventRecord");
     // records written and the residue check, then outputs sized by the records
-    CKH(cudaMemcpyAsync(h->h_words, h->d_words, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, e->stream),
+    CKH(cudaMemcpyAsync(h->h_words, h->d_words, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, e->stream),
         "read counts");
     CKH(cudaStreamSynchronize(e->stream), "pipelined search");
     float ms = 0.f;
     if (cudaEventElapsedTime(&ms, e->ev_scan0, e->ev_scan1) == cudaSuccess) e->last_scan_ms = ms;
     cudaGetLastError();
     const uint32_t recs = h->h_words[0];
+    if (h->h_words[2]) {
+        cudaStreamSynchronize(h->back);
+        bp_query_destroy(q);
+        return bp_set_error(e, BP_ERR_INVALID, "bp_blastp_host: offsets must be non-decreasing, subjects < 2^29");
+    }
     if (h->h_words[1]) {
+        cudaStreamSynchronize(h->back);
         bp_query_destroy(q);
         return bp_set_error(e, BP_ERR_INVALID, "bp_blastp_host: residue code >= 28");
     }
     if (recs > e->rec_cap) {
         // more HSPs than the record buffer held: the unpipelined path grows and re-runs
+        cudaStreamSynchronize(h->back);
         bp_query_destroy(q);
         return bp_blastp_host_staged(e, query, qlen, p, residues, n_residues, offsets, n_subjects, counters, hsp_off,
                                      hsps, hsp_cap, n_hsps);
@@ -226,7 +292,7 @@ extern "C" bp_status bp_blastp_host(bp_engine* e, const uint8_t* query, int32_t 
         "order kernels launch");
     if (n_hsps) *n_hsps = recs;
     cudaError_t err = cudaSuccess;
-    if (counters && n_subjects > 0)
+    if (counters && n_subjects > 0 && !counters_pinned)
         err = cudaMemcpyAsync(counters, h->d_counters, (size_t)n_subjects * 12, cudaMemcpyDeviceToHost, e->stream);
     if (err == cudaSuccess && hsp_off)
         err = cudaMemcpyAsync(hsp_off, h->d_hsp_off, ((size_t)n_subjects + 1) * 8, cudaMemcpyDeviceToHost, e->stream);
@@ -236,6 +302,8 @@ extern "C" bp_status bp_blastp_host(bp_engine* e, const uint8_t* query, int32_t 
     cudaFreeAsync(d_hsps, e->stream);
     cudaFreeAsync(d_keys, e->stream);
     if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
+    const cudaError_t err_back = cudaStreamSynchronize(h->back);
+    if (err == cudaSuccess) err = err_back;
     bp_query_destroy(q);
     if (err != cudaSuccess) return bp_set_cuda_error(e, err, "bp_blastp_host: results");
     return st;

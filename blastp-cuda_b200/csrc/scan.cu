@@ -663,6 +663,25 @@ __device__ void scan_subject(const ScanArgs& a, const int8_t* m, const uint8_t* 
     base += slen + a.window;
 }
 
+// Longest first (see ScanArgs::long_ids): cursor slot s < n_long is the
+// range's s-th long subject, slot n_long + i is subject i of the range,
+// skipped there when it is long (it was scanned in the first pass).
+constexpr uint32_t kSecond = 0x80000000u;   // a second-pass slot
+constexpr uint32_t kNone = 0x7fffffffu;     // past the last slot
+
+__device__ __forceinline__ uint32_t slot_subject(const ScanArgs& a, int n_long, uint32_t slot) {
+    if (slot < (uint32_t)n_long) return (uint32_t)(__ldg(a.long_ids + slot) - a.first);
+    slot -= (uint32_t)n_long;
+    return slot < (uint32_t)a.n ? (slot | kSecond) : kNone;
+}
+
+__device__ __forceinline__ bool in_range(const ScanArgs& a, uint32_t id) { return (id & ~kSecond) < (uint32_t)a.n; }
+
+// A second-pass slot of a subject the first pass scanned.
+__device__ __forceinline__ bool done_first(const ScanArgs& a, int n_long, uint32_t id, long long len) {
+    return (id & kSecond) && n_long > 0 && len >= a.long_min;
+}
+
 // Per-warp regions: diagonal array, lane position table, task queue, blocked
 // list, and (packed layouts) per-member counters.
 template <typename DiagT>
@@ -690,6 +709,9 @@ __device__ __forceinline__ WarpRegions<DiagT> warp_regions(const ScanLayout& lay
 template <typename CellT, bool kCellsSmem, bool kDefer, typename DiagT>
 __global__ void __launch_bounds__(kMaxWarps * 32, 1)
 scan_kernel(ScanArgs a, ScanLayout lay) {
+    // an earlier check on the device refused the inputs: nothing to scan
+    if (a.abort_if && *a.abort_if) return;
+    const int n_long = a.n_long_at ? *a.n_long_at : a.n_long;
     uint8_t* sm = bp_smem;
     int8_t* m = reinterpret_cast<int8_t*>(sm);
     uint8_t* qs = sm + lay.off_query;
@@ -716,41 +738,45 @@ scan_kernel(ScanArgs a, ScanLayout lay) {
     //   cur (+ cs, ce)   subject i, offsets known: scan it now
     //   oid1 (+ s1, e1)  subject i+1, offsets known: prefetch its residues now
     //   oid2             subject i+2, id known: load its offsets now
-    // and the id of subject i+3 is taken from the cursor.
-    int cur = 0, oid1 = 0, oid2 = 0;
+    // and the id of subject i+3 is taken from the cursor (slot_subject:
+    // subject index in the range, kSecond on second-pass slots, kNone past
+    // the end).
+    uint32_t cur = 0, oid1 = 0, oid2 = 0;
     long long cs = 0, ce = 0, s1 = 0, e1 = 0;
     if (lane == 0) {
-        cur = (int)atomicAdd(a.cursor, 1u);
-        oid1 = (int)atomicAdd(a.cursor, 1u);
-        oid2 = (int)atomicAdd(a.cursor, 1u);
-        if (cur < a.n) {
-            cs = a.db_off[a.first + cur];
-            ce = a.db_off[a.first + cur + 1];
+        cur = slot_subject(a, n_long, atomicAdd(a.cursor, 1u));
+        oid1 = slot_subject(a, n_long, atomicAdd(a.cursor, 1u));
+        oid2 = slot_subject(a, n_long, atomicAdd(a.cursor, 1u));
+        if (in_range(a, cur)) {
+            cs = a.db_off[a.first + (cur & ~kSecond)];
+            ce = a.db_off[a.first + (cur & ~kSecond) + 1];
         }
-        if (oid1 < a.n) {
-            s1 = a.db_off[a.first + oid1];
-            e1 = a.db_off[a.first + oid1 + 1];
+        if (in_range(a, oid1)) {
+            s1 = a.db_off[a.first + (oid1 & ~kSecond)];
+            e1 = a.db_off[a.first + (oid1 & ~kSecond) + 1];
         }
     }
     cur = __shfl_sync(kFull, cur, 0);
     cs = __shfl_sync(kFull, cs, 0);
     ce = __shfl_sync(kFull, ce, 0);
     int base = a.window;   // diagonal stamp offset (gpu_blastp_kernel.cu:308)
-    while (cur < a.n) {
+    while (in_range(a, cur)) {
         long long s2 = 0, e2 = 0;
-        int oid3 = 0;
+        uint32_t oid3 = 0;
         if (lane == 0) {
-            if (oid1 < a.n && e1 > s1) prefetch_l2(a.db + (s1 & ~15LL), (uint32_t)(((e1 + 15) & ~15LL) - (s1 & ~15LL)));
-            if (oid2 < a.n) {
-                s2 = a.db_off[a.first + oid2];
-                e2 = a.db_off[a.first + oid2 + 1];
+            if (in_range(a, oid1) && e1 > s1 && !done_first(a, n_long, oid1, e1 - s1))
+                prefetch_l2(a.db + (s1 & ~15LL), (uint32_t)(((e1 + 15) & ~15LL) - (s1 & ~15LL)));
+            if (in_range(a, oid2)) {
+                s2 = a.db_off[a.first + (oid2 & ~kSecond)];
+                e2 = a.db_off[a.first + (oid2 & ~kSecond) + 1];
             }
-            oid3 = (int)atomicAdd(a.cursor, 1u);
+            oid3 = slot_subject(a, n_long, atomicAdd(a.cursor, 1u));
         }
-        scan_subject<CellT, kDefer, false>(a, m, qs, cells, entries, wr.diag, lay.L, wr.lane_pos, wr.tasks,
-                                           wr.blocked, wr.wcnt, a.oid_base + cur, a.db + cs, (int)(ce - cs), base,
-                                           lane);
-        int nxt = 0;
+        if (!done_first(a, n_long, cur, ce - cs))
+            scan_subject<CellT, kDefer, false>(a, m, qs, cells, entries, wr.diag, lay.L, wr.lane_pos, wr.tasks,
+                                               wr.blocked, wr.wcnt, a.oid_base + (int)(cur & ~kSecond), a.db + cs,
+                                               (int)(ce - cs), base, lane);
+        uint32_t nxt = 0;
         long long ns = 0, ne = 0;
         if (lane == 0) {
             nxt = oid1;
@@ -878,9 +904,12 @@ scan_batch_kernel(BatchArgs b, ScanLayout lay) {
             unsigned s = 0;
             if (lane == 0) s = atomicAdd(&ctl->sub_ctr, 1u);
             s = __shfl_sync(kFull, s, 0);
-            if (s >= (unsigned)wi.count) break;
-            const int oid = wi.first + (int)s;
+            // longest first: the item's long subjects, then the others in order
+            if (s >= (unsigned)(wi.n_long + wi.count)) break;
+            const bool second = s >= (unsigned)wi.n_long;
+            const int oid = second ? wi.first + (int)s - wi.n_long : __ldg(b.long_ids + wi.long_first + (int)s);
             const long long so = b.db_off[oid], eo = b.db_off[oid + 1];
+            if (second && wi.n_long > 0 && eo - so >= b.long_min) continue;   // scanned in the first pass
             // (offset resets clear the launch's whole array, lay.L entries:
             // queries with a longer array than this one read past its end)
             scan_subject<CellT, kDefer, kPacked>(ctl->args, m, qs, cells, entries, wr.diag, lay.L, wr.lane_pos,

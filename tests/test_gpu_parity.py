@@ -186,6 +186,29 @@ def test_host_path_overlapped_chunks(engine, matrix):
     assert_same(got, (ref.counters, ref.hsp_off, ref.hsps_as_array()), "pinned")
     got = engine.blastp_host(q, default_params(), pin.numpy(), w.db.offsets)
     assert_same(got, (ref.counters, ref.hsp_off, ref.hsps_as_array()), "pinned, again")
+    # pinned outputs: each chunk's counters come back as soon as its scan ends
+    cnt = torch.full((w.db.n_subjects, 3), -1, dtype=torch.int32, pin_memory=True)
+    hoff = torch.full((w.db.n_subjects + 1,), -1, dtype=torch.int64, pin_memory=True)
+    got = engine.blastp_host(q, default_params(), pin.numpy(), w.db.offsets, counters=cnt.numpy(),
+                             hsp_off=hoff.numpy())
+    assert_same(got, (ref.counters, ref.hsp_off, ref.hsps_as_array()), "pinned in and out")
+
+
+def test_host_path_rejects_bad_offsets(engine):
+    # a decreasing offset inside the first chunk (the chunk boundaries are
+    # in order): refused before any scan, the engine stays usable
+    rng = np.random.default_rng(3)
+    n = 5000
+    off = np.concatenate([[0], np.cumsum(rng.integers(50, 400, size=n))]).astype(np.int64)
+    res = synth.residues(rng, int(off[-1]))
+    bad = off.copy()
+    bad[100], bad[101] = off[101], off[100]
+    q = synth.residues(rng, 300)
+    with pytest.raises(BpError):
+        engine.blastp_host(q, default_params(), res, bad)
+    got = engine.blastp_host(q, default_params(), res, off)
+    ref = gpu_search(engine, q, res, off)
+    assert_same(got, (ref.counters, ref.hsp_off, ref.hsps_as_array()), "after a refused call")
 
 
 def test_host_path_rejects_bad_residues(engine):
