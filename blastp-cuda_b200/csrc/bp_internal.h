@@ -235,7 +235,8 @@ bool bp_scan_defers(int32_t qlen);
 // ---- launchers ------------------------------------------------------------
 cudaError_t bp_launch_table_build(bp_engine* e, const uint8_t* d_q, int32_t qlen, int32_t threshold,
                                   uint32_t* d_cells, uint16_t* d_entries, uint32_t* d_counts_tmp, int pass);
-cudaError_t bp_launch_scan(bp_engine* e, const ScanArgs& a);
+cudaError_t bp_launch_scan(bp_engine* e, const ScanArgs& a);                       // on the engine stream
+cudaError_t bp_launch_scan_on(bp_engine* e, cudaStream_t stream, const ScanArgs& a);
 cudaError_t bp_launch_scan_batch(bp_engine* e, cudaStream_t stream, const BatchArgs& b, int32_t max_qlen,
                                  int32_t max_diag_len, int64_t max_entries, int grid, int max_warps, bool packed);
 // Packed table of several queries: cells = sum of the members' cells,

@@ -10,7 +10,10 @@
 // boundaries (they bound the copies); every subject's length is checked on
 // the device, chunk by chunk, by the kernel that also lists the chunk's long
 // subjects for the scan to take first, and a chunk whose check failed is not
-// scanned.  The query's table is built on the engine stream meanwhile.  All chunks write one set
+// scanned.  Checks run on their own stream and consecutive chunks' scans on
+// two streams, so a chunk's checks and its scan's first CTAs take the SMs
+// that the previous scan's last subjects leave idle.  The query's table is
+// built on the engine stream meanwhile.  All chunks write one set
 // of per-subject counters and one record buffer (subject index = chunk start
 // + index in the chunk), ordered once at the end; into pinned host memory
 // each chunk's counters go back as soon as its scan ends.  Device buffers are
@@ -32,7 +35,11 @@
 struct HostPath {
     cudaStream_t copy = nullptr;        // uploads
     cudaStream_t back = nullptr;        // per-chunk counter read-back
+    cudaStream_t checks = nullptr;      // per-chunk residue and offsets checks
+    cudaStream_t scan2 = nullptr;       // odd chunks' scans (even ones: the engine stream)
+    cudaEvent_t fork = nullptr, join = nullptr;
     std::vector<cudaEvent_t> ready;     // one per chunk slot: uploaded
+    std::vector<cudaEvent_t> checked;   // one per chunk slot: checked
     std::vector<cudaEvent_t> scanned;   // one per chunk slot: scanned
     uint8_t* d_res = nullptr;
     size_t res_cap = 0;
@@ -90,12 +97,15 @@ cudaError_t grow_buf(T** p, size_t* cap, size_t need) {
 void bp_host_path_free(bp_engine* e) {
     HostPath* h = e->host_path;
     if (!h) return;
-    if (h->copy) cudaStreamSynchronize(h->copy);
-    if (h->back) cudaStreamSynchronize(h->back);
+    for (cudaStream_t s : {h->copy, h->back, h->checks, h->scan2})
+        if (s) cudaStreamSynchronize(s);
     for (cudaEvent_t ev : h->ready) cudaEventDestroy(ev);
+    for (cudaEvent_t ev : h->checked) cudaEventDestroy(ev);
     for (cudaEvent_t ev : h->scanned) cudaEventDestroy(ev);
-    if (h->copy) cudaStreamDestroy(h->copy);
-    if (h->back) cudaStreamDestroy(h->back);
+    for (cudaEvent_t ev : {h->fork, h->join})
+        if (ev) cudaEventDestroy(ev);
+    for (cudaStream_t s : {h->copy, h->back, h->checks, h->scan2})
+        if (s) cudaStreamDestroy(s);
     cudaFree(h->d_res);
     cudaFree(h->d_off);
     cudaFree(h->d_counters);
@@ -138,11 +148,17 @@ extern "C" bp_status bp_blastp_host(bp_engine* e, const uint8_t* query, int32_t 
     HostPath* h = e->host_path;
     if (!h->copy) CKH(cudaStreamCreateWithFlags(&h->copy, cudaStreamNonBlocking), "cudaStreamCreate");
     if (!h->back) CKH(cudaStreamCreateWithFlags(&h->back, cudaStreamNonBlocking), "cudaStreamCreate");
+    if (!h->checks) CKH(cudaStreamCreateWithFlags(&h->checks, cudaStreamNonBlocking), "cudaStreamCreate");
+    if (!h->scan2) CKH(cudaStreamCreateWithFlags(&h->scan2, cudaStreamNonBlocking), "cudaStreamCreate");
+    if (!h->fork) CKH(cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming), "cudaEventCreate");
+    if (!h->join) CKH(cudaEventCreateWithFlags(&h->join, cudaEventDisableTiming), "cudaEventCreate");
     if (!h->h_words) CKH(cudaMallocHost((void**)&h->h_words, 4 * sizeof(uint32_t)), "cudaMallocHost");
     while ((int)h->ready.size() < n_chunks) {
         cudaEvent_t ev = nullptr;
         CKH(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreate");
         h->ready.push_back(ev);
+        CKH(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreate");
+        h->checked.push_back(ev);
         CKH(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreate");
         h->scanned.push_back(ev);
     }
@@ -211,14 +227,20 @@ extern "C" bp_status bp_blastp_host(bp_engine* e, const uint8_t* query, int32_t 
     int32_t* long_counts = (int32_t*)(h->d_words + 4 + n_chunks);
     CKH(cudaMemsetAsync(h->d_words, 0, (4 + 2 * (size_t)n_chunks) * sizeof(uint32_t), e->stream), "memset");
     CKH(cudaEventRecord(e->ev_scan0, e->stream), "cudaEventRecord");
+    CKH(cudaEventRecord(h->fork, e->stream), "cudaEventRecord");
+    CKH(cudaStreamWaitEvent(h->checks, h->fork, 0), "cudaStreamWaitEvent");
+    CKH(cudaStreamWaitEvent(h->scan2, h->fork, 0), "cudaStreamWaitEvent");
     for (int k = 0; k < n_chunks; ++k) {
         const int64_t lo = offsets[cf[k]], hi = offsets[cf[k + 1]];
         if (!pinned) CKH(upload(k), "upload residues");
-        CKH(cudaStreamWaitEvent(e->stream, h->ready[k], 0), "cudaStreamWaitEvent");
-        CKH(bp_launch_check_residues(e, e->stream, h->d_res + lo, hi - lo, bad_res), "residue check");
-        CKH(bp_launch_long_list(e, e->stream, h->d_off, cf[k], cf[k + 1] - cf[k], long_min, h->d_long + cf[k],
+        CKH(cudaStreamWaitEvent(h->checks, h->ready[k], 0), "cudaStreamWaitEvent");
+        CKH(bp_launch_check_residues(e, h->checks, h->d_res + lo, hi - lo, bad_res), "residue check");
+        CKH(bp_launch_long_list(e, h->checks, h->d_off, cf[k], cf[k + 1] - cf[k], long_min, h->d_long + cf[k],
                                 long_counts + k, bad_off),
             "offsets check");
+        CKH(cudaEventRecord(h->checked[k], h->checks), "cudaEventRecord");
+        cudaStream_t ss = (k & 1) ? h->scan2 : e->stream;
+        CKH(cudaStreamWaitEvent(ss, h->checked[k], 0), "cudaStreamWaitEvent");
         ScanArgs a{};
         a.db = h->d_res;
         a.db_off = h->d_off;
@@ -245,16 +267,18 @@ extern "C" bp_status bp_blastp_host(bp_engine* e, const uint8_t* query, int32_t 
         a.n_long_at = long_counts + k;
         a.long_min = long_min;
         a.abort_if = bad_off;
-        CKH(bp_launch_scan(e, a), "scan kernel launch");
+        CKH(bp_launch_scan_on(e, ss, a), "scan kernel launch");
         if (counters_pinned && cf[k + 1] > cf[k]) {
             // this chunk's counters are final: back to the host under the next scans
-            CKH(cudaEventRecord(h->scanned[k], e->stream), "cudaEventRecord");
+            CKH(cudaEventRecord(h->scanned[k], ss), "cudaEventRecord");
             CKH(cudaStreamWaitEvent(h->back, h->scanned[k], 0), "cudaStreamWaitEvent");
             CKH(cudaMemcpyAsync(counters + 3 * (int64_t)cf[k], h->d_counters + 3 * (int64_t)cf[k],
                                 (size_t)(cf[k + 1] - cf[k]) * 12, cudaMemcpyDeviceToHost, h->back),
                 "read counters");
         }
     }
+    CKH(cudaEventRecord(h->join, h->scan2), "cudaEventRecord");
+    CKH(cudaStreamWaitEvent(e->stream, h->join, 0), "cudaStreamWaitEvent");
     CKH(cudaEventRecord(e->ev_scan1, e->stream), "cudaEventRecord");
     // records written and the residue check, then outputs sized by the records
     CKH(cudaMemcpyAsync(h->h_words, h->d_words, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, e->stream),

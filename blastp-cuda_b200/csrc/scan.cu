@@ -979,7 +979,7 @@ bool choose_layout(int qlen, int L, int64_t n_entries, int smem_optin, ScanLayou
 }
 
 template <typename CellT, bool kCellsSmem, bool kDefer, typename DiagT>
-cudaError_t launch(bp_engine* e, const ScanArgs& a, const ScanLayout& lay) {
+cudaError_t launch(bp_engine* e, cudaStream_t stream, const ScanArgs& a, const ScanLayout& lay) {
     auto kern = scan_kernel<CellT, kCellsSmem, kDefer, DiagT>;
     // the largest allowed size, not this launch's: launches of one instance
     // with different layouts (batch classes, captured graph nodes replayed
@@ -989,7 +989,7 @@ cudaError_t launch(bp_engine* e, const ScanArgs& a, const ScanLayout& lay) {
     int grid = e->sm_count;
     const int need = (a.n + lay.warps - 1) / lay.warps;   // no more CTAs than subjects to feed them
     if (grid > need) grid = need > 0 ? need : 1;
-    kern<<<grid, lay.warps * 32, lay.total, e->stream>>>(a, lay);
+    kern<<<grid, lay.warps * 32, lay.total, stream>>>(a, lay);
     e->launches += 1;
     return cudaGetLastError();
 }
@@ -1067,23 +1067,25 @@ bool bp_scan_fits(int32_t qlen, int32_t diag_len, int64_t n_entries, int smem_op
     return choose_layout(qlen, diag_len, n_entries, smem_optin, &l);
 }
 
-cudaError_t bp_launch_scan(bp_engine* e, const ScanArgs& a) {
+cudaError_t bp_launch_scan(bp_engine* e, const ScanArgs& a) { return bp_launch_scan_on(e, e->stream, a); }
+
+cudaError_t bp_launch_scan_on(bp_engine* e, cudaStream_t st, const ScanArgs& a) {
     ScanLayout lay;
     if (!choose_layout(a.qlen, a.diag_len, a.n_entries, e->smem_optin, &lay)) return cudaErrorInvalidValue;
     using N = uint16_t;
     if (lay.L > kNarrowMaxL) {
         // (32-bit arrays always queue their extensions: a query that is short
         // but has a very large window gets the same results either way)
-        if (lay.cells_mode == 0) return launch<uint16_t, true, true, uint32_t>(e, a, lay);
-        if (lay.cells_mode == 1) return launch<uint32_t, true, true, uint32_t>(e, a, lay);
-        return launch<uint32_t, false, true, uint32_t>(e, a, lay);
+        if (lay.cells_mode == 0) return launch<uint16_t, true, true, uint32_t>(e, st, a, lay);
+        if (lay.cells_mode == 1) return launch<uint32_t, true, true, uint32_t>(e, st, a, lay);
+        return launch<uint32_t, false, true, uint32_t>(e, st, a, lay);
     }
     if (a.qlen >= kDeferMinQlen) {
-        if (lay.cells_mode == 0) return launch<uint16_t, true, true, N>(e, a, lay);
-        if (lay.cells_mode == 1) return launch<uint32_t, true, true, N>(e, a, lay);
-        return launch<uint32_t, false, true, N>(e, a, lay);
+        if (lay.cells_mode == 0) return launch<uint16_t, true, true, N>(e, st, a, lay);
+        if (lay.cells_mode == 1) return launch<uint32_t, true, true, N>(e, st, a, lay);
+        return launch<uint32_t, false, true, N>(e, st, a, lay);
     }
-    if (lay.cells_mode == 0) return launch<uint16_t, true, false, N>(e, a, lay);
-    if (lay.cells_mode == 1) return launch<uint32_t, true, false, N>(e, a, lay);
-    return launch<uint32_t, false, false, N>(e, a, lay);
+    if (lay.cells_mode == 0) return launch<uint16_t, true, false, N>(e, st, a, lay);
+    if (lay.cells_mode == 1) return launch<uint32_t, true, false, N>(e, st, a, lay);
+    return launch<uint32_t, false, false, N>(e, st, a, lay);
 }
