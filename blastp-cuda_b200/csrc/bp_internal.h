@@ -145,6 +145,22 @@ struct ScanArgs {
     int32_t long_min;
     const int32_t* n_long_at;   // when set, n_long is read from here (a list built on the device)
     const uint32_t* abort_if;   // when set and non-zero at launch, the kernel scans nothing
+    // streaming (the host-to-host search's single launch): the range's
+    // subjects arrive in n_chunks chunks while the kernel runs.  Chunk c holds
+    // subjects [chunk_first[c], chunk_first[c+1]) of the range, whose offsets
+    // span [chunk_lo[c], chunk_lo[c+1]); its residues start at db +
+    // chunk_base[c] and are there once chunk_flag[c] == gen.  A subject whose
+    // offsets leave its chunk sets *bad_off and is skipped; a residue code of
+    // 28 or more sets *error; a chunk not there within wait_ns sets *stalled.
+    int32_t n_chunks;
+    const int32_t* chunk_first;
+    const int64_t* chunk_lo;
+    const int64_t* chunk_base;
+    const uint32_t* chunk_flag;
+    uint32_t gen;
+    uint64_t wait_ns;
+    uint32_t* bad_off;
+    uint32_t* stalled;
     // packed tables (batched kernel): per query {id, offset, length, x-drop,
     // cutoff}, the query of every packed offset, and the segment stride
     const int32_t* members;
@@ -237,6 +253,10 @@ cudaError_t bp_launch_table_build(bp_engine* e, const uint8_t* d_q, int32_t qlen
                                   uint32_t* d_cells, uint16_t* d_entries, uint32_t* d_counts_tmp, int pass);
 cudaError_t bp_launch_scan(bp_engine* e, const ScanArgs& a);                       // on the engine stream
 cudaError_t bp_launch_scan_on(bp_engine* e, cudaStream_t stream, const ScanArgs& a);
+// The streaming scan (ScanArgs::n_chunks >= 1), for diagonal arrays of 16-bit
+// entries (bp_scan_streams); cudaErrorNotSupported otherwise.
+bool bp_scan_streams(int32_t diag_len);
+cudaError_t bp_launch_scan_stream(bp_engine* e, cudaStream_t stream, const ScanArgs& a);
 cudaError_t bp_launch_scan_batch(bp_engine* e, cudaStream_t stream, const BatchArgs& b, int32_t max_qlen,
                                  int32_t max_diag_len, int64_t max_entries, int grid, int max_warps, bool packed);
 // Packed table of several queries: cells = sum of the members' cells,

@@ -6,7 +6,18 @@
 // into chunks (8, 16, 32, then 64 MiB of residues); a copy stream uploads them one
 // after the other, each followed by an event, and the engine stream checks
 // and scans every chunk as soon as its event has fired, so the transfer of
-// chunk k+1 runs under the scan of chunk k.  The host checks only the chunk
+// chunk k+1 runs under the scan of chunk k.
+//
+// Queries whose diagonal arrays take 16-bit entries (all but those of about
+// 8,000 letters and more) are scanned by ONE streaming launch
+// (scan_stream_kernel): it starts once the offsets are up and takes the
+// subjects in order, each warp waiting (bounded) for its subject's chunk,
+// whose arrival a 4-byte copy queued after the chunk's data announces.  No
+// kernel runs on the upload stream, so the copies never wait for SMs the
+// scan holds; chunks start on 128-byte boundaries of the device buffer;
+// residue codes and offsets are checked by the scan itself.
+//
+// Otherwise each chunk gets its own scan launch.  The host checks only the chunk
 // boundaries (they bound the copies); every subject's length is checked on
 // the device, chunk by chunk, by the kernel that also lists the chunk's long
 // subjects for the scan to take first, and a chunk whose check failed is not
@@ -55,11 +66,26 @@ struct HostPath {
     uint32_t* h_words = nullptr;        // pinned read-back
     int32_t* d_long = nullptr;          // chunk k's long subjects at d_long + its first subject
     size_t long_cap = 0;
+    // streaming: chunk tables (first subjects, first offsets, device bases),
+    // arrival flags, and the value this call's flag copies write
+    uint8_t* d_tab = nullptr;
+    size_t tab_cap = 0;
+    uint8_t* h_tab = nullptr;
+    size_t h_tab_cap = 0;
+    uint32_t* d_flags = nullptr;
+    size_t flags_cap = 0;
+    uint32_t* h_gen = nullptr;
+    uint32_t gen = 0;
+    cudaEvent_t tabs_ready = nullptr;
 };
 
 namespace {
 
 constexpr int64_t kChunkResidues = (int64_t)64 << 20;
+// Streaming launch: chunks of this many residues throughout.  A chunk costs
+// only its arrival flag, and the scan, which runs about as fast as the
+// transfer, trails it by at most one chunk.
+constexpr int64_t kStreamChunkResidues = (int64_t)8 << 20;
 
 // First index t in [lo, hi] with off[t] > limit, for non-decreasing off; on
 // any other array still some index in [lo, hi] (the caller checks the
@@ -112,7 +138,12 @@ void bp_host_path_free(bp_engine* e) {
     cudaFree(h->d_hsp_off);
     cudaFree(h->d_words);
     cudaFree(h->d_long);
+    cudaFree(h->d_tab);
+    cudaFree(h->d_flags);
     if (h->h_words) cudaFreeHost(h->h_words);
+    if (h->h_tab) cudaFreeHost(h->h_tab);
+    if (h->h_gen) cudaFreeHost(h->h_gen);
+    if (h->tabs_ready) cudaEventDestroy(h->tabs_ready);
     delete h;
     e->host_path = nullptr;
 }
@@ -126,14 +157,20 @@ extern "C" bp_status bp_blastp_host(bp_engine* e, const uint8_t* query, int32_t 
         return bp_set_error(e, BP_ERR_INVALID, "bp_blastp_host: bad argument");
     if (offsets[0] != 0 || offsets[n_subjects] != n_residues)
         return bp_set_error(e, BP_ERR_INVALID, "bp_blastp_host: offsets must run from 0 to n_residues");
-    // chunks of whole subjects: 8 MiB, 16, 32, then 64 MiB of residues, so
-    // the first scan starts after a short upload
+    CKH(cudaSetDevice(e->device), "cudaSetDevice");
+    // streaming: one launch for every chunk (16-bit diagonal entries, residues
+    // in pinned memory, so that every copy is queued before the launch)
+    const bool pinned = is_pinned(residues);
+    const bool streaming = pinned && n_subjects > 0 && bp_scan_streams(bp_diag_len(qlen, p->window));
+    // chunks of whole subjects: streaming, kStreamChunkResidues each;
+    // otherwise 8 MiB, 16, 32, then 64 MiB of residues, so the first scan
+    // starts after a short upload and later launches stay few
     std::vector<int32_t> cf(1, 0);
-    int64_t chunk = kChunkResidues / 8;
+    int64_t chunk = streaming ? kStreamChunkResidues : kChunkResidues / 8;
     while (cf.back() < n_subjects) {
         const int32_t s = cf.back();
         const int64_t limit = offsets[s] + chunk;
-        chunk = std::min(kChunkResidues, chunk * 2);
+        if (!streaming) chunk = std::min(kChunkResidues, chunk * 2);
         const int32_t t = first_above(offsets, s + 1, n_subjects + 1, limit) - 1;
         cf.push_back(std::max(t, s + 1));
     }
@@ -143,7 +180,6 @@ extern "C" bp_status bp_blastp_host(bp_engine* e, const uint8_t* query, int32_t 
     for (int k = 0; k < n_chunks; ++k)
         if (offsets[cf[k]] < 0 || offsets[cf[k + 1]] < offsets[cf[k]] || offsets[cf[k + 1]] > n_residues)
             return bp_set_error(e, BP_ERR_INVALID, "bp_blastp_host: offsets must be non-decreasing, subjects < 2^29");
-    CKH(cudaSetDevice(e->device), "cudaSetDevice");
     if (!e->host_path) e->host_path = new HostPath();
     HostPath* h = e->host_path;
     if (!h->copy) CKH(cudaStreamCreateWithFlags(&h->copy, cudaStreamNonBlocking), "cudaStreamCreate");
@@ -162,7 +198,19 @@ extern "C" bp_status bp_blastp_host(bp_engine* e, const uint8_t* query, int32_t 
         CKH(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreate");
         h->scanned.push_back(ev);
     }
-    const size_t res_bytes = (size_t)((n_residues + 15) & ~15LL) + 32;
+    // streaming: chunk k's residues at device offset base[k], 128-byte aligned
+    std::vector<int64_t> base(n_chunks, 0);
+    size_t res_bytes = (size_t)((n_residues + 15) & ~15LL) + 32;
+    if (streaming) {
+        int64_t at = 0;
+        for (int k = 0; k < n_chunks; ++k) {
+            base[k] = at;
+            at = (at + (offsets[cf[k + 1]] - offsets[cf[k]]) + 127) & ~127LL;
+        }
+        res_bytes = (size_t)at + 256;
+    } else {
+        for (int k = 0; k < n_chunks; ++k) base[k] = offsets[cf[k]];
+    }
     CKH(grow_buf(&h->d_res, &h->res_cap, res_bytes), "cudaMalloc(database)");
     CKH(grow_buf(&h->d_off, &h->off_cap, (size_t)n_subjects + 1), "cudaMalloc(offsets)");
     if (h->subj_cap < (size_t)n_subjects + 1) {
@@ -181,19 +229,56 @@ extern "C" bp_status bp_blastp_host(bp_engine* e, const uint8_t* query, int32_t 
     // uploads: from pinned memory every chunk is queued now, so the transfers
     // start under the table build; from pageable memory each copy call returns
     // only once staged, so those copies are interleaved with the scans below
-    const bool pinned = is_pinned(residues);
-    const bool counters_pinned = counters && n_subjects > 0 && is_pinned(counters);
+    // (chunked launches only: each chunk's counters go back as its scan ends)
+    const bool counters_pinned = !streaming && counters && n_subjects > 0 && is_pinned(counters);
     auto upload = [&](int k) -> cudaError_t {
         const int64_t lo = offsets[cf[k]], hi = offsets[cf[k + 1]];
         cudaError_t err = cudaSuccess;
         if (hi > lo)
-            err = cudaMemcpyAsync(h->d_res + lo, residues + lo, (size_t)(hi - lo), cudaMemcpyHostToDevice, h->copy);
+            err = cudaMemcpyAsync(h->d_res + base[k], residues + lo, (size_t)(hi - lo), cudaMemcpyHostToDevice,
+                                  h->copy);
         if (err == cudaSuccess) err = cudaEventRecord(h->ready[k], h->copy);
+        // streaming: the chunk's arrival flag, after its data in the same stream
+        if (err == cudaSuccess && streaming)
+            err = cudaMemcpyAsync(h->d_flags + k, h->h_gen, sizeof(uint32_t), cudaMemcpyHostToDevice, h->copy);
         return err;
     };
-    CKH(cudaMemsetAsync(h->d_res + n_residues, 0, res_bytes - (size_t)n_residues, h->copy), "memset(pad)");
+    // chunk tables: first offsets (n + 1), device bases (n), then first subjects (n + 1)
+    const size_t tab_bytes = (size_t)(n_chunks + 1) * 8 + (size_t)n_chunks * 8 + (size_t)(n_chunks + 1) * 4;
+    if (streaming) {
+        // chunk tables and flags; the tables go up first on the upload stream
+        // (a copy queued on another stream could wait behind the chunks)
+        if (!h->h_gen) CKH(cudaMallocHost((void**)&h->h_gen, sizeof(uint32_t)), "cudaMallocHost");
+        if (!h->tabs_ready) CKH(cudaEventCreateWithFlags(&h->tabs_ready, cudaEventDisableTiming), "cudaEventCreate");
+        if (h->flags_cap < (size_t)n_chunks) {
+            CKH(grow_buf(&h->d_flags, &h->flags_cap, (size_t)n_chunks), "cudaMalloc(flags)");
+            CKH(cudaMemsetAsync(h->d_flags, 0, h->flags_cap * sizeof(uint32_t), e->stream), "memset(flags)");
+            CKH(cudaStreamSynchronize(e->stream), "memset(flags)");
+        }
+        CKH(grow_buf(&h->d_tab, &h->tab_cap, tab_bytes), "cudaMalloc(chunk tables)");
+        if (h->h_tab_cap < tab_bytes) {
+            if (h->h_tab) cudaFreeHost(h->h_tab);
+            h->h_tab = nullptr;
+            h->h_tab_cap = 0;
+            CKH(cudaMallocHost((void**)&h->h_tab, tab_bytes * 2), "cudaMallocHost");
+            h->h_tab_cap = tab_bytes * 2;
+        }
+        int64_t* tlo = (int64_t*)h->h_tab;
+        int64_t* tb = tlo + n_chunks + 1;
+        int32_t* tf = (int32_t*)(tb + n_chunks);
+        for (int k = 0; k <= n_chunks; ++k) {
+            tf[k] = cf[k];
+            tlo[k] = offsets[cf[k]];
+            if (k < n_chunks) tb[k] = base[k];
+        }
+        *h->h_gen = ++h->gen;
+        CKH(cudaMemcpyAsync(h->d_tab, h->h_tab, tab_bytes, cudaMemcpyHostToDevice, h->copy), "upload chunk tables");
+    } else {
+        CKH(cudaMemsetAsync(h->d_res + n_residues, 0, res_bytes - (size_t)n_residues, h->copy), "memset(pad)");
+    }
     CKH(cudaMemcpyAsync(h->d_off, offsets, ((size_t)n_subjects + 1) * 8, cudaMemcpyHostToDevice, h->copy),
         "upload offsets");
+    if (streaming) CKH(cudaEventRecord(h->tabs_ready, h->copy), "cudaEventRecord");
     if (pinned)
         for (int k = 0; k < n_chunks; ++k) CKH(upload(k), "upload residues");
     const int32_t long_min = bp_long_threshold(n_residues, n_subjects);
@@ -220,12 +305,49 @@ extern "C" bp_status bp_blastp_host(bp_engine* e, const uint8_t* query, int32_t 
     size_t bc = (size_t)e->blocksum_cap;
     CKH(grow_buf(&e->d_blocksums, &bc, (size_t)bp_order_blocksums_needed(n_subjects)), "cudaMalloc(sums)");
     e->blocksum_cap = (int32_t)bc;
-    // chunk k's checks and scan run on the engine stream behind its event
     uint32_t* bad_res = h->d_words + 1;
     uint32_t* bad_off = h->d_words + 2;
     uint32_t* cursors = h->d_words + 4;
     int32_t* long_counts = (int32_t*)(h->d_words + 4 + n_chunks);
     CKH(cudaMemsetAsync(h->d_words, 0, (4 + 2 * (size_t)n_chunks) * sizeof(uint32_t), e->stream), "memset");
+    if (streaming) {
+        // one launch; it starts once the tables and offsets are up
+        CKH(cudaStreamWaitEvent(e->stream, h->tabs_ready, 0), "cudaStreamWaitEvent");
+        CKH(cudaEventRecord(e->ev_scan0, e->stream), "cudaEventRecord");
+        ScanArgs a{};
+        a.db = h->d_res;
+        a.db_off = h->d_off;
+        a.first = 0;
+        a.n = n_subjects;
+        a.query = q->d_q;
+        a.qlen = q->qlen;
+        a.cells = q->d_cells;
+        a.entries = q->d_entries;
+        a.n_entries = (int32_t)q->n_entries;
+        a.ctx = q->d_ctx;
+        a.n_ctx = q->n_ctx;
+        a.matrix = e->d_matrix;
+        a.window = q->p.window;
+        a.diag_len = q->diag_len;
+        a.counters = h->d_counters;
+        a.recs = e->d_recs;
+        a.rec_cap = e->rec_cap;
+        a.rec_count = h->d_words;
+        a.cursor = cursors;
+        a.error = bad_res;
+        a.bad_off = bad_off;
+        a.stalled = h->d_words + 3;
+        a.n_chunks = n_chunks;
+        a.chunk_lo = (const int64_t*)h->d_tab;
+        a.chunk_base = a.chunk_lo + n_chunks + 1;
+        a.chunk_first = (const int32_t*)(a.chunk_base + n_chunks);
+        a.chunk_flag = h->d_flags;
+        a.gen = h->gen;
+        a.wait_ns = 20ull * 1000 * 1000 * 1000;   // a chunk more than 20 s late: the scan gives up
+        CKH(bp_launch_scan_stream(e, e->stream, a), "streaming scan launch");
+        CKH(cudaEventRecord(e->ev_scan1, e->stream), "cudaEventRecord");
+    } else {
+    // chunk k's checks and scan run on the engine stream behind its event
     CKH(cudaEventRecord(e->ev_scan0, e->stream), "cudaEventRecord");
     CKH(cudaEventRecord(h->fork, e->stream), "cudaEventRecord");
     CKH(cudaStreamWaitEvent(h->checks, h->fork, 0), "cudaStreamWaitEvent");
@@ -280,14 +402,23 @@ extern "C" bp_status bp_blastp_host(bp_engine* e, const uint8_t* query, int32_t 
     CKH(cudaEventRecord(h->join, h->scan2), "cudaEventRecord");
     CKH(cudaStreamWaitEvent(e->stream, h->join, 0), "cudaStreamWaitEvent");
     CKH(cudaEventRecord(e->ev_scan1, e->stream), "cudaEventRecord");
+    }
     // records written and the residue check, then outputs sized by the records
-    CKH(cudaMemcpyAsync(h->h_words, h->d_words, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, e->stream),
+    CKH(cudaMemcpyAsync(h->h_words, h->d_words, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, e->stream),
         "read counts");
     CKH(cudaStreamSynchronize(e->stream), "pipelined search");
+    // every copy is done too (a scan that skipped a bad subject may not have
+    // waited for its chunk): the caller may reuse its buffers on return
+    CKH(cudaStreamSynchronize(h->copy), "pipelined search");
     float ms = 0.f;
     if (cudaEventElapsedTime(&ms, e->ev_scan0, e->ev_scan1) == cudaSuccess) e->last_scan_ms = ms;
     cudaGetLastError();
     const uint32_t recs = h->h_words[0];
+    if (h->h_words[3]) {
+        cudaStreamSynchronize(h->copy);
+        bp_query_destroy(q);
+        return bp_set_error(e, BP_ERR_TIMEOUT, "bp_blastp_host: a chunk of the upload did not arrive in time");
+    }
     if (h->h_words[2]) {
         cudaStreamSynchronize(h->back);
         bp_query_destroy(q);

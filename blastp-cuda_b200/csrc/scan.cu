@@ -88,6 +88,7 @@ struct ScanLayout {
     int entries_smem;
     int L;                 // diagonal entries per warp (the longest query's)
     int off_cells, off_entries, off_query, off_members, off_mof, off_warps, off_ctl;
+    int off_stream;        // streaming launches: per-warp pipeline state
     int warp_bytes;        // diagonal array + per-lane position table + task queue + blocked list
                            // (+ per-member counters when packed)
     int total;
@@ -276,10 +277,17 @@ __device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
 
-// Residues r..r+kP+1 of the window starting at `sl` (code-1, or -1 past the end).
-__device__ __forceinline__ void load_window(const uint8_t* __restrict__ sub, int slen, int sl, int (&r)[kP + 2]) {
+// Residues r..r+kP+1 of the window starting at `sl` (code-1, or -1 past the
+// end).  kCheck: codes of 28 and more (r > 26) are noted in `bad`; every
+// residue of a subject passes through some lane's window.
+template <bool kCheck = false>
+__device__ __forceinline__ void load_window(const uint8_t* __restrict__ sub, int slen, int sl, int (&r)[kP + 2],
+                                            uint32_t& bad) {
 #pragma unroll
-    for (int i = 0; i < kP + 2; ++i) r[i] = (sl + i < slen) ? (int)__ldg(sub + sl + i) - 1 : -1;
+    for (int i = 0; i < kP + 2; ++i) {
+        r[i] = (sl + i < slen) ? (int)__ldg(sub + sl + i) - 1 : -1;
+        if (kCheck) bad |= r[i] > BP_ALPHABET - 2 ? 1u : 0u;
+    }
 }
 
 // One warp's view of the subject it is scanning.
@@ -526,7 +534,7 @@ __device__ __forceinline__ void rebase_diag(DiagT* diag, int n, int delta, int l
 // base + s0 + 128 + qlen (a hit lies before s0 + 128 and a right walk ends
 // within qlen letters of it), so the offset is reset when that bound could
 // reach DiagBits::kMax.  clear_len: entries of the warp's whole array.
-template <typename CellT, bool kDefer, bool kPacked, typename DiagT>
+template <typename CellT, bool kDefer, bool kPacked, typename DiagT, bool kCheck = false>
 __device__ void scan_subject(const ScanArgs& a, const int8_t* m, const uint8_t* qs, const CellT* cells,
                              const uint16_t* entries, DiagT* diag, int clear_len, uint32_t* lane_pos, Task* tasks,
                              Task* blocked, int* wcnt, int oid, const uint8_t* __restrict__ sub, int slen, int& base,
@@ -564,7 +572,8 @@ __device__ void scan_subject(const ScanArgs& a, const int8_t* m, const uint8_t* 
     const int last_pos = slen - BP_WORD;
     const uint32_t* my_row = lane_pos - lane * kRow;
     int r[kP + 2];
-    load_window(sub, slen, lane * kP, r);
+    uint32_t bad = 0;
+    load_window<kCheck>(sub, slen, lane * kP, r, bad);
     for (int s0 = 0; s0 <= last_pos; s0 += 32 * kP) {
         if (base + s0 + 129 + a.qlen >= B::kMax) {
             // long subject: settle every queued extension, then move the offset
@@ -575,7 +584,7 @@ __device__ void scan_subject(const ScanArgs& a, const int8_t* m, const uint8_t* 
             w.base = base;
         }
         int rn[kP + 2];
-        load_window(sub, slen, s0 + 32 * kP + lane * kP, rn);    // next window, in flight meanwhile
+        load_window<kCheck>(sub, slen, s0 + 32 * kP + lane * kP, rn, bad);   // next window, in flight meanwhile
         const int sl = s0 + lane * kP;
         uint32_t lane_cnt = 0;
 #pragma unroll
@@ -648,6 +657,7 @@ __device__ void scan_subject(const ScanArgs& a, const int8_t* m, const uint8_t* 
         base += slen + a.window;
         return;
     }
+    if (kCheck && __any_sync(kFull, bad != 0) && lane == 0) atomicOr(a.error, 1u);
     int ext = w.ext, succ = w.succ;
 #pragma unroll
     for (int o = 16; o >= 1; o >>= 1) {
@@ -706,20 +716,15 @@ __device__ __forceinline__ WarpRegions<DiagT> warp_regions(const ScanLayout& lay
     return r;
 }
 
-template <typename CellT, bool kCellsSmem, bool kDefer, typename DiagT>
-__global__ void __launch_bounds__(kMaxWarps * 32, 1)
-scan_kernel(ScanArgs a, ScanLayout lay) {
-    // an earlier check on the device refused the inputs: nothing to scan
-    if (a.abort_if && *a.abort_if) return;
-    const int n_long = a.n_long_at ? *a.n_long_at : a.n_long;
+// The scoring matrix, the query and (when they fit) the compact table, into
+// shared memory for every warp of the CTA (callers synchronise after).
+template <typename CellT, bool kCellsSmem>
+__device__ __forceinline__ void load_tables(const ScanArgs& a, const ScanLayout& lay, const int8_t*& m,
+                                            const uint8_t*& qs, const CellT*& cells, const uint16_t*& entries) {
     uint8_t* sm = bp_smem;
-    int8_t* m = reinterpret_cast<int8_t*>(sm);
-    uint8_t* qs = sm + lay.off_query;
-    const CellT* cells = kCellsSmem ? reinterpret_cast<const CellT*>(sm + lay.off_cells)
-                                    : reinterpret_cast<const CellT*>(a.cells);
-    const uint16_t* entries = lay.entries_smem ? reinterpret_cast<const uint16_t*>(sm + lay.off_entries) : a.entries;
-
-    for (int i = threadIdx.x; i < 28 * BP_MROW; i += blockDim.x) m[i] = a.matrix[i];
+    int8_t* mm = reinterpret_cast<int8_t*>(sm);
+    uint8_t* q = sm + lay.off_query;
+    for (int i = threadIdx.x; i < 28 * BP_MROW; i += blockDim.x) mm[i] = a.matrix[i];
     if (kCellsSmem) {
         CellT* c = reinterpret_cast<CellT*>(sm + lay.off_cells);
         for (int i = threadIdx.x; i <= BP_NC; i += blockDim.x) c[i] = (CellT)a.cells[i];
@@ -728,7 +733,24 @@ scan_kernel(ScanArgs a, ScanLayout lay) {
         uint16_t* e = reinterpret_cast<uint16_t*>(sm + lay.off_entries);
         for (int i = threadIdx.x; i < a.n_entries; i += blockDim.x) e[i] = a.entries[i];
     }
-    for (int i = threadIdx.x; i < a.qlen; i += blockDim.x) qs[i] = a.query[i];
+    for (int i = threadIdx.x; i < a.qlen; i += blockDim.x) q[i] = a.query[i];
+    m = mm;
+    qs = q;
+    cells = kCellsSmem ? reinterpret_cast<const CellT*>(sm + lay.off_cells) : reinterpret_cast<const CellT*>(a.cells);
+    entries = lay.entries_smem ? reinterpret_cast<const uint16_t*>(sm + lay.off_entries) : a.entries;
+}
+
+template <typename CellT, bool kCellsSmem, bool kDefer, typename DiagT>
+__global__ void __launch_bounds__(kMaxWarps * 32, 1)
+scan_kernel(ScanArgs a, ScanLayout lay) {
+    // an earlier check on the device refused the inputs: nothing to scan
+    if (a.abort_if && *a.abort_if) return;
+    const int n_long = a.n_long_at ? *a.n_long_at : a.n_long;
+    const int8_t* m;
+    const uint8_t* qs;
+    const CellT* cells;
+    const uint16_t* entries;
+    load_tables<CellT, kCellsSmem>(a, lay, m, qs, cells, entries);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const WarpRegions<DiagT> wr = warp_regions<DiagT>(lay, warp, lane);
     for (int i = lane; i < lay.L; i += 32) wr.diag[i] = 0;
@@ -790,6 +812,141 @@ scan_kernel(ScanArgs a, ScanLayout lay) {
         cur = __shfl_sync(kFull, nxt, 0);
         cs = __shfl_sync(kFull, ns, 0);
         ce = __shfl_sync(kFull, ne, 0);
+    }
+}
+
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Lane 0 of a streaming launch: whether chunk c's residues are there.  The
+// wait is bounded by a.wait_ns and by a poll count; when either runs out, or
+// another warp has given up already, *stalled is set and the warp stops.
+__device__ bool wait_chunk(const ScanArgs& a, int c) {
+    const volatile uint32_t* f = a.chunk_flag + c;
+    if (*f != a.gen) {
+        const volatile uint32_t* st = a.stalled;
+        const uint64_t t0 = global_ns();
+        uint32_t polls = 0;
+        while (*f != a.gen) {
+            if (*st || ++polls >= (1u << 26) || global_ns() - t0 > a.wait_ns) {
+                atomicOr(a.stalled, 1u);
+                return false;
+            }
+            __nanosleep(256);
+        }
+    }
+    __threadfence();
+    return true;
+}
+
+// Lane 0 of a streaming launch: the device span [s, e) of subject id of the
+// range and its chunk c; false when its offsets leave the chunk (out of
+// order).  A warp's subjects come in increasing order, so the chunk hint
+// only moves forward.
+__device__ __forceinline__ bool locate(const ScanArgs& a, uint32_t id, int& hint, long long& s, long long& e,
+                                       int& c) {
+    while (hint + 1 < a.n_chunks && (int)id >= a.chunk_first[hint + 1]) ++hint;
+    c = hint;
+    const long long lo = a.db_off[a.first + id], hi = a.db_off[a.first + id + 1];
+    const long long clo = a.chunk_lo[c], chi = a.chunk_lo[c + 1];
+    if (lo < clo || hi < lo || hi > chi || hi - lo > (1LL << 29)) return false;
+    s = a.chunk_base[c] + (lo - clo);
+    e = s + (hi - lo);
+    return true;
+}
+
+// Streaming form of scan_kernel for the host-to-host search: one launch over
+// all subjects while their residues are still being uploaded in chunks.  The
+// subjects go in index order through the same three-stage pipeline; before
+// a subject is scanned, lane 0 waits (bounded) for its chunk's flag, which
+// the upload stream writes with a 4-byte copy after the chunk's data.  Each
+// chunk starts on a 128-byte boundary of the device buffer, so no cache
+// line read after a flag can hold bytes loaded before it.  Residue codes are
+// checked as they are read; offsets are checked against their chunk before
+// any residue of the subject is touched.
+// Lane 0's pipeline state of a streaming launch (shared memory, one per
+// warp): a ring of three subjects -- the one being scanned, the next (span
+// known, residues prefetched), the one after (id known) -- so that little
+// lives in registers across the scan of a subject.
+struct StreamSubj {
+    long long s, e;        // device span of the residues
+    uint32_t id;           // subject of the range (>= n: none)
+    int c;                 // chunk
+    int ok;                // offsets inside the chunk
+    int pad;
+};
+struct StreamCtl {
+    StreamSubj q[3];
+    int hint, ready;       // chunk hint of locate(); highest chunk known to be there
+};
+
+template <typename CellT, bool kCellsSmem, bool kDefer>
+__global__ void __launch_bounds__(kMaxWarps * 32, 1)
+scan_stream_kernel(ScanArgs a, ScanLayout lay) {
+    const int8_t* m;
+    const uint8_t* qs;
+    const CellT* cells;
+    const uint16_t* entries;
+    load_tables<CellT, kCellsSmem>(a, lay, m, qs, cells, entries);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const WarpRegions<uint16_t> wr = warp_regions<uint16_t>(lay, warp, lane);
+    for (int i = lane; i < lay.L; i += 32) wr.diag[i] = 0;
+    StreamCtl* sc = reinterpret_cast<StreamCtl*>(bp_smem + lay.off_stream) + warp;
+    const uint32_t n = (uint32_t)a.n;
+    if (lane == 0) {
+        sc->hint = 0;
+        sc->ready = -1;
+        for (int k = 0; k < 3; ++k) {
+            StreamSubj& q = sc->q[k];
+            q.id = atomicAdd(a.cursor, 1u);
+            q.ok = 0;
+            if (k < 2 && q.id < n) q.ok = locate(a, q.id, sc->hint, q.s, q.e, q.c);
+        }
+    }
+    __syncthreads();
+    int base = a.window;
+    for (int i = 0;; i = i == 2 ? 0 : i + 1) {
+        const int i1 = i == 2 ? 0 : i + 1, i2 = i1 == 2 ? 0 : i1 + 1;
+        int go = 0;
+        if (lane == 0) {
+            StreamSubj& cur = sc->q[i];
+            StreamSubj& nx = sc->q[i1];
+            StreamSubj& nx2 = sc->q[i2];
+            if (cur.id >= n) {
+                go = -2;                                     // nothing left
+            } else {
+                if (nx.id < n && nx.ok && nx.c <= sc->ready && nx.e > nx.s)
+                    prefetch_l2(a.db + (nx.s & ~15LL), (uint32_t)(((nx.e + 15) & ~15LL) - (nx.s & ~15LL)));
+                if (nx2.id < n) nx2.ok = locate(a, nx2.id, sc->hint, nx2.s, nx2.e, nx2.c);
+                if (!cur.ok) {
+                    atomicOr(a.bad_off, 1u);
+                } else if (cur.c <= sc->ready) {
+                    go = 1;
+                } else if (wait_chunk(a, cur.c)) {
+                    sc->ready = cur.c;
+                    go = 1;
+                } else {
+                    go = -1;                                 // the upload stalled: the host reports it
+                }
+            }
+        }
+        go = __shfl_sync(kFull, go, 0);
+        if (go < 0) break;
+        __syncwarp();
+        const StreamSubj& cur = sc->q[i];
+        if (go) {
+            const long long s0 = cur.s, e0 = cur.e;
+            scan_subject<CellT, kDefer, false, uint16_t, true>(a, m, qs, cells, entries, wr.diag, lay.L, wr.lane_pos,
+                                                              wr.tasks, wr.blocked, wr.wcnt,
+                                                              a.oid_base + (int)cur.id, a.db + s0, (int)(e0 - s0),
+                                                              base, lane);
+        }
+        __syncwarp();
+        if (lane == 0) sc->q[i].id = atomicAdd(a.cursor, 1u);   // becomes the one after next
+        __syncwarp();
     }
 }
 
@@ -921,7 +1078,7 @@ scan_batch_kernel(BatchArgs b, ScanLayout lay) {
 }
 
 ScanLayout make_layout(int qlen, int L, int64_t n_entries, int warps, int cells_mode, int entries_smem,
-                       bool packed) {
+                       bool packed, bool stream = false) {
     ScanLayout l{};
     l.warps = warps;
     l.cells_mode = cells_mode;
@@ -955,20 +1112,23 @@ ScanLayout make_layout(int qlen, int L, int64_t n_entries, int warps, int cells_
     off = al(off, 16);
     l.off_ctl = (int)(off > big ? big : off);
     off += 512;                                       // batched kernel's control block
+    l.off_stream = (int)(off > big ? big : off);
+    if (stream) off += kMaxWarps * (long long)sizeof(StreamCtl);
     l.total = (int)(off > big ? big : off);
     return l;
 }
 
 // Picks the layout with the most warps, preferring the whole table in shared
 // memory as long as that still leaves at least 16 warps.
-bool choose_layout(int qlen, int L, int64_t n_entries, int smem_optin, ScanLayout* out, bool packed = false) {
+bool choose_layout(int qlen, int L, int64_t n_entries, int smem_optin, ScanLayout* out, bool packed = false,
+                   bool stream = false) {
     const int cell_modes[2] = {n_entries < 65536 ? 0 : 1, 2};
     for (int min_w : {16, 8, 1})
         for (int cm : cell_modes)
             for (int es = 1; es >= 0; --es) {
                 if (es && cm == 2) continue;
                 for (int w = kMaxWarps; w >= min_w; --w) {
-                    const ScanLayout l = make_layout(qlen, L, n_entries, w, cm, es, packed);
+                    const ScanLayout l = make_layout(qlen, L, n_entries, w, cm, es, packed, stream);
                     if (l.total <= smem_optin) {
                         *out = l;
                         return true;
@@ -994,6 +1154,19 @@ cudaError_t launch(bp_engine* e, cudaStream_t stream, const ScanArgs& a, const S
     return cudaGetLastError();
 }
 
+template <typename CellT, bool kCellsSmem, bool kDefer>
+cudaError_t launch_stream(bp_engine* e, cudaStream_t stream, const ScanArgs& a, const ScanLayout& lay) {
+    auto kern = scan_stream_kernel<CellT, kCellsSmem, kDefer>;
+    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, e->smem_optin);
+    if (err != cudaSuccess) return err;
+    int grid = e->sm_count;
+    const int need = (a.n + lay.warps - 1) / lay.warps;
+    if (grid > need) grid = need > 0 ? need : 1;
+    kern<<<grid, lay.warps * 32, lay.total, stream>>>(a, lay);
+    e->launches += 1;
+    return cudaGetLastError();
+}
+
 template <typename CellT, bool kCellsSmem, bool kDefer, bool kPacked, typename DiagT>
 cudaError_t launch_batch(bp_engine* e, cudaStream_t stream, const BatchArgs& b, const ScanLayout& lay, int grid) {
     auto kern = scan_batch_kernel<CellT, kCellsSmem, kDefer, kPacked, DiagT>;
@@ -1011,6 +1184,7 @@ cudaError_t launch_batch(bp_engine* e, cudaStream_t stream, const BatchArgs& b, 
 
 static_assert(sizeof(BatchCtl) <= 512, "batched control block must fit its shared-memory slot");
 static_assert(sizeof(Task) == 16, "task layout");
+static_assert(sizeof(BatchCtl) % 8 == 0 && 512 % 8 == 0, "stream control blocks stay 8-byte aligned");
 static_assert((32 * kRow * 4) % 16 == 0, "the task queue after the position table stays 16-byte aligned");
 static_assert(kRow % 2 == 1, "odd row stride: one bank per lane");
 static_assert(kMaxMembers == BP_MAX_PACK_MEMBERS, "pack size limit");
@@ -1068,6 +1242,23 @@ bool bp_scan_fits(int32_t qlen, int32_t diag_len, int64_t n_entries, int smem_op
 }
 
 cudaError_t bp_launch_scan(bp_engine* e, const ScanArgs& a) { return bp_launch_scan_on(e, e->stream, a); }
+
+bool bp_scan_streams(int32_t diag_len) { return diag_len <= kNarrowMaxL; }
+
+cudaError_t bp_launch_scan_stream(bp_engine* e, cudaStream_t st, const ScanArgs& a) {
+    ScanLayout lay;
+    if (!choose_layout(a.qlen, a.diag_len, a.n_entries, e->smem_optin, &lay, false, true))
+        return cudaErrorInvalidValue;
+    if (lay.L > kNarrowMaxL || a.n_chunks < 1) return cudaErrorNotSupported;
+    if (a.qlen >= kDeferMinQlen) {
+        if (lay.cells_mode == 0) return launch_stream<uint16_t, true, true>(e, st, a, lay);
+        if (lay.cells_mode == 1) return launch_stream<uint32_t, true, true>(e, st, a, lay);
+        return launch_stream<uint32_t, false, true>(e, st, a, lay);
+    }
+    if (lay.cells_mode == 0) return launch_stream<uint16_t, true, false>(e, st, a, lay);
+    if (lay.cells_mode == 1) return launch_stream<uint32_t, true, false>(e, st, a, lay);
+    return launch_stream<uint32_t, false, false>(e, st, a, lay);
+}
 
 cudaError_t bp_launch_scan_on(bp_engine* e, cudaStream_t st, const ScanArgs& a) {
     ScanLayout lay;

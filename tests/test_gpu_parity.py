@@ -209,10 +209,29 @@ def test_host_path_rejects_bad_offsets(engine):
     got = engine.blastp_host(q, default_params(), res, off)
     ref = gpu_search(engine, q, res, off)
     assert_same(got, (ref.counters, ref.hsp_off, ref.hsps_as_array()), "after a refused call")
+    # from pinned memory (the single streaming launch checks the offsets itself)
+    import torch
+    pin = torch.empty(len(res), dtype=torch.uint8, pin_memory=True)
+    pin.numpy()[:] = res
+    with pytest.raises(BpError):
+        engine.blastp_host(q, default_params(), pin.numpy(), bad)
+    got = engine.blastp_host(q, default_params(), pin.numpy(), off)
+    assert_same(got, (ref.counters, ref.hsp_off, ref.hsps_as_array()), "pinned, after a refused call")
 
 
 def test_host_path_rejects_bad_residues(engine):
+    import torch
     res = np.ones(1000, dtype=np.uint8)
     res[777] = 50
     with pytest.raises(BpError):
         engine.blastp_host(enc("WCWHEAL"), default_params(), res, np.array([0, 500, 1000], np.int64))
+    # pinned: the streaming launch checks residue codes as it reads them
+    pin = torch.empty(len(res), dtype=torch.uint8, pin_memory=True)
+    pin.numpy()[:] = res
+    with pytest.raises(BpError):
+        engine.blastp_host(enc("WCWHEAL"), default_params(), pin.numpy(), np.array([0, 500, 1000], np.int64))
+    pin.numpy()[777] = 28
+    with pytest.raises(BpError):
+        engine.blastp_host(enc("WCWHEAL"), default_params(), pin.numpy(), np.array([0, 500, 1000], np.int64))
+    pin.numpy()[777] = 27
+    engine.blastp_host(enc("WCWHEAL"), default_params(), pin.numpy(), np.array([0, 500, 1000], np.int64))
