@@ -88,7 +88,7 @@ struct ScanLayout {
     int entries_smem;
     int L;                 // diagonal entries per warp (the longest query's)
     int off_cells, off_entries, off_query, off_members, off_mof, off_warps, off_ctl;
-    int off_stream;        // streaming launches: per-warp pipeline state
+    int off_stream;        // plain and streaming launches: per-warp subject pipeline
     int warp_bytes;        // diagonal array + per-lane position table + task queue + blocked list
                            // (+ per-member counters when packed)
     int total;
@@ -740,6 +740,23 @@ __device__ __forceinline__ void load_tables(const ScanArgs& a, const ScanLayout&
     entries = lay.entries_smem ? reinterpret_cast<const uint16_t*>(sm + lay.off_entries) : a.entries;
 }
 
+// Lane 0's subject pipeline (shared memory, one per warp, plain and
+// streaming launches): a ring of three subjects -- the one being scanned,
+// the next (span known, residues prefetched), the one after (id known) -- so
+// that little lives in registers across the scan of a subject (in registers
+// this state made the scan spill).
+struct StreamSubj {
+    long long s, e;        // device span of the residues
+    uint32_t id;           // subject of the range (>= n: none)
+    int c;                 // chunk
+    int ok;                // offsets inside the chunk
+    int pad;
+};
+struct StreamCtl {
+    StreamSubj q[3];
+    int hint, ready;       // chunk hint of locate(); highest chunk known to be there
+};
+
 template <typename CellT, bool kCellsSmem, bool kDefer, typename DiagT>
 __global__ void __launch_bounds__(kMaxWarps * 32, 1)
 scan_kernel(ScanArgs a, ScanLayout lay) {
@@ -756,62 +773,57 @@ scan_kernel(ScanArgs a, ScanLayout lay) {
     for (int i = lane; i < lay.L; i += 32) wr.diag[i] = 0;
     __syncthreads();
 
-    // Subject pipeline, kept by lane 0.  At the top of iteration i:
-    //   cur (+ cs, ce)   subject i, offsets known: scan it now
-    //   oid1 (+ s1, e1)  subject i+1, offsets known: prefetch its residues now
-    //   oid2             subject i+2, id known: load its offsets now
-    // and the id of subject i+3 is taken from the cursor (slot_subject:
-    // subject index in the range, kSecond on second-pass slots, kNone past
-    // the end).
-    uint32_t cur = 0, oid1 = 0, oid2 = 0;
-    long long cs = 0, ce = 0, s1 = 0, e1 = 0;
+    // Subject pipeline, kept by lane 0 in a per-warp ring in shared memory:
+    // the subject being scanned, the next (offsets known, residues
+    // prefetched into L2), the one after (id known, offsets loaded this
+    // round); a new id is taken from the cursor after each scan.
+    // slot_subject: subject index in the range, kSecond on second-pass
+    // slots, kNone past the end.
+    StreamCtl* sc = reinterpret_cast<StreamCtl*>(bp_smem + lay.off_stream) + warp;
     if (lane == 0) {
-        cur = slot_subject(a, n_long, atomicAdd(a.cursor, 1u));
-        oid1 = slot_subject(a, n_long, atomicAdd(a.cursor, 1u));
-        oid2 = slot_subject(a, n_long, atomicAdd(a.cursor, 1u));
-        if (in_range(a, cur)) {
-            cs = a.db_off[a.first + (cur & ~kSecond)];
-            ce = a.db_off[a.first + (cur & ~kSecond) + 1];
-        }
-        if (in_range(a, oid1)) {
-            s1 = a.db_off[a.first + (oid1 & ~kSecond)];
-            e1 = a.db_off[a.first + (oid1 & ~kSecond) + 1];
+        for (int k = 0; k < 3; ++k) {
+            StreamSubj& q = sc->q[k];
+            q.id = slot_subject(a, n_long, atomicAdd(a.cursor, 1u));
+            if (k < 2 && in_range(a, q.id)) {
+                q.s = a.db_off[a.first + (q.id & ~kSecond)];
+                q.e = a.db_off[a.first + (q.id & ~kSecond) + 1];
+            }
         }
     }
-    cur = __shfl_sync(kFull, cur, 0);
-    cs = __shfl_sync(kFull, cs, 0);
-    ce = __shfl_sync(kFull, ce, 0);
+    __syncwarp();
     int base = a.window;   // diagonal stamp offset (gpu_blastp_kernel.cu:308)
-    while (in_range(a, cur)) {
-        long long s2 = 0, e2 = 0;
-        uint32_t oid3 = 0;
+    for (int i = 0;; i = i == 2 ? 0 : i + 1) {
+        const int i1 = i == 2 ? 0 : i + 1, i2 = i1 == 2 ? 0 : i1 + 1;
+        int go = 0;
         if (lane == 0) {
-            if (in_range(a, oid1) && e1 > s1 && !done_first(a, n_long, oid1, e1 - s1))
-                prefetch_l2(a.db + (s1 & ~15LL), (uint32_t)(((e1 + 15) & ~15LL) - (s1 & ~15LL)));
-            if (in_range(a, oid2)) {
-                s2 = a.db_off[a.first + (oid2 & ~kSecond)];
-                e2 = a.db_off[a.first + (oid2 & ~kSecond) + 1];
+            const StreamSubj& cur = sc->q[i];
+            const StreamSubj& nx = sc->q[i1];
+            StreamSubj& nx2 = sc->q[i2];
+            if (!in_range(a, cur.id)) {
+                go = -1;
+            } else {
+                if (in_range(a, nx.id) && nx.e > nx.s && !done_first(a, n_long, nx.id, nx.e - nx.s))
+                    prefetch_l2(a.db + (nx.s & ~15LL), (uint32_t)(((nx.e + 15) & ~15LL) - (nx.s & ~15LL)));
+                if (in_range(a, nx2.id)) {
+                    nx2.s = a.db_off[a.first + (nx2.id & ~kSecond)];
+                    nx2.e = a.db_off[a.first + (nx2.id & ~kSecond) + 1];
+                }
+                go = done_first(a, n_long, cur.id, cur.e - cur.s) ? 0 : 1;
             }
-            oid3 = slot_subject(a, n_long, atomicAdd(a.cursor, 1u));
         }
-        if (!done_first(a, n_long, cur, ce - cs))
+        go = __shfl_sync(kFull, go, 0);
+        if (go < 0) break;
+        __syncwarp();
+        if (go) {
+            const StreamSubj& cur = sc->q[i];
+            const long long s0 = cur.s, e0 = cur.e;
             scan_subject<CellT, kDefer, false>(a, m, qs, cells, entries, wr.diag, lay.L, wr.lane_pos, wr.tasks,
-                                               wr.blocked, wr.wcnt, a.oid_base + (int)(cur & ~kSecond), a.db + cs,
-                                               (int)(ce - cs), base, lane);
-        uint32_t nxt = 0;
-        long long ns = 0, ne = 0;
-        if (lane == 0) {
-            nxt = oid1;
-            ns = s1;
-            ne = e1;
-            oid1 = oid2;
-            s1 = s2;
-            e1 = e2;
-            oid2 = oid3;
+                                               wr.blocked, wr.wcnt, a.oid_base + (int)(cur.id & ~kSecond), a.db + s0,
+                                               (int)(e0 - s0), base, lane);
         }
-        cur = __shfl_sync(kFull, nxt, 0);
-        cs = __shfl_sync(kFull, ns, 0);
-        ce = __shfl_sync(kFull, ne, 0);
+        __syncwarp();
+        if (lane == 0) sc->q[i].id = slot_subject(a, n_long, atomicAdd(a.cursor, 1u));
+        __syncwarp();
     }
 }
 
@@ -867,22 +879,6 @@ __device__ __forceinline__ bool locate(const ScanArgs& a, uint32_t id, int& hint
 // line read after a flag can hold bytes loaded before it.  Residue codes are
 // checked as they are read; offsets are checked against their chunk before
 // any residue of the subject is touched.
-// Lane 0's pipeline state of a streaming launch (shared memory, one per
-// warp): a ring of three subjects -- the one being scanned, the next (span
-// known, residues prefetched), the one after (id known) -- so that little
-// lives in registers across the scan of a subject.
-struct StreamSubj {
-    long long s, e;        // device span of the residues
-    uint32_t id;           // subject of the range (>= n: none)
-    int c;                 // chunk
-    int ok;                // offsets inside the chunk
-    int pad;
-};
-struct StreamCtl {
-    StreamSubj q[3];
-    int hint, ready;       // chunk hint of locate(); highest chunk known to be there
-};
-
 template <typename CellT, bool kCellsSmem, bool kDefer>
 __global__ void __launch_bounds__(kMaxWarps * 32, 1)
 scan_stream_kernel(ScanArgs a, ScanLayout lay) {
@@ -1262,7 +1258,8 @@ cudaError_t bp_launch_scan_stream(bp_engine* e, cudaStream_t st, const ScanArgs&
 
 cudaError_t bp_launch_scan_on(bp_engine* e, cudaStream_t st, const ScanArgs& a) {
     ScanLayout lay;
-    if (!choose_layout(a.qlen, a.diag_len, a.n_entries, e->smem_optin, &lay)) return cudaErrorInvalidValue;
+    if (!choose_layout(a.qlen, a.diag_len, a.n_entries, e->smem_optin, &lay, false, true))
+        return cudaErrorInvalidValue;
     using N = uint16_t;
     if (lay.L > kNarrowMaxL) {
         // (32-bit arrays always queue their extensions: a query that is short
