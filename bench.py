@@ -451,54 +451,63 @@ def run_ours(args):
     value = units * args.steps / (total_ms / 1e3)
 
     # end to end through the C ABI: pinned host buffers in and out every step
-    res_pin = torch.empty(len(w.db.residues), dtype=torch.uint8, pin_memory=True)
-    res_pin.numpy()[:] = w.db.residues
-    off_pin = torch.empty(len(w.db.offsets), dtype=torch.int64, pin_memory=True)
-    off_pin.numpy()[:] = w.db.offsets
+    # (--e2e-steps 0 leaves it out, e.g. for profiling runs: the streaming scan
+    # it launches waits on copies from another stream)
     n = w.db.n_subjects
-    cnt_pin = torch.empty((n, 3), dtype=torch.int32, pin_memory=True)
-    hoff_pin = torch.empty(n + 1, dtype=torch.int64, pin_memory=True)
     ref_hsps = eng.search(db, qry).fetch()
-    cap = len(ref_hsps.hsps) + 1024
-    hsp_pin = torch.empty((cap, 6), dtype=torch.int32, pin_memory=True)
-    import ctypes
-    from blastp_b200._lib import lib, check
-    p = bp.default_params()
-    nh = ctypes.c_int64(0)
-    qarr = np.ascontiguousarray(q)
+    e2e = None
+    if args.e2e_steps > 0:
+        res_pin = torch.empty(len(w.db.residues), dtype=torch.uint8, pin_memory=True)
+        res_pin.numpy()[:] = w.db.residues
+        off_pin = torch.empty(len(w.db.offsets), dtype=torch.int64, pin_memory=True)
+        off_pin.numpy()[:] = w.db.offsets
+        cnt_pin = torch.empty((n, 3), dtype=torch.int32, pin_memory=True)
+        hoff_pin = torch.empty(n + 1, dtype=torch.int64, pin_memory=True)
+        cap = len(ref_hsps.hsps) + 1024
+        hsp_pin = torch.empty((cap, 6), dtype=torch.int32, pin_memory=True)
+        import ctypes
+        from blastp_b200._lib import lib, check
+        p = bp.default_params()
+        nh = ctypes.c_int64(0)
+        qarr = np.ascontiguousarray(q)
 
-    def e2e_step():
-        check(lib().bp_blastp_host(eng.h, qarr.ctypes.data, len(q), ctypes.byref(p), res_pin.data_ptr(),
-                                   len(w.db.residues), off_pin.data_ptr(), n, cnt_pin.data_ptr(),
-                                   hoff_pin.data_ptr(), hsp_pin.data_ptr(), cap, ctypes.byref(nh)), eng.h)
+        def e2e_step():
+            check(lib().bp_blastp_host(eng.h, qarr.ctypes.data, len(q), ctypes.byref(p), res_pin.data_ptr(),
+                                       len(w.db.residues), off_pin.data_ptr(), n, cnt_pin.data_ptr(),
+                                       hoff_pin.data_ptr(), hsp_pin.data_ptr(), cap, ctypes.byref(nh)), eng.h)
 
-    e2e_step()
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.e2e_steps):
         e2e_step()
-    barrier()
-    e2e_s = time.perf_counter() - t0
-    t = torch.tensor([e2e_s], device="cuda")
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    e2e_s = float(t.item())
-    h2d = len(w.db.residues) + 8 * len(w.db.offsets) + len(q)
-    # the host link's own rate for the same bytes (pinned, one copy): the floor
-    # of the end-to-end step next to the scan kernel's time
-    dev_buf = torch.empty(len(w.db.residues), dtype=torch.uint8, device="cuda")
-    link = []
-    for _ in range(3):
-        c0 = torch.cuda.Event(enable_timing=True)
-        c1 = torch.cuda.Event(enable_timing=True)
-        c0.record()
-        dev_buf.copy_(res_pin, non_blocking=True)
-        c1.record()
-        torch.cuda.synchronize()
-        link.append(c0.elapsed_time(c1))
-    link_ms = float(min(link))
-    del dev_buf
-    d2h = 12 * n + 8 * (n + 1) + 24 * int(nh.value)
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            e2e_step()
+        barrier()
+        e2e_s = time.perf_counter() - t0
+        t = torch.tensor([e2e_s], device="cuda")
+        if world > 1:
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+        h2d = len(w.db.residues) + 8 * len(w.db.offsets) + len(q)
+        # the host link's own rate for the same bytes (pinned, one copy): the floor
+        # of the end-to-end step next to the scan kernel's time
+        dev_buf = torch.empty(len(w.db.residues), dtype=torch.uint8, device="cuda")
+        link = []
+        for _ in range(3):
+            c0 = torch.cuda.Event(enable_timing=True)
+            c1 = torch.cuda.Event(enable_timing=True)
+            c0.record()
+            dev_buf.copy_(res_pin, non_blocking=True)
+            c1.record()
+            torch.cuda.synchronize()
+            link.append(c0.elapsed_time(c1))
+        link_ms = float(min(link))
+        del dev_buf
+        d2h = 12 * n + 8 * (n + 1) + 24 * int(nh.value)
+        e2e = {"value": w.db.n_residues * world * args.e2e_steps / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "ms_per_step": 1e3 * e2e_s / args.e2e_steps,
+               "upload_overlapped_with_scan": True,
+               "link_ms_per_step": link_ms, "link_gbs": len(w.db.residues) / (link_ms / 1e3) / 1e9}
 
     peak, peak_kind = measured_peak_hbm()
     scan_avg_ms = float(np.mean(scan_ms))
@@ -514,11 +523,7 @@ def run_ours(args):
                    "residues_per_gpu": w.db.n_residues, "word": 3, "threshold": 11, "window": 40,
                    "x_dropoff": 16, "cutoff": 41, "parallelism": "shard%d" % world,
                    "l2": "inputs larger than L2 (%.2f GB database)" % (w.db.n_residues / 1e9)},
-        "e2e": {"value": w.db.n_residues * world * args.e2e_steps / e2e_s, "unit": UNIT,
-                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "ms_per_step": 1e3 * e2e_s / args.e2e_steps,
-                "upload_overlapped_with_scan": True,
-                "link_ms_per_step": link_ms, "link_gbs": len(w.db.residues) / (link_ms / 1e3) / 1e9},
+        "e2e": e2e,
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
