@@ -139,7 +139,13 @@ void bp_result_destroy(bp_result* r);
 
 /* One call from host buffers to host buffers: uploads the database and the
  * query, searches, and copies the results back (the end-to-end form).
- * hsps may be NULL to only size the result (n_hsps out). */
+ * hsps may be NULL to only size the result (n_hsps out).  The upload runs
+ * under the scan: from pinned residues (cudaMallocHost / cudaHostRegister)
+ * one scan launch follows 8 MiB chunks as they arrive; from pageable memory
+ * each chunk gets its own launch, and pinned counters receive each chunk's
+ * counters as soon as its scan ends.  BP_ERR_INVALID for offsets out of order
+ * or residue codes >= 28 (checked on the device); BP_ERR_TIMEOUT if a chunk
+ * did not arrive within 20 s. */
 bp_status bp_blastp_host(bp_engine* e, const uint8_t* query, int32_t qlen, const bp_params* p,
                          const uint8_t* residues, int64_t n_residues, const int64_t* offsets,
                          int32_t n_subjects, int32_t* counters, int64_t* hsp_off,
