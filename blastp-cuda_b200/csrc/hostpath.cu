@@ -59,8 +59,9 @@ struct HostPath {
     int32_t* d_counters = nullptr;
     int64_t* d_hsp_off = nullptr;
     size_t subj_cap = 0;
-    // [0] records, [1] bad residue, [2] bad offsets, [3] unused,
-    // [4 .. 4 + chunks) chunk cursors, then the chunks' long-subject counts
+    // [0] records, [1] bad residue, [2] bad offsets, [3] a streaming chunk
+    // stalled, [4 .. 4 + chunks) chunk cursors (streaming: [4] only), then the
+    // chunks' long-subject counts
     uint32_t* d_words = nullptr;
     size_t words_cap = 0;
     uint32_t* h_words = nullptr;        // pinned read-back

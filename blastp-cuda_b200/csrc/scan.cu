@@ -1233,8 +1233,9 @@ int bp_scan_warps(int32_t qlen, int32_t diag_len, int64_t n_entries, int smem_op
 bool bp_scan_defers(int32_t qlen) { return qlen >= kDeferMinQlen; }
 
 bool bp_scan_fits(int32_t qlen, int32_t diag_len, int64_t n_entries, int smem_optin) {
+    // (with the per-warp subject pipelines the plain and streaming launches reserve)
     ScanLayout l;
-    return choose_layout(qlen, diag_len, n_entries, smem_optin, &l);
+    return choose_layout(qlen, diag_len, n_entries, smem_optin, &l, false, true);
 }
 
 cudaError_t bp_launch_scan(bp_engine* e, const ScanArgs& a) { return bp_launch_scan_on(e, e->stream, a); }
