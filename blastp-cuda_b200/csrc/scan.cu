@@ -166,10 +166,12 @@ __device__ __forceinline__ void warp_xdrop(const int8_t* m, const uint8_t* __res
     }
 }
 
-// The same walk by one lane, letter by letter as in the reference's loops
-// (gpu_blastp_kernel.cu:435-481, :503-549); residues are fetched four
-// letters at a time so the loads overlap the dependent score chain, and only
-// the last, partial group of four checks the walk's end.
+// The same walk by one lane, with the outcome of the reference's
+// letter-by-letter loops (gpu_blastp_kernel.cu:435-481, :503-549): residues
+// are fetched four letters at a time so the loads overlap the dependent score
+// chain, a group of four is tested for a stop once (the running scores and
+// bests of its letters are all known), and only a group that stops, or the
+// last partial one, is resolved letter by letter.
 template <bool kRight>
 __device__ __forceinline__ void lane_xdrop(const int8_t* m, const uint8_t* __restrict__ subj, const uint8_t* qry,
                                            int s0, int q0, int n, int start, int xdrop, int& best, int& best_i,
@@ -186,18 +188,43 @@ __device__ __forceinline__ void lane_xdrop(const int8_t* m, const uint8_t* __res
         int sc[4];
 #pragma unroll
         for (int k = 0; k < 4; ++k) sc[k] = msc(m, qp[D * (i0 + k)], __ldg(sp + D * (i0 + k)));
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            run += sc[k];
-            if (run > best) {
-                best = run;
-                best_i = i0 + k;
-            }
-            if (best - run >= xdrop || (kRight && run <= 0)) {
-                stop_i = i0 + k;
-                return;
-            }
+        // the group's running scores and bests; one test for a stop anywhere in it
+        const int r0 = run + sc[0], r1 = r0 + sc[1], r2 = r1 + sc[2], r3 = r2 + sc[3];
+        const int b0 = max(best, r0), b1 = max(b0, r1), b2 = max(b1, r2), b3 = max(b2, r3);
+        bool t0 = b0 - r0 >= xdrop, t1 = b1 - r1 >= xdrop, t2 = b2 - r2 >= xdrop, t3 = b3 - r3 >= xdrop;
+        if (kRight) {
+            t0 |= r0 <= 0;
+            t1 |= r1 <= 0;
+            t2 |= r2 <= 0;
+            t3 |= r3 <= 0;
         }
+        if (t0 | t1 | t2 | t3) {
+            // the first stopping letter k, with the best (and where it was
+            // first reached) as of that letter
+            const int k = t0 ? 0 : t1 ? 1 : t2 ? 2 : 3;
+            if (r0 > best) {
+                best = r0;
+                best_i = i0;
+            }
+            if (k >= 1 && r1 > best) {
+                best = r1;
+                best_i = i0 + 1;
+            }
+            if (k >= 2 && r2 > best) {
+                best = r2;
+                best_i = i0 + 2;
+            }
+            if (k >= 3 && r3 > best) {
+                best = r3;
+                best_i = i0 + 3;
+            }
+            stop_i = i0 + k;
+            return;
+        }
+        // no stop: the group's best was first reached at the first letter equal to it
+        if (b3 > best) best_i = i0 + (r0 == b3 ? 0 : r1 == b3 ? 1 : r2 == b3 ? 2 : 3);
+        best = b3;
+        run = r3;
     }
     for (; i0 < n; ++i0) {
         run += msc(m, qp[D * i0], __ldg(sp + D * i0));
