@@ -185,6 +185,15 @@ extern "C" bp_status bp_blastp_host(bp_engine* e, const uint8_t* query, int32_t 
     HostPath* h = e->host_path;
     if (!h->copy) CKH(cudaStreamCreateWithFlags(&h->copy, cudaStreamNonBlocking), "cudaStreamCreate");
     if (!h->back) CKH(cudaStreamCreateWithFlags(&h->back, cudaStreamNonBlocking), "cudaStreamCreate");
+    // whichever way this call returns, no copy is still reading or writing
+    // the caller's buffers afterwards
+    struct CopiesDone {
+        HostPath* h;
+        ~CopiesDone() {
+            cudaStreamSynchronize(h->copy);
+            cudaStreamSynchronize(h->back);
+        }
+    } copies_done{h};
     if (!h->checks) CKH(cudaStreamCreateWithFlags(&h->checks, cudaStreamNonBlocking), "cudaStreamCreate");
     if (!h->scan2) CKH(cudaStreamCreateWithFlags(&h->scan2, cudaStreamNonBlocking), "cudaStreamCreate");
     if (!h->fork) CKH(cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming), "cudaEventCreate");

@@ -194,6 +194,26 @@ def test_host_path_overlapped_chunks(engine, matrix):
     assert_same(got, (ref.counters, ref.hsp_off, ref.hsps_as_array()), "pinned in and out")
 
 
+def test_host_path_pinned_edges(engine, matrix):
+    # pinned residues: empty, 1- and 2-letter, identical and very long subjects
+    # through the single streaming launch, then a query of 8,200 letters
+    # (32-bit diagonal entries), which takes one launch per chunk instead
+    import torch
+    rng = np.random.default_rng(29)
+    q = synth.residues(rng, 400)
+    parts = [enc(""), enc("W"), enc("WC"), q.copy(), enc("")]
+    parts.append(synth.residues(rng, 40_000))
+    parts += [synth.residues(rng, int(n)) for n in rng.integers(0, 600, size=3000)]
+    parts.append(np.concatenate([q[50:200], q[50:200]]))
+    res = np.concatenate(parts).astype(np.uint8)
+    off = np.concatenate([[0], np.cumsum([len(x) for x in parts])]).astype(np.int64)
+    pin = torch.empty(len(res), dtype=torch.uint8, pin_memory=True)
+    pin.numpy()[:] = res
+    for query in (q, synth.residues(rng, 8200)):
+        got = engine.blastp_host(query, default_params(), pin.numpy(), off)
+        assert_same(got, oracle_search(query, res, off, matrix), "pinned, qlen %d" % len(query))
+
+
 def test_host_path_rejects_bad_offsets(engine):
     # a decreasing offset inside the first chunk (the chunk boundaries are
     # in order): refused before any scan, the engine stays usable
