@@ -3,7 +3,7 @@
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline and
 reference legs may import this package, and only as the checker or the timed
 CPU baseline; the product path never does.  Parity against the reference's
-own outputs is unpinned (see oracle.h).
+own kernel is pinned by tests/test_ref_pinned.py (see oracle.h).
 """
 import ctypes
 import os

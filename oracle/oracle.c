@@ -1,9 +1,9 @@
 /*
  * oracle.c -- CPU oracle for blastp's two-hit word finder + ungapped X-drop
  * extension.  TEST INFRASTRUCTURE ONLY (see oracle.h): the product path never
- * links, loads or calls this file.  Parity against the reference's own
- * outputs is UNPINNED (nothing in the reference can be built or run here);
- * the scoring table and hand-computed cases pin it instead.
+ * links, loads or calls this file.  Pinned to the reference's own kernel
+ * source, host-compiled into oracle/_ref (ref_driver.cpp), by
+ * tests/test_ref_pinned.py; also by the scoring table and hand-computed cases.
  *
  * Plain C99 + pthreads.  Subjects are independent, so threads take chunks of
  * subjects from an atomic cursor; each thread owns one diagonal array and

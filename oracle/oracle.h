@@ -4,12 +4,16 @@
  * CPU-baseline leg of bench.py use it as the checker; the product path never
  * links, loads or calls it.
  *
- * Parity status: UNPINNED against the reference's own outputs.  The reference
- * (GPU-BLAST 1.1 over NCBI BLAST+ 2.2.28) ships no tests or golden vectors and
- * its hot path cannot be built here (NCBI toolkit headers absent; legacy
- * texture reference rejected by CUDA 12).  What is pinned: the scoring table
- * (against the reference's BLOSUM62 held as a fixture) and hand-computed
- * known-answer cases in tests/.
+ * Parity status: PINNED to the reference's own code.  The reference (GPU-BLAST
+ * 1.1 over NCBI BLAST+ 2.2.28) ships no tests or golden vectors, and its GPU
+ * build needs the absent NCBI toolkit; but its kernel source
+ * (gpu_blastp_kernel.cu) is host-compiled unmodified into oracle/_ref by
+ * ref_driver.cpp, and tests/test_ref_pinned.py requires this oracle's
+ * counters and complete HSP sets to equal that kernel's on config-sized and
+ * edge-case inputs.  Also pinned: the scoring table (the reference's BLOSUM62
+ * held as a fixture) and hand-computed known-answer cases in tests/.  Still
+ * unpinned: NCBI's own neighbour-word rule and cutoff formula, which the
+ * reference calls but does not ship.
  *
  * Semantics restated (file:line into the reference project):
  *   word scan + presence test + cell fetch   gpu_blastp_kernel.cu:151-192

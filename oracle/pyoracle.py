@@ -7,9 +7,10 @@ the masked diagonal with an explicit "no hit yet" value instead of the
 reference's running diagonal offset, so agreement with oracle.c also checks
 that the offset trick is equivalent to a fresh table per subject.
 
-Parity status: unpinned against the reference's own outputs (nothing in the
-reference builds or runs here); pinned by the fixture BLOSUM62 and by the
-hand-computed cases in tests/.
+Parity status: pinned through oracle.c, which tests/test_oracle.py checks
+against this file and tests/test_ref_pinned.py against the reference's own
+kernel source host-compiled into oracle/_ref (ref_driver.cpp); also pinned by
+the fixture BLOSUM62 and the hand-computed cases in tests/.
 """
 
 WORD = 3

@@ -1,10 +1,9 @@
 """Generate the committed golden fixtures under tests/golden/.
 
 The reference (GPU-BLAST over NCBI BLAST+ 2.2.28) ships no tests, fixtures or
-known-answer vectors, and its hot path cannot be compiled here (it needs the
-absent NCBI toolkit headers, and its kernel header declares a legacy texture
-reference that CUDA 12 rejects).  What it does ship as data is its scoring
-table: the int8 28x28 BLOSUM62 in NCBIstdaa order, held in
+known-answer vectors.  (Its kernel source is host-compiled by `make -C oracle
+ref` to pin the oracle's algorithm; see oracle/ref_driver.cpp.)  What it ships
+as data is its scoring table: the int8 28x28 BLOSUM62 in NCBIstdaa order, held in
 ``ReadSubstitutionMatrix`` (gpu_blastp.c:44-86, values at :46-75), of which
 only the first 640 bytes are sent to the GPU (SUBSTITUTION_MATRIX_LENGTH,
 ncbi_blast_files/gpu_cpu_common.h:28).
@@ -14,9 +13,9 @@ to ``blosum62_ncbistdaa.txt`` (28 rows of 28 integers).  The oracle and the
 CUDA path take their matrix from the package's own table; the CPU tests pin
 that table against this fixture, so a transcription error in either shows up.
 
-Run from the repository root:  python tests/golden/make_golden.py [REF_ROOT]
-(REF_ROOT defaults to the read-only reference checkout).  The reference is not
-needed afterwards: only the generated fixture travels with the tests.
+Run from the repository root:  python tests/golden/make_golden.py REF_ROOT
+where REF_ROOT is the reference source tree.  The reference is not needed
+afterwards: only the generated fixture travels with the tests.
 """
 import os
 import re
@@ -43,7 +42,9 @@ def parse_reference_blosum(path):
 
 
 def main():
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <reference source root (the tree holding gpu_blastp.c)>")
+    ref_root = sys.argv[1]
     rows = parse_reference_blosum(os.path.join(ref_root, "gpu_blastp.c"))
     out = os.path.join(HERE, "blosum62_ncbistdaa.txt")
     with open(out, "w") as f:
