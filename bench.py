@@ -15,8 +15,17 @@ no explicit flush is needed between steps.
 With N > 1 (launched by torch.distributed.run) each rank scans its own
 1,000,000-subject shard (weak scaling, no collective on the data path); the
 timed region is bracketed by barriers and the max over ranks is reported.
-`--impl reference` times the reference algorithm's CPU implementation on the
-host cores (the oracle port: the reference itself cannot be built here).
+`--impl reference` times the reference's own kernel code on the host cores:
+gpu_blastp_kernel.cu host-compiled into oracle/_ref (one POSIX thread per
+CUDA thread; its database layout built beforehand, as the reference's
+database writer does), or, where oracle/_ref was not built, the oracle port.
+
+Beside the headline the line carries: the 300-aa query against 10,000
+subjects (the size the plain form's roofline target is quoted on), the scan
+kernel's issue-rate roofline and its word-hit and extension rates, the
+256-query batched workload with every query's result checked against its
+plain search (device digests), and the serving loop with a sample of served
+results checked the same way.
 """
 import argparse
 import json
@@ -45,6 +54,8 @@ def parse():
     ap.add_argument("--subjects", type=int, default=1_000_000)
     ap.add_argument("--qlen", type=int, default=500)
     ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--config1", type=int, default=1, help="also time one 300-aa query vs 10,000 subjects")
+    ap.add_argument("--config1-reps", type=int, default=100)
     ap.add_argument("--cpu-seconds", type=float, default=3.0, help="wall-clock budget of the CPU baseline sample")
     ap.add_argument("--batched", type=int, default=1, help="also measure the batched workload (1 GPU runs only)")
     ap.add_argument("--batch-subjects", type=int, default=2_000_000)
@@ -55,6 +66,7 @@ def parse():
     ap.add_argument("--serve-subjects", type=int, default=5_000_000)
     ap.add_argument("--serve-requests", type=int, default=128)
     ap.add_argument("--serve-rate", type=float, default=1000.0, help="offered load, queries/s (Poisson)")
+    ap.add_argument("--serve-check", type=int, default=32, help="served requests checked against plain searches")
     return ap.parse_args()
 
 
@@ -137,40 +149,149 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-def profiled_traffic_per_residue():
-    """dram bytes per database residue of the scan kernel, from the committed
-    ncu summary (profiles/scan_kernel_q500_vs_1M.md), or None."""
+def profiled_per_residue(key):
+    """A per-residue figure of the scan kernel (dram bytes, warp
+    instructions) from the committed ncu summary
+    (profiles/scan_kernel_q500_vs_1M.md), or None."""
     path = os.path.join(ROOT, "profiles", "scan_kernel_q500_vs_1M.md")
     try:
         for line in open(path):
-            if line.startswith("traffic_bytes_per_residue:"):
+            if line.startswith(key + ":"):
                 return float(line.split(":", 1)[1])
     except OSError:
         pass
     return None
 
 
-def cpu_baseline(matrix, w, budget_s, threads):
-    """Oracle (multithreaded C) on a bounded prefix of the same database:
-    table build + scan, repeated until the budget is used."""
+def reference_threads():
+    """POSIX threads (= CUDA threads of one block) the reference kernel runs
+    with on the host: a few per core, a multiple of 16 as its shared-memory
+    layout requires."""
+    n = 4 * (os.cpu_count() or 1)
+    return max(64, min(1024, 16 * ((n + 15) // 16)))
+
+
+def time_cpu_sample(matrix, q, res, off, prefer_reference=True):
+    """One search of a sample on the host cores: the neighbour-word table
+    build plus the reference's own kernel (oracle/_ref, kind "reference") --
+    its kernel time alone, the interleaved layout being built beforehand as
+    the reference's database writer does -- or else the oracle port (kind
+    "port").  The reference requires length-sorted volumes
+    (functions.cpp:433-438), so the sample is given to it sorted.
+    Returns (seconds, kind, threads)."""
     import oracle
-    q = w.queries[0]
-    n = min(w.db.n_subjects, 200_000)
-    off = w.db.offsets[:n + 1]
-    res = w.db.residues[:off[-1]]
-    done_res, t0, reps = 0, time.perf_counter(), 0
-    while True:
+    from oracle import refkernel
+    if prefer_reference and refkernel.available(2):
+        t0 = time.perf_counter()
         table = oracle.build_table(q, matrix, 11)
-        oracle.scan(res, off, q, table, matrix, [(0, 16, 41)], threads=threads)
-        done_res += int(off[-1])
-        reps += 1
-        if time.perf_counter() - t0 >= budget_s:
-            break
-    dt = time.perf_counter() - t0
-    return {"value": done_res / dt, "unit": UNIT, "cores": threads, "kind": "port",
-            "residue_pairs_per_s": done_res * len(q) / dt,
-            "sample": "first %d subjects (%d residues) x %d reps, query %d aa, all host threads; %.1f s wall"
-                      % (n, int(off[-1]), reps, len(q), dt)}
+        t_table = time.perf_counter() - t0
+        tm = {}
+        refkernel.two_hit(res, off, q, table, matrix, [(0, 16, 41)], slots=2, threads=reference_threads(),
+                          timing=tm)
+        return t_table + tm["kernel_s"], "reference", reference_threads()
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    table = oracle.build_table(q, matrix, 11)
+    oracle.scan(res, off, q, table, matrix, [(0, 16, 41)], threads=threads)
+    return time.perf_counter() - t0, "port", threads
+
+
+def sorted_sample(w, n):
+    """The first n subjects of a workload, sorted by length (ascending)."""
+    off = w.db.offsets[:n + 1]
+    lens = np.diff(off)
+    order = np.argsort(lens, kind="stable")
+    res = np.concatenate([w.db.residues[off[i]:off[i + 1]] for i in order]).astype(np.uint8)
+    soff = np.zeros(n + 1, dtype=np.int64)
+    np.cumsum(lens[order], out=soff[1:])
+    return res, soff
+
+
+def cpu_baseline(matrix, w, budget_s):
+    """The reference's kernel on the host cores (oracle/_ref; the oracle port
+    where it was not built) on a bounded, length-sorted prefix of the same
+    database, repeated until the budget is used; the port's rate on the same
+    sample beside it."""
+    q = w.queries[0]
+    n = min(w.db.n_subjects, 100_000)
+    res, off = sorted_sample(w, n)
+    out = None
+    for prefer in (True, False):
+        done_res, busy, reps, t0 = 0, 0.0, 0, time.perf_counter()
+        while True:
+            dt, kind, threads = time_cpu_sample(matrix, q, res, off, prefer_reference=prefer)
+            busy += dt
+            done_res += int(off[-1])
+            reps += 1
+            if time.perf_counter() - t0 >= budget_s:
+                break
+        r = {"value": done_res / busy, "unit": UNIT, "cores": os.cpu_count() or 1, "threads": threads,
+             "kind": kind, "residue_pairs_per_s": done_res * len(q) / busy,
+             "sample": "first %d subjects (%d residues, sorted by length) x %d reps, query %d aa; "
+                       "table build + %s" % (n, int(off[-1]), reps, len(q),
+                                             "the reference's own kernel (gpu_blastp_kernel.cu host-compiled, "
+                                             "one POSIX thread per CUDA thread)" if kind == "reference"
+                                             else "the oracle port's scan on all host threads")}
+        if out is None:
+            out = r
+            if kind != "reference":
+                break
+        else:
+            out["port"] = {"value": r["value"], "threads": r["threads"],
+                           "note": "the oracle's C restatement, tuned for CPUs, on the same sample"}
+    return out
+
+
+def run_config1(eng, matrix, args, torch, peak):
+    """One 300-aa query against 10,000 subjects (3.6M residues, 3.6 MB): the
+    workload the plain form's roofline target is quoted on.  Each search
+    (scan + ordering pass + count read-back) is timed alone with CUDA events
+    on the engine stream, L2 flushed before it by a 256 MB write; the scan
+    kernel's own time comes from the engine's events around it."""
+    from blastp_b200 import synth
+    w = synth.shape1(matrix)
+    db = eng.database(w.db.residues, w.db.offsets)
+    qry = eng.query(w.queries[0])
+    stream = torch.cuda.ExternalStream(eng.stream)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    search_ms, scan_ms = [], []
+    launches0 = eng.launches
+    for i in range(args.config1_reps + 5):
+        flush.fill_(i & 0xff)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = eng.search(db, qry)
+        e1.record(stream)
+        r.wait()
+        torch.cuda.synchronize()
+        if i >= 5:
+            search_ms.append(e0.elapsed_time(e1))
+            scan_ms.append(eng.last_scan_ms)
+        r.close()
+    launches = (eng.launches - launches0) / (args.config1_reps + 5)
+    res = eng.search(db, qry).fetch()
+    qry.close()
+    db.close()
+    del flush
+    n = w.db.n_subjects
+    s_med = float(np.median(search_ms))
+    k_med = float(np.median(scan_ms))
+    alg = w.db.n_residues + 8 * (n + 1) + 12 * n
+    return {"workload": w.name, "query_len": len(w.queries[0]), "subjects": n, "residues": w.db.n_residues,
+            "reps": len(search_ms), "l2": "flushed before every search (256 MB write)",
+            "search_us_median": 1e3 * s_med, "search_us_min": 1e3 * float(np.min(search_ms)),
+            "scan_kernel_us_median": 1e3 * k_med,
+            "overhead_us_median": 1e3 * (s_med - k_med),
+            "launches_per_search": launches,
+            "value": w.db.n_residues / (s_med / 1e3), "unit": UNIT,
+            "scan_kernel_value": w.db.n_residues / (k_med / 1e3),
+            "roofline": {"bound": "hbm", "algorithmic_bytes": alg, "achieved": alg / (k_med / 1e3) / 1e9,
+                         "peak": peak, "unit": "GB/s", "frac": alg / (k_med / 1e3) / 1e9 / peak,
+                         "hbm_floor_us": alg / (peak * 1e9) * 1e6},
+            "hits": int(res.counters[:, 0].sum()), "extensions": int(res.counters[:, 2].sum()),
+            "hsps": int(len(res.hsps))}
 
 
 def run_batched(eng, matrix, args, torch):
@@ -209,6 +330,8 @@ def run_batched(eng, matrix, args, torch):
     for r in rs:
         r.wait()
         plain_counts.append(int(lib().bp_result_hsps(r.h)))
+    # every query's plain result, as a device digest (counters, offsets, records)
+    plain_digests = [r.digest() for r in rs]
     check_q = [0, len(qs) // 2, len(qs) - 1]
     plain_check = {i: eng.search(db, qs[i]).fetch() for i in check_q}
     for r in rs:
@@ -233,6 +356,7 @@ def run_batched(eng, matrix, args, torch):
                            "trial_fields": ["chunk_residues", "pack_residues", "schedule", "max_warps", "ms"]}
         variants["autotuned"] = dict(best)
     identical = True
+    identical_all = True
     res = {}
     for name, kw in variants.items():
         if kw["schedule"] == SCHED_COSTS:
@@ -255,6 +379,10 @@ def run_batched(eng, matrix, args, torch):
                      "launches_per_run": (eng.launches - launches0) // max(1, args.batch_reps)}
         if b.n_hsps != sum(plain_counts):
             identical = False
+        mismatched = [i for i in range(len(qs)) if b.digest(i) != plain_digests[i]]
+        res[name]["queries_differing_from_plain"] = len(mismatched)
+        if mismatched:
+            identical_all = False
         for i in check_q:
             r = b.fetch(i)
             p = plain_check[i]
@@ -276,6 +404,10 @@ def run_batched(eng, matrix, args, torch):
         b.close()
     out["batched"] = res
     out["identical_to_plain"] = identical
+    out["identical_to_plain_all"] = identical and identical_all
+    out["parity_check"] = ("every variant: each of the %d queries' counters, CSR offsets and HSP records equal its "
+                           "plain search's (128-bit device digests), total HSP count equal, and queries %s "
+                           "compared field by field on the host" % (len(qs), check_q))
     out["hsps"] = int(sum(plain_counts))
     try:
         with open(os.path.join(os.path.dirname(costmodel.MODEL_PATH), "costmodel_b200_report.json")) as f:
@@ -335,11 +467,22 @@ def run_serving(eng, matrix, args):
         srv = Server(eng, db, max_batch_queries=32, lanes=2, schedule=SCHED_COSTS, model=model,
                      chunk_residues=1 << 20)
         arrivals = serving.poisson_arrivals(rng, rate, n)
+        digests = []
+        n_check = min(n, args.serve_check)
         t0 = time.perf_counter()
-        _, lat, late = serving.drive(srv, qs, arrivals, keep_results=False)
+        _, lat, late = serving.drive(srv, qs, arrivals, keep_results=False, digests=digests,
+                                     digest_first=n_check)
         wall = time.perf_counter() - t0
         st = srv.stats()
         srv.close()
+        # the served results against plain searches of the same queries alone
+        same = 0
+        for q, dg in zip(qs[:n_check], digests):
+            h = eng.query(q)
+            r = eng.search(db, h)
+            same += int(r.digest() == dg)
+            r.close()
+            h.close()
         qres = float(sum(len(q) for q in qs))
         runs[label] = {"offered_qps": rate, "requests": n, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
                        "max_ms": st["max_ms"], "throughput_qps": st["queries_per_s"],
@@ -348,10 +491,14 @@ def run_serving(eng, matrix, args):
                        "mean_batch": st["mean_batch"], "max_in_flight": st["max_in_flight"],
                        "mem_peak_gb": st["mem_peak"] / 1e9, "wall_s": wall,
                        "submit_lateness_ms_max": float(late.max()) if len(late) else 0.0,
-                       "query_residues": qres}
+                       "query_residues": qres,
+                       "identical_to_plain": same == n_check, "checked_requests": n_check,
+                       "check": "served result digest (counters, offsets, HSP records) == the query's plain "
+                                "search alone, first %d requests" % n_check}
         if capacity is None:
             capacity = st["queries_per_s"]
     out["runs"] = runs
+    out["identical_to_plain"] = all(r["identical_to_plain"] for r in runs.values())
     db.close()
     return out
 
@@ -362,22 +509,19 @@ def run_reference(args):
         return 0
     sys.path.insert(0, ROOT)
     import oracle
-    from blastp_b200 import synth
     matrix = oracle.load_fixture_matrix()
     w = load_workload(matrix, 0, args.subjects, args.qlen)
     q = w.queries[0]
-    threads = os.cpu_count() or 1
-    # each step: table build + scan of a bounded sample of the workload
-    n = min(w.db.n_subjects, 100_000)
-    off = w.db.offsets[:n + 1]
-    res = w.db.residues[:off[-1]]
+    # each step: table build + the reference kernel over a bounded,
+    # length-sorted sample of the workload
+    n = min(w.db.n_subjects, 50_000)
+    res, off = sorted_sample(w, n)
     times = []
+    kind, threads = "port", os.cpu_count() or 1
     for i in range(args.warmup + args.steps):
-        t0 = time.perf_counter()
-        table = oracle.build_table(q, matrix, 11)
-        oracle.scan(res, off, q, table, matrix, [(0, 16, 41)], threads=threads)
+        dt, kind, threads = time_cpu_sample(matrix, q, res, off)
         if i >= args.warmup:
-            times.append(time.perf_counter() - t0)
+            times.append(dt)
     dt = float(np.sum(times))
     value = int(off[-1]) * len(times) / dt
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
@@ -387,10 +531,14 @@ def run_reference(args):
             "config": {"workload": w.name, "query_len": len(q), "subjects": w.db.n_subjects,
                        "residues": w.db.n_residues, "sample_subjects": n, "word": 3, "threshold": 11,
                        "window": 40, "x_dropoff": 16, "cutoff": 41},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": "first %d subjects (%d residues) per step; the reference's CPU path is "
-                                       "NCBI BLAST 2.2.28, which is not in this image, so the oracle port of "
-                                       "its algorithm is timed" % (n, int(off[-1]))},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count() or 1, "threads": threads,
+                             "kind": kind,
+                             "sample": "first %d subjects (%d residues, sorted by length, as the reference "
+                                       "requires) per step: table build + %s" % (
+                                           n, int(off[-1]),
+                                           "the reference's own kernel (gpu_blastp_kernel.cu host-compiled "
+                                           "into oracle/_ref, one POSIX thread per CUDA thread)"
+                                           if kind == "reference" else "the oracle port's scan")},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "residue_pairs_per_s": value * len(q)}
     print(json.dumps(line), flush=True)
@@ -513,7 +661,25 @@ def run_ours(args):
     scan_avg_ms = float(np.mean(scan_ms))
     alg_bytes = w.db.n_residues + 8 * (n + 1) + 12 * n
     achieved = alg_bytes / (scan_avg_ms / 1e3) / 1e9
-    tpr = profiled_traffic_per_residue()
+    tpr = profiled_per_residue("traffic_bytes_per_residue")
+    # the bound the scan actually meets: instruction issue.  Warp instructions
+    # per residue from the committed ncu capture of the same kernel, against
+    # 4 issue slots per SM per cycle at the SM clock sampled under load.
+    ipr = profiled_per_residue("warp_instructions_per_residue")
+    clocks = clk.summary()
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    issue = None
+    if ipr and clocks:
+        ach = ipr * w.db.n_residues / (scan_avg_ms / 1e3)
+        pk = sms * 4 * clocks["sm_mhz"] * 1e6
+        issue = {"achieved": ach, "peak": pk, "unit": "warp-instructions/s", "frac": ach / pk,
+                 "warp_instructions_per_residue": ipr, "sms": sms, "sm_mhz": clocks["sm_mhz"],
+                 "source": "profiles/scan_kernel_q500_vs_1M.md (ncu smsp__inst_executed)"}
+    cnt = ref_hsps.counters
+    rates = {"word_hits_per_s": float(cnt[:, 0].sum()) / (scan_avg_ms / 1e3),
+             "extensions_per_s": float(cnt[:, 2].sum()) / (scan_avg_ms / 1e3),
+             "word_hits_per_residue": float(cnt[:, 0].sum()) / w.db.n_residues,
+             "extensions_per_residue": float(cnt[:, 2].sum()) / w.db.n_residues}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -529,19 +695,22 @@ def run_ours(args):
                      "frac": achieved / peak, "peak_kind": peak_kind,
                      "traffic": (tpr * w.db.n_residues) if tpr else None,
                      "kernel": "scan_kernel", "kernel_ms": scan_avg_ms,
-                     "algorithmic_bytes": alg_bytes},
+                     "algorithmic_bytes": alg_bytes, "issue": issue},
+        "rates": rates,
         "hsps": int(len(ref_hsps.hsps)),
         # the same rate weighted by query length (DB residues x query residues / s)
         "residue_pairs_per_s": value * len(q),
     }
-    line["clocks"] = clk.summary()
+    line["clocks"] = clocks
+    if world == 1 and args.config1:
+        line["config1"] = run_config1(eng, matrix, args, torch, peak)
     if world == 1 and args.batched:
         line["batched"] = run_batched(eng, matrix, args, torch)
     if world == 1 and args.serve:
         line["serving"] = run_serving(eng, matrix, args)
     if rank == 0:
         sys.path.insert(0, ROOT)
-        line["cpu_baseline"] = cpu_baseline(matrix, w, args.cpu_seconds, os.cpu_count() or 1)
+        line["cpu_baseline"] = cpu_baseline(matrix, w, args.cpu_seconds)
         print(json.dumps(line), flush=True)
     qry.close()
     db.close()

@@ -80,6 +80,11 @@ SIGNATURES = {
     "bp_engine_launch_count": (u64, [P]),
     "bp_engine_last_scan_ms": (ctypes.c_float, [P]),
     "bp_engine_synchronize": (ctypes.c_int, [P]),
+    "bp_result_digest": (ctypes.c_int, [P, P]),
+    "bp_batch_digest": (ctypes.c_int, [P, ctypes.c_int32, P]),
+    "bp_server_digest": (ctypes.c_int, [P, ctypes.c_uint64, P]),
+    "bp_engine_set_upload_wait": (ctypes.c_int, [P, ctypes.c_uint32]),
+    "bp_engine_drop_chunk_flag": (ctypes.c_int, [P, ctypes.c_int32]),
     "bp_db_create": (ctypes.c_int, [P, P, i64, P, i32, P]),
     "bp_db_create_device": (ctypes.c_int, [P, P, i64, P, i32, P]),
     "bp_db_destroy": (None, [P]),

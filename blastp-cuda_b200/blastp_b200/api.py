@@ -80,6 +80,15 @@ class Engine:
     def synchronize(self):
         check(lib().bp_engine_synchronize(self.h), self.h)
 
+    def set_upload_wait(self, ms: int):
+        """How long a streaming blastp_host scan waits for one upload chunk."""
+        check(lib().bp_engine_set_upload_wait(self.h, int(ms)), self.h)
+
+    def drop_chunk_flag(self, chunk: int):
+        """Fault injection: the next streaming blastp_host call does not
+        announce upload chunk `chunk`, so the scan's bounded wait runs out."""
+        check(lib().bp_engine_drop_chunk_flag(self.h, int(chunk)), self.h)
+
     def database(self, residues: np.ndarray, offsets: np.ndarray) -> "Database":
         return Database(self, residues, offsets)
 
@@ -334,6 +343,12 @@ class PendingResult:
         check(lib().bp_result_copy(self.h, _p(counters), _p(hoff), _p(hsps)), self.engine.h)
         return Result(counters, hoff, hsps[:k])
 
+    def digest(self) -> tuple:
+        """128-bit device-side digest of the result (bp_result_digest)."""
+        out = (ctypes.c_uint64 * 2)()
+        check(lib().bp_result_digest(self.h, out), self.engine.h)
+        return (int(out[0]), int(out[1]))
+
     def close(self):
         if self.h:
             lib().bp_result_destroy(self.h)
@@ -400,6 +415,12 @@ class Batch:
         check(lib().bp_batch_copy_query(self.h, qi, _p(counters), _p(hoff), _p(hsps), ctypes.byref(nh)),
               self.engine.h)
         return Result(counters, hoff, hsps[:nh.value])
+
+    def digest(self, qi: int) -> tuple:
+        """Query qi's result digest (bp_batch_digest), equal to its plain search's."""
+        out = (ctypes.c_uint64 * 2)()
+        check(lib().bp_batch_digest(self.h, qi, out), self.engine.h)
+        return (int(out[0]), int(out[1]))
 
     def close(self):
         if self.h:
@@ -525,6 +546,12 @@ class Server:
         hsps = np.zeros(max(nh.value, 1), dtype=HSP_DTYPE)
         check(lib().bp_server_result(self.h, ticket, _p(counters), _p(hoff), _p(hsps), ctypes.byref(nh), None))
         return Result(counters, hoff, hsps[:nh.value]), float(lat.value)
+
+    def digest(self, ticket: int) -> tuple:
+        """A finished request's result digest (bp_server_digest)."""
+        out = (ctypes.c_uint64 * 2)()
+        check(lib().bp_server_digest(self.h, ticket, out))
+        return (int(out[0]), int(out[1]))
 
     def latency(self, ticket: int) -> float:
         """Arrival-to-completion time (ms) of a finished request."""

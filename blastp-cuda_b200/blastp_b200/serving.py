@@ -26,9 +26,13 @@ def percentile(values, p: float) -> float:
     return float(v[i])
 
 
-def drive(server, queries, arrivals, keep_results: bool = True, release: bool = True):
+def drive(server, queries, arrivals, keep_results: bool = True, release: bool = True, digests=None,
+          digest_first: int = 0):
     """Submits queries[i] at arrivals[i] (seconds after the call), waits for
-    all, and returns (results or None, latencies in ms, submit lateness in ms)."""
+    all, and returns (results or None, latencies in ms, submit lateness in ms).
+    With a list as `digests`, the result digests of the first `digest_first`
+    requests are appended to it (taken after every request was submitted, so
+    they do not delay submissions)."""
     t0 = time.perf_counter()
     tickets, late = [], []
     for q, at in zip(queries, arrivals):
@@ -38,8 +42,10 @@ def drive(server, queries, arrivals, keep_results: bool = True, release: bool = 
         late.append(max(0.0, (time.perf_counter() - t0 - at) * 1e3))
         tickets.append(server.submit(q))
     results, lat = [], []
-    for t in tickets:
+    for i, t in enumerate(tickets):
         server.wait(t)
+        if digests is not None and i < digest_first:
+            digests.append(server.digest(t))
         if keep_results:
             r, ms = server.result(t)
             results.append(r)

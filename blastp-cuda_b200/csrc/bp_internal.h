@@ -48,6 +48,12 @@ struct bp_engine {
     std::vector<int> pool_free;
     std::mutex pool_mu;
     struct HostPath* host_path = nullptr;   // buffers and copy stream of bp_blastp_host
+    // streaming host-to-host search: how long the scan waits for one upload
+    // chunk, and (fault injection, one call) a chunk whose arrival flag is
+    // not sent
+    uint64_t upload_wait_ns = 20ull * 1000 * 1000 * 1000;
+    int32_t drop_flag_chunk = -1;
+    unsigned long long* d_digest = nullptr;   // result digests' two sums
 };
 
 // Frees bp_blastp_host's buffers (engine destruction).
@@ -117,6 +123,7 @@ struct bp_result {
 // Everything the scan kernel reads, by value.
 struct ScanArgs {
     const uint8_t* db;
+    int64_t db_bytes;           // readable bytes from db: the L2 prefetch of a subject stops there
     const int64_t* db_off;
     int32_t first;              // first subject
     int32_t n;                  // subjects to scan
@@ -275,3 +282,8 @@ cudaError_t bp_launch_order(bp_engine* e, int32_t n, const int32_t* d_counters, 
                             int32_t* d_fill, bp_hsp* d_out, int32_t* d_keys, int64_t* d_blocksums);
 int32_t bp_order_blocksums_needed(int32_t n);
 bp_status bp_run_search(bp_engine* e, bp_result* r);
+// Digest of one query's result in device memory: counters (3n), CSR offsets
+// (n+1, taken relative to d_hsp_off[0]) and the records they cover; waits
+// for `st` (see digest.cu).
+bp_status bp_digest_range(bp_engine* e, cudaStream_t st, const int32_t* d_counters, int32_t n,
+                          const int64_t* d_hsp_off, const bp_hsp* d_hsps, uint64_t out[2]);

@@ -169,6 +169,7 @@ bp_status bp_run_search(bp_engine* e, bp_result* r) {
 
     ScanArgs a{};
     a.db = db->d_res;
+    a.db_bytes = ((db->nres + 15) & ~15LL) + 32;   // the allocation's zero padding included
     a.db_off = db->d_off;
     a.first = r->first;
     a.n = n;
@@ -318,6 +319,7 @@ void bp_engine_destroy(bp_engine* e) {
     cudaFree(e->d_counts);
     cudaFree(e->d_fill);
     cudaFree(e->d_blocksums);
+    cudaFree(e->d_digest);
     if (e->h_pool) cudaFreeHost(e->h_pool);
     if (e->ev_scan0) cudaEventDestroy(e->ev_scan0);
     if (e->ev_scan1) cudaEventDestroy(e->ev_scan1);
@@ -333,6 +335,18 @@ float bp_engine_last_scan_ms(const bp_engine* e) { return e ? e->last_scan_ms : 
 bp_status bp_engine_synchronize(bp_engine* e) {
     if (!e) return BP_ERR_INVALID;
     CK(cudaStreamSynchronize(e->stream), "cudaStreamSynchronize");
+    return BP_OK;
+}
+
+bp_status bp_engine_set_upload_wait(bp_engine* e, uint32_t ms) {
+    if (!e || ms == 0) return BP_ERR_INVALID;
+    e->upload_wait_ns = (uint64_t)ms * 1000 * 1000;
+    return BP_OK;
+}
+
+bp_status bp_engine_drop_chunk_flag(bp_engine* e, int32_t chunk) {
+    if (!e) return BP_ERR_INVALID;
+    e->drop_flag_chunk = chunk < 0 ? -1 : chunk;
     return BP_OK;
 }
 
@@ -596,7 +610,6 @@ bp_status bp_result_wait(bp_result* r) {
         float ms = 0.f;
         if (cudaEventElapsedTime(&ms, e->ev_scan0, e->ev_scan1) == cudaSuccess) e->last_scan_ms = ms;
         cudaGetLastError();
-        if (r->h_count[2]) return bp_set_error(e, BP_ERR_TIMEOUT, "scan kernel: a bounded wait ran out");
         const uint32_t count = r->h_count[0];
         if (count <= r->cap) {
             r->n_hsps = count;

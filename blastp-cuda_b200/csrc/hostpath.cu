@@ -241,6 +241,8 @@ extern "C" bp_status bp_blastp_host(bp_engine* e, const uint8_t* query, int32_t 
     // only once staged, so those copies are interleaved with the scans below
     // (chunked launches only: each chunk's counters go back as its scan ends)
     const bool counters_pinned = !streaming && counters && n_subjects > 0 && is_pinned(counters);
+    const int32_t drop_flag = e->drop_flag_chunk;   // fault injection: consumed by this call
+    e->drop_flag_chunk = -1;
     auto upload = [&](int k) -> cudaError_t {
         const int64_t lo = offsets[cf[k]], hi = offsets[cf[k + 1]];
         cudaError_t err = cudaSuccess;
@@ -249,7 +251,7 @@ extern "C" bp_status bp_blastp_host(bp_engine* e, const uint8_t* query, int32_t 
                                   h->copy);
         if (err == cudaSuccess) err = cudaEventRecord(h->ready[k], h->copy);
         // streaming: the chunk's arrival flag, after its data in the same stream
-        if (err == cudaSuccess && streaming)
+        if (err == cudaSuccess && streaming && k != drop_flag)
             err = cudaMemcpyAsync(h->d_flags + k, h->h_gen, sizeof(uint32_t), cudaMemcpyHostToDevice, h->copy);
         return err;
     };
@@ -326,6 +328,7 @@ extern "C" bp_status bp_blastp_host(bp_engine* e, const uint8_t* query, int32_t 
         CKH(cudaEventRecord(e->ev_scan0, e->stream), "cudaEventRecord");
         ScanArgs a{};
         a.db = h->d_res;
+        a.db_bytes = (int64_t)h->res_cap;
         a.db_off = h->d_off;
         a.first = 0;
         a.n = n_subjects;
@@ -353,7 +356,7 @@ extern "C" bp_status bp_blastp_host(bp_engine* e, const uint8_t* query, int32_t 
         a.chunk_first = (const int32_t*)(a.chunk_base + n_chunks);
         a.chunk_flag = h->d_flags;
         a.gen = h->gen;
-        a.wait_ns = 20ull * 1000 * 1000 * 1000;   // a chunk more than 20 s late: the scan gives up
+        a.wait_ns = e->upload_wait_ns;   // a chunk later than this: the scan gives up
         CKH(bp_launch_scan_stream(e, e->stream, a), "streaming scan launch");
         CKH(cudaEventRecord(e->ev_scan1, e->stream), "cudaEventRecord");
     } else {
@@ -375,6 +378,7 @@ extern "C" bp_status bp_blastp_host(bp_engine* e, const uint8_t* query, int32_t 
         CKH(cudaStreamWaitEvent(ss, h->checked[k], 0), "cudaStreamWaitEvent");
         ScanArgs a{};
         a.db = h->d_res;
+        a.db_bytes = (int64_t)h->res_cap;
         a.db_off = h->d_off;
         a.first = cf[k];
         a.n = cf[k + 1] - cf[k];

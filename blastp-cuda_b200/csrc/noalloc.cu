@@ -58,17 +58,26 @@ struct DeviceSetup {
 std::mutex g_setup_mu;
 DeviceSetup g_setup[64];
 
-// counts[3] |= 1 when a query residue is 0 or >= 28, counts[4] |= 1 when a
-// database residue is >= 28.
+// Words of the counts block: [0] records written, [1] subject cursor, [2]
+// unused (the plain scan sets no error word), [3] a query residue is 0 or
+// >= 28, [4] a database residue is >= 28, [5] the offsets are malformed, [6]
+// long subjects listed for the longest-first cursor.
+constexpr int kBadQuery = 3, kBadResidue = 4, kBadOffsets = 5, kLongCount = 6;
+
+// Residue codes of the query and the database, and the ends of the offsets
+// (off[0] == 0, off[n_subjects] == n); the lengths in between are checked by
+// the long-subject listing (each in [0, 2^29]), so together every subject
+// lies inside the caller's residue buffer.
 __global__ void check_inputs(const uint8_t* __restrict__ q, int32_t qlen, const uint8_t* __restrict__ res,
-                             int64_t n, uint32_t* counts) {
+                             int64_t n, const int64_t* __restrict__ off, int32_t n_subjects, uint32_t* counts) {
     uint32_t bq = 0, bd = 0;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     for (int64_t i = t; i < qlen; i += stride) bq |= (q[i] == 0 || q[i] >= BP_ALPHABET);
     for (int64_t i = t; i < n; i += stride) bd |= res[i] >= BP_ALPHABET;
-    if (bq) atomicOr(counts + 3, 1u);
-    if (bd) atomicOr(counts + 4, 1u);
+    if (bq) atomicOr(counts + kBadQuery, 1u);
+    if (bd) atomicOr(counts + kBadResidue, 1u);
+    if (t == 0 && (off[0] != 0 || off[n_subjects] != n)) atomicOr(counts + kBadOffsets, 1u);
 }
 
 bp_status setup_device(int dev, DeviceSetup** out) {
@@ -140,22 +149,30 @@ extern "C" bp_status bp_search_noalloc(const uint8_t* d_query, int32_t qlen, con
 
     const int diag = bp_diag_len(qlen, p->window);
     const int32_t ctx_h[4] = {0, p->x_dropoff, p->cutoff_score, 0};
-    uint32_t hostc[5] = {0, 0, 0, 0, 0};
+    uint32_t hostc[7] = {0, 0, 0, 0, 0, 0, 0};
     uint32_t total = 0;
+    // longest first, as bp_search schedules: the long subjects' list goes into
+    // the fill cursors' slice, which the ordering pass clears after the scan
+    const int32_t long_min = bp_long_threshold(n_residues, n_subjects);
     cudaError_t err = cudaMemsetAsync(counts, 0, 16 * sizeof(uint32_t), cs);
     if (err == cudaSuccess) err = cudaMemcpyAsync(ctx, ctx_h, sizeof(ctx_h), cudaMemcpyHostToDevice, cs);
-    if (err == cudaSuccess && (qlen > 0 || n_residues > 0)) {
-        check_inputs<<<s->sm_count * 4, 256, 0, cs>>>(d_query, qlen, d_residues, n_residues, counts);
+    if (err == cudaSuccess) {
+        check_inputs<<<s->sm_count * 4, 256, 0, cs>>>(d_query, qlen, d_residues, n_residues, d_offsets, n_subjects,
+                                                      counts);
         err = cudaGetLastError();
     }
-    // the residue check must pass before the table build indexes the matrix with query letters
+    if (err == cudaSuccess)
+        err = bp_launch_long_list(&e, cs, d_offsets, 0, n_subjects, long_min, fill, (int32_t*)(counts + kLongCount),
+                                  counts + kBadOffsets);
+    // the checks must pass before the table build indexes the matrix with
+    // query letters and before the scan reads any subject
     if (err == cudaSuccess) err = cudaMemcpyAsync(hostc, counts, sizeof(hostc), cudaMemcpyDeviceToHost, cs);
     if (err == cudaSuccess) err = cudaStreamSynchronize(cs);
     if (err != cudaSuccess) {
         cudaGetLastError();
         return BP_ERR_CUDA;
     }
-    if (hostc[3] || hostc[4]) return BP_ERR_INVALID;
+    if (hostc[kBadQuery] || hostc[kBadResidue] || hostc[kBadOffsets]) return BP_ERR_INVALID;
     err = bp_launch_table_build(&e, d_query, qlen, p->threshold, cells, nullptr, tmp, 0);
     if (err == cudaSuccess) err = cudaMemcpyAsync(&total, cells + BP_NC, sizeof(total), cudaMemcpyDeviceToHost, cs);
     if (err == cudaSuccess) err = cudaStreamSynchronize(cs);
@@ -170,6 +187,7 @@ extern "C" bp_status bp_search_noalloc(const uint8_t* d_query, int32_t qlen, con
     const uint32_t cap = (uint32_t)(hsp_cap < kMaxRecords ? hsp_cap : kMaxRecords);
     ScanArgs a{};
     a.db = d_residues;
+    a.db_bytes = n_residues;   // the caller's buffer: no padding assumed
     a.db_off = d_offsets;
     a.first = 0;
     a.n = n_subjects;
@@ -189,6 +207,9 @@ extern "C" bp_status bp_search_noalloc(const uint8_t* d_query, int32_t qlen, con
     a.rec_count = counts;
     a.cursor = counts + 1;
     a.error = counts + 2;
+    a.long_ids = fill;
+    a.n_long_at = (const int32_t*)(counts + kLongCount);
+    a.long_min = long_min;
     if (err == cudaSuccess && n_subjects > 0) err = bp_launch_scan(&e, a);
     if (err == cudaSuccess)
         err = bp_launch_order(&e, n_subjects, d_counters, d_hsp_off, recs, cap, counts, fill, d_hsps, keys, sums);
@@ -199,7 +220,6 @@ extern "C" bp_status bp_search_noalloc(const uint8_t* d_query, int32_t qlen, con
         return BP_ERR_CUDA;
     }
     *n_hsps = hostc[0];
-    if (hostc[2]) return BP_ERR_TIMEOUT;
     if (hostc[0] > cap) return BP_ERR_TOO_LARGE;   // counters and offsets are complete; HSPs were not written
     return BP_OK;
 }

@@ -304,6 +304,15 @@ __device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
 
+// Prefetches the residues [s, e) of a subject into L2 in whole 16-byte
+// blocks, none of which reaches past db_bytes (a partial last block is left
+// to the warp's own loads).
+__device__ __forceinline__ void prefetch_span(const uint8_t* db, long long db_bytes, long long s, long long e) {
+    const long long lo = s & ~15LL;
+    const long long hi = min((e + 15) & ~15LL, db_bytes & ~15LL);
+    if (hi > lo) prefetch_l2(db + lo, (uint32_t)(hi - lo));
+}
+
 // Residues r..r+kP+1 of the window starting at `sl` (code-1, or -1 past the
 // end).  kCheck: codes of 28 and more (r > 26) are noted in `bad`; every
 // residue of a subject passes through some lane's window.
@@ -830,7 +839,7 @@ scan_kernel(ScanArgs a, ScanLayout lay) {
                 go = -1;
             } else {
                 if (in_range(a, nx.id) && nx.e > nx.s && !done_first(a, n_long, nx.id, nx.e - nx.s))
-                    prefetch_l2(a.db + (nx.s & ~15LL), (uint32_t)(((nx.e + 15) & ~15LL) - (nx.s & ~15LL)));
+                    prefetch_span(a.db, a.db_bytes, nx.s, nx.e);
                 if (in_range(a, nx2.id)) {
                     nx2.s = a.db_off[a.first + (nx2.id & ~kSecond)];
                     nx2.e = a.db_off[a.first + (nx2.id & ~kSecond) + 1];
@@ -942,7 +951,7 @@ scan_stream_kernel(ScanArgs a, ScanLayout lay) {
                 go = -2;                                     // nothing left
             } else {
                 if (nx.id < n && nx.ok && nx.c <= sc->ready && nx.e > nx.s)
-                    prefetch_l2(a.db + (nx.s & ~15LL), (uint32_t)(((nx.e + 15) & ~15LL) - (nx.s & ~15LL)));
+                    prefetch_span(a.db, a.db_bytes, nx.s, nx.e);
                 if (nx2.id < n) nx2.ok = locate(a, nx2.id, sc->hint, nx2.s, nx2.e, nx2.c);
                 if (!cur.ok) {
                     atomicOr(a.bad_off, 1u);

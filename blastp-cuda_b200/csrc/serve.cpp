@@ -349,6 +349,23 @@ bp_status bp_server_result(bp_server* s, uint64_t ticket, int32_t* counters, int
     return bp_batch_copy_query(job->batch, index, counters, hsp_off, hsps, n_hsps);
 }
 
+bp_status bp_server_digest(bp_server* s, uint64_t ticket, uint64_t out[2]) {
+    if (!s || !out) return BP_ERR_INVALID;
+    Job* job = nullptr;
+    int index = -1;
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        auto it = s->reqs.find(ticket);
+        if (it == s->reqs.end()) return BP_ERR_INVALID;
+        Req* r = it->second;
+        if (r->state == BP_REQ_FAILED) return r->status;
+        if (r->state != BP_REQ_DONE) return BP_ERR_NOT_READY;
+        job = r->job;
+        index = r->index;
+    }
+    return bp_batch_digest(job->batch, index, out);
+}
+
 bp_status bp_server_release(bp_server* s, uint64_t ticket) {
     if (!s) return BP_ERR_INVALID;
     std::lock_guard<std::mutex> lock(s->mu);

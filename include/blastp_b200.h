@@ -85,6 +85,15 @@ void* bp_engine_stream(bp_engine* e);               /* cudaStream_t */
 uint64_t bp_engine_launch_count(const bp_engine* e); /* kernels launched so far */
 float bp_engine_last_scan_ms(const bp_engine* e);    /* scan kernel time of the last search */
 bp_status bp_engine_synchronize(bp_engine* e);
+/* The longest a streaming bp_blastp_host call lets its scan wait for one
+ * upload chunk to arrive (default 20,000 ms); past it the scan stops and the
+ * call returns BP_ERR_TIMEOUT, leaving the engine usable.  No counterpart in
+ * the reference, whose upload completes before its launch. */
+bp_status bp_engine_set_upload_wait(bp_engine* e, uint32_t ms);
+/* Fault injection for tests of that bounded wait: the next bp_blastp_host
+ * call that streams copies upload chunk `chunk` but does not announce its
+ * arrival, so the scan's wait for it runs out (chunk < 0: none). */
+bp_status bp_engine_drop_chunk_flag(bp_engine* e, int32_t chunk);
 
 /* Database: residues (NCBIstdaa, each < 28) of n_subjects subjects laid end
  * to end, with n_subjects+1 int64 offsets.  bp_db_create copies from host
@@ -135,6 +144,13 @@ int64_t bp_result_hsps(const bp_result* r);          /* after bp_result_wait */
  *   hsp_off   int64[subjects+1]: CSR offsets into hsps
  *   hsps      bp_hsp[bp_result_hsps()], per subject in discovery order */
 bp_status bp_result_copy(bp_result* r, int32_t* counters, int64_t* hsp_off, bp_hsp* hsps);
+/* A 128-bit digest of the result (counters, CSR offsets, HSP records in
+ * order), computed on the device; equal results give equal digests, and
+ * different ones differ with overwhelming probability.  For comparing large
+ * result sets without copying them to the host (bp_batch_digest and
+ * bp_server_digest give the same digest for the same result).  No
+ * counterpart in the reference. */
+bp_status bp_result_digest(bp_result* r, uint64_t out[2]);
 void bp_result_destroy(bp_result* r);
 
 /* One call from host buffers to host buffers: uploads the database and the
@@ -201,6 +217,8 @@ float bp_batch_last_scan_ms(const bp_batch* b);      /* device time of the last 
  * for the batch's subjects (index 0 = subject_first). */
 bp_status bp_batch_copy_query(bp_batch* b, int32_t qi, int32_t* counters, int64_t* hsp_off, bp_hsp* hsps,
                               int64_t* n_hsps);
+/* Query qi's result digest (as bp_result_digest). */
+bp_status bp_batch_digest(bp_batch* b, int32_t qi, uint64_t out[2]);
 /* Predicted load of each CTA queue (BP_SCHED_COSTS), for reporting. */
 bp_status bp_batch_queue_costs(const bp_batch* b, double* costs, int32_t* n_queues);
 /* Queue (index into bp_batch_queue_costs' list) of every item q*n_chunks + c;
@@ -339,6 +357,8 @@ bp_status bp_server_wait(bp_server* s, uint64_t ticket, int32_t timeout_ms);
 /* The finished request's results, in the bp_result_copy layout. */
 bp_status bp_server_result(bp_server* s, uint64_t ticket, int32_t* counters, int64_t* hsp_off, bp_hsp* hsps,
                            int64_t* n_hsps, double* latency_ms);
+/* The finished request's result digest (as bp_result_digest). */
+bp_status bp_server_digest(bp_server* s, uint64_t ticket, uint64_t out[2]);
 /* Gives the request's device memory back to the budget. */
 bp_status bp_server_release(bp_server* s, uint64_t ticket);
 bp_status bp_server_stats(bp_server* s, bp_server_metrics* out);
@@ -350,10 +370,13 @@ void bp_server_destroy(bp_server* s);
  * buffers come from an outside allocator.  No counterpart in the reference.
  *
  * The caller passes device buffers for everything: the query (d_query,
- * residues 1..27), the database (d_residues, d_offsets with n_subjects+1
- * entries running from 0 to n_residues), and the outputs d_counters
- * (3*n_subjects int32), d_hsp_off (n_subjects+1 int64) and d_hsps (hsp_cap
- * records).  Scratch -- neighbour table, unordered HSP records, ordering
+ * residues 1..27), the database (d_residues, exactly n_residues bytes: no
+ * padding is read past them; d_offsets with n_subjects+1 entries running
+ * from 0 to n_residues, non-decreasing, each subject below 2^29 residues --
+ * checked on the device before anything is scanned), and the outputs
+ * d_counters (3*n_subjects int32), d_hsp_off (n_subjects+1 int64) and d_hsps
+ * (hsp_cap records).  Subjects of twice the mean length are scanned first, as
+ * bp_search does.  Scratch -- neighbour table, unordered HSP records, ordering
  * cursors -- is one static 16 MiB device array in the library; the call makes
  * no cudaMalloc or cudaFree.  Limits: n_subjects <= 1,048,576, qlen <= 4096,
  * neighbour-table entries <= 1,048,576, HSPs per call <= min(hsp_cap, 262,144);
@@ -363,7 +386,9 @@ void bp_server_destroy(bp_server* s);
  * in place.  The first call on a device sets the array up (looks up its
  * device address and copies the scoring matrix, synchronously), so make it
  * before any stream capture.  Every call reuses the same array: calls that
- * overlap on the GPU race and must be serialised by the caller. */
+ * overlap on the GPU race and must be serialised by the caller.  Returns
+ * BP_OK, BP_ERR_INVALID (bad arguments, residue codes or offsets),
+ * BP_ERR_TOO_LARGE (a limit above), BP_ERR_NO_DEVICE or BP_ERR_CUDA. */
 bp_status bp_search_noalloc(const uint8_t* d_query, int32_t qlen, const bp_params* p, const uint8_t* d_residues,
                             int64_t n_residues, const int64_t* d_offsets, int32_t n_subjects, int32_t* d_counters,
                             int64_t* d_hsp_off, bp_hsp* d_hsps, int64_t hsp_cap, int64_t* n_hsps, void* stream);

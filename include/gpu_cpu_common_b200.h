@@ -20,9 +20,12 @@
  * copies d_Hits[oid*3+{hits, successful extensions, extensions}] and the
  * two-slot-per-subject HSP ring to the host; GPU_BLASTP_free_memory frees the
  * slots.  What changed behind it: the slots hold this engine's buffers, every
- * CUDA call is checked (a failure is printed and leaves the counters zero so
- * the caller's CPU path re-searches), and the ring is filled from the
- * complete, ordered HSP set.
+ * CUDA call is checked, and the ring is filled from the complete, ordered HSP
+ * set.  On a failure the cause is printed and every subject's counters read
+ * {0 hits, 3 successful extensions, 0 extensions}: more successful
+ * extensions than the two ring slots hold, which is the condition under
+ * which NCBI's ingestion re-searches a subject on the CPU
+ * (blast_engine.c:529-538), so no subject is silently dropped.
  *
  * Build inside the NCBI tree with -DBLASTP_B200_WITH_NCBI so the NCBI types
  * come from NCBI's headers; otherwise they come from ncbi_compat.h.

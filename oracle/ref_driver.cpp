@@ -46,6 +46,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <chrono>
 #include <vector>
 
 dim3 gridDim;
@@ -121,7 +122,10 @@ extern "C" int32_t ref_ring_slots(void) { return MAX_SUCCESSFUL_HITS_PER_SEQUENC
  *   blocks, threads     the launch shape; threads a multiple of 16
  * Out: hits[n*3] (hits, successful extensions, extensions), ring[n*slots*6]
  * (GPUBlastInitHitList records, slot = rank mod slots, zero when unused),
- * group_len[n] (the padded length each subject was scanned over).
+ * group_len[n] (the padded length each subject was scanned over), and, when
+ * kernel_ns is not null, the wall time of the kernel's execution alone (the
+ * blocks' threads from start to join; the layout work before it, which the
+ * reference does once when it writes its database file, is not included).
  * Returns 0, or a negative code for arguments outside the kernel's limits.
  */
 extern "C" int32_t ref_two_hit(const uint8_t* residues, const int64_t* offsets, int32_t n_subjects,
@@ -130,7 +134,7 @@ extern "C" int32_t ref_two_hit(const uint8_t* residues, const int64_t* offsets, 
                                int32_t n_ctx, const int32_t* ctx_offset, const int32_t* ctx_xdrop,
                                const int32_t* ctx_cutoff, int32_t window, int32_t diag_array_length,
                                int32_t diag_offset, int32_t blocks, int32_t threads, int32_t* hits,
-                               int32_t* ring, int32_t* group_len)
+                               int32_t* ring, int32_t* group_len, int64_t* kernel_ns)
 {
     if (n_subjects < 0 || qlen < 0 || qlen > QUERY_LENGTH_MAX) return -1;
     if (n_ctx < 1 || n_ctx > NUM_QUERIES_MAX) return -2;
@@ -216,6 +220,7 @@ extern "C" int32_t ref_two_hit(const uint8_t* residues, const int64_t* offsets, 
     std::vector<KernelArgs> args(threads);
     std::vector<pthread_t> tid(threads);
     int rc = 0;
+    const auto t0 = std::chrono::steady_clock::now();
     for (int b = 0; b < blocks && rc == 0; ++b) {
         memset(array, 0, sizeof(int) * shared_ints);
         pthread_barrier_init(&refshim_block_barrier, nullptr, threads);
@@ -235,6 +240,9 @@ extern "C" int32_t ref_two_hit(const uint8_t* residues, const int64_t* offsets, 
         for (int t = 0; t < started; ++t) pthread_join(tid[t], nullptr);
         pthread_barrier_destroy(&refshim_block_barrier);
     }
+    if (kernel_ns)
+        *kernel_ns = std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - t0)
+                         .count();
     memcpy(ring, list.data(), sizeof(int32_t) * 6 * (size_t)n_subjects * slots);
     return rc;
 }

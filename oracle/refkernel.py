@@ -39,7 +39,7 @@ def _lib(slots):
         L.ref_ring_slots.argtypes = []
         L.ref_two_hit.restype = i32
         L.ref_two_hit.argtypes = [P, P, i32, P, i32, P, P, P, i32, i32, P, P, P, i32, i32, i32,
-                                  i32, i32, P, P, P]
+                                  i32, i32, P, P, P, P]
         assert L.ref_ring_slots() == slots
         _libs[slots] = L
     return _libs[slots]
@@ -51,9 +51,10 @@ def _p(a):
 
 def two_hit(residues, offsets, query, table, matrix28, contexts, window=40,
             diag_array_length=None, diag_offset=None, blocks=1, threads=64,
-            matrix_bytes=28 * 28, slots=64):
+            matrix_bytes=28 * 28, slots=64, timing=None):
     """contexts: list of (query_offset, xdrop, cutoff).  Returns
-    (hits int32[n,3], ring int32[n,slots,6], group_len int32[n])."""
+    (hits int32[n,3], ring int32[n,slots,6], group_len int32[n]); when
+    `timing` is a dict, timing["kernel_s"] receives the kernel's own time."""
     res = np.ascontiguousarray(residues, dtype=np.uint8)
     off = np.ascontiguousarray(offsets, dtype=np.int64)
     q = np.ascontiguousarray(query, dtype=np.uint8)
@@ -72,13 +73,16 @@ def two_hit(residues, offsets, query, table, matrix28, contexts, window=40,
     hits = np.zeros((max(n, 1), 3), dtype=np.int32)
     ring = np.zeros((max(n, 1), slots, 6), dtype=np.int32)
     glen = np.zeros(max(n, 1), dtype=np.int32)
+    kns = ctypes.c_int64(0)
     rc = _lib(slots).ref_two_hit(_p(res if len(res) else np.zeros(1, np.uint8)), _p(off), n, _p(q), len(q),
                                  _p(start), _p(ent), _p(m), matrix_bytes, len(contexts), _p(co), _p(cx),
                                  _p(cc), window, diag_array_length,
                                  window if diag_offset is None else diag_offset, blocks, threads,
-                                 _p(hits), _p(ring), _p(glen))
+                                 _p(hits), _p(ring), _p(glen), ctypes.byref(kns))
     if rc != 0:
         raise ValueError("ref_two_hit rejected its arguments (code %d)" % rc)
+    if timing is not None:
+        timing["kernel_s"] = kns.value / 1e9
     return hits[:n], ring[:n], glen[:n]
 
 

@@ -29,7 +29,10 @@ def test_reference_line():
     assert d["value"] > 0 and d["higher_is_better"] is True
     assert d["steps"] == 2 and d["warmup"] == 3 and d["n_gpus"] == 1
     assert d["config"]["workload"] == "q500_vs_1M" and d["config"]["query_len"] == 500
-    assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["value"] == d["value"]
+    # the reference's own kernel host-compiled (oracle/_ref) where it was built, else the oracle port
+    from oracle import refkernel
+    assert d["cpu_baseline"]["kind"] == ("reference" if refkernel.available(2) else "port")
+    assert d["cpu_baseline"]["value"] == d["value"]
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
     # one query per step: the length-weighted rate is the value times the query length
     assert abs(d["residue_pairs_per_s"] - d["value"] * 500) <= 1e-6 * d["residue_pairs_per_s"]

@@ -209,3 +209,27 @@ def test_many_short_queries_packed(engine, matrix):
         s = engine.search(d, h, 100, 4500).fetch()
         assert_same(b.fetch(i), (s.counters, s.hsp_off, s.hsps_as_array()), "short query %d" % i)
     b.close()
+
+
+def test_digests_match_plain_and_tell_results_apart(engine, workload):
+    # The device-side digest of each query's batched result equals the digest
+    # of its plain search; the queries' digests all differ (their results do),
+    # and a result differing in one HSP field changes the digest.
+    qs, db = workload
+    d = engine.database(db.residues, db.offsets)
+    hs = [engine.query(q) for q in qs]
+    plain = []
+    for h in hs:
+        r = engine.search(d, h)
+        plain.append((r.digest(), r.fetch()))
+        r.close()
+    b = engine.search_batch(d, hs, chunk_residues=1 << 16)
+    digests = [b.digest(i) for i in range(len(qs))]
+    for i, (pd, res) in enumerate(plain):
+        assert digests[i] == pd, "query %d" % i
+    distinct = {digests[i] for i in range(len(qs)) if len(plain[i][1].hsps)}
+    assert len(distinct) == sum(1 for _, r in plain if len(r.hsps))
+    b.close()
+    for h in hs:
+        h.close()
+    d.close()

@@ -255,3 +255,29 @@ def test_host_path_rejects_bad_residues(engine):
         engine.blastp_host(enc("WCWHEAL"), default_params(), pin.numpy(), np.array([0, 500, 1000], np.int64))
     pin.numpy()[777] = 27
     engine.blastp_host(enc("WCWHEAL"), default_params(), pin.numpy(), np.array([0, 500, 1000], np.int64))
+
+
+def test_host_path_stalled_chunk_times_out(engine, matrix):
+    # A chunk whose arrival is never announced (its data is copied, its flag
+    # is not): the streaming scan's bounded wait runs out after the set limit,
+    # the call returns BP_ERR_TIMEOUT within seconds, and the engine then
+    # searches correctly with the default limit restored.
+    import time
+
+    import torch
+    w = synth.shape2(matrix, rep=4, n_subjects=60_000)      # ~21.6M residues: three 8 MiB chunks
+    q = w.queries[0]
+    pin = torch.empty(len(w.db.residues), dtype=torch.uint8, pin_memory=True)
+    pin.numpy()[:] = w.db.residues
+    ref = gpu_search(engine, q, w.db.residues, w.db.offsets)
+    for chunk in (1, 0):
+        engine.set_upload_wait(5)
+        engine.drop_chunk_flag(chunk)
+        t0 = time.time()
+        with pytest.raises(BpError) as ei:
+            engine.blastp_host(q, default_params(), pin.numpy(), w.db.offsets)
+        assert ei.value.status == 5, str(ei.value)          # BP_ERR_TIMEOUT
+        assert time.time() - t0 < 10.0
+        engine.set_upload_wait(20_000)
+        got = engine.blastp_host(q, default_params(), pin.numpy(), w.db.offsets)
+        assert_same(got, (ref.counters, ref.hsp_off, ref.hsps_as_array()), "after a stalled chunk %d" % chunk)

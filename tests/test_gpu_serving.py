@@ -92,3 +92,19 @@ def test_bad_requests_rejected(engine, world):
     with pytest.raises(BpError):
         srv.submit(np.ones(70_000, np.uint8))
     srv.close()
+
+
+def test_served_digests_equal_plain(engine, world):
+    # the digest of each served request equals its plain search's digest
+    qs, db, d, alone = world
+    srv = Server(engine, d, max_batch_queries=4, lanes=2, chunk_residues=1 << 18)
+    tickets = [srv.submit(q) for q in qs[:8]]
+    for i, t in enumerate(tickets):
+        srv.wait(t)
+        h = engine.query(qs[i])
+        r = engine.search(d, h)
+        assert srv.digest(t) == r.digest(), "request %d" % i
+        r.close()
+        h.close()
+        srv.release(t)
+    srv.close()

@@ -77,3 +77,43 @@ def test_noalloc_reports_limits():
     bad[3] = 0
     st, *_ = run_noalloc(bad, w.db.residues, w.db.offsets, p, 1024)
     assert st == 1
+
+
+def test_noalloc_rejects_malformed_offsets():
+    # Offsets are checked on the device before any subject is read: a
+    # decreasing pair, an end past the residues, a start other than 0 and a
+    # subject longer than 2^29 are each refused with BP_ERR_INVALID, and the
+    # next call with good offsets still matches bp_search.
+    matrix = np.asarray(__import__("blastp_b200").blosum62())
+    w = synth.shape1(matrix, n_subjects=4_000)
+    q = w.queries[0]
+    p = default_params()
+    off = w.db.offsets
+    bads = []
+    b = off.copy()
+    b[100], b[101] = off[101], off[100]
+    bads.append(b)
+    b = off.copy()
+    b[2000] = off[-1] + 4096
+    bads.append(b)
+    b = off.copy()
+    b[-1] = off[-1] + 64
+    bads.append(b)
+    b = off.copy()
+    b[0] = 8
+    bads.append(b)
+    b = off.copy()
+    b[1:] = off[-1]
+    b[1] = (1 << 29) + 1
+    bads.append(b)
+    for k, bad in enumerate(bads):
+        st, *_ = run_noalloc(q, w.db.residues, bad, p, 1024)
+        assert st == 1, "malformed offsets %d: status %d" % (k, st)
+    eng = Engine(0)
+    try:
+        ref = eng.search(eng.database(w.db.residues, off), eng.query(q, p)).fetch()
+    finally:
+        eng.close()
+    st, nh, counters, hoff, hsps = run_noalloc(q, w.db.residues, off, p, hsp_cap=65536)
+    assert st == 0 and nh == len(ref.hsps)
+    assert_same(_R(counters, hoff, hsps), (ref.counters, ref.hsp_off, ref.hsps_as_array()), "after refusals")
