@@ -56,6 +56,7 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--config1", type=int, default=1, help="also time one 300-aa query vs 10,000 subjects")
     ap.add_argument("--config1-reps", type=int, default=100)
+    ap.add_argument("--gapped", type=int, default=1, help="also time the gapped stage on the headline search")
     ap.add_argument("--cpu-seconds", type=float, default=3.0, help="wall-clock budget of the CPU baseline sample")
     ap.add_argument("--batched", type=int, default=1, help="also measure the batched workload (1 GPU runs only)")
     ap.add_argument("--batch-subjects", type=int, default=2_000_000)
@@ -292,6 +293,25 @@ def run_config1(eng, matrix, args, torch, peak):
                          "hbm_floor_us": alg / (peak * 1e9) * 1e6},
             "hits": int(res.counters[:, 0].sum()), "extensions": int(res.counters[:, 2].sum()),
             "hsps": int(len(res.hsps))}
+
+
+def run_gapped_stage(eng, db, qry, reps=5):
+    """The gapped stage (bp_gapped_run) on the headline search's ungapped
+    HSPs: device time of the stage (its own CUDA events), HSPs in and out."""
+    import blastp_b200 as bp
+    r = eng.search(db, qry)
+    r.wait()
+    times, g = [], None
+    for _ in range(reps + 1):
+        g = r.gapped(bp.gapped_params())
+        times.append(g.ms)
+    r.close()
+    ms = float(np.median(times[1:]))
+    n_ext = int(g.counters[:, 2].sum())
+    return {"params": {"gap_open": 11, "gap_extend": 1, "x_dropoff": 38, "cutoff": 0},
+            "ms": ms, "ungapped_hsps": int(g.counters[:, 0].sum()), "extensions": n_ext,
+            "gapped_hsps": int(len(g.hsps)), "extensions_per_s": n_ext / (ms / 1e3),
+            "subjects_with_hsps": int((g.counters[:, 0] > 0).sum())}
 
 
 def run_batched(eng, matrix, args, torch):
@@ -704,6 +724,8 @@ def run_ours(args):
     line["clocks"] = clocks
     if world == 1 and args.config1:
         line["config1"] = run_config1(eng, matrix, args, torch, peak)
+    if world == 1 and args.gapped:
+        line["gapped"] = run_gapped_stage(eng, db, qry)
     if world == 1 and args.batched:
         line["batched"] = run_batched(eng, matrix, args, torch)
     if world == 1 and args.serve:

@@ -6,6 +6,7 @@ synthetic-data generators used by the benchmark and the tests.
 """
 from . import synth  # noqa: F401
 from ._lib import BpError, BpParams, lib  # noqa: F401
-from .api import (HSP_DTYPE, Batch, Database, Engine, Mlp, PendingResult, Query, Result, Server,  # noqa: F401
-                  blosum62, default_params, read_database_file, write_database_file)
+from .api import (GAPPED_DTYPE, HSP_DTYPE, Batch, Database, Engine, GappedResult, Mlp, PendingResult,  # noqa: F401
+                  Query, Result, Server, blosum62, default_params, gapped_params, read_database_file,
+                  write_database_file)
 from . import costmodel  # noqa: F401,E402

@@ -25,6 +25,10 @@ class BpParams(ctypes.Structure):
                 ("x_dropoff", i32), ("cutoff_score", i32)]
 
 
+class BpGappedParams(ctypes.Structure):
+    _fields_ = [("gap_open", i32), ("gap_extend", i32), ("x_dropoff", i32), ("cutoff_score", i32)]
+
+
 class BpBatchOptions(ctypes.Structure):
     _fields_ = [("chunk_residues", i32), ("schedule", i32), ("ctas", i32), ("max_warps", i32),
                 ("use_graph", i32), ("item_costs", P), ("subject_first", i32), ("subject_count", i32),
@@ -83,6 +87,13 @@ SIGNATURES = {
     "bp_result_digest": (ctypes.c_int, [P, P]),
     "bp_batch_digest": (ctypes.c_int, [P, ctypes.c_int32, P]),
     "bp_server_digest": (ctypes.c_int, [P, ctypes.c_uint64, P]),
+    "bp_gapped_params_default": (None, [P]),
+    "bp_gapped_run": (ctypes.c_int, [P, P, P]),
+    "bp_gapped_run_ring": (ctypes.c_int, [P, P, ctypes.c_int32, P]),
+    "bp_gapped_hsps": (ctypes.c_int64, [P]),
+    "bp_gapped_ms": (ctypes.c_float, [P]),
+    "bp_gapped_copy": (ctypes.c_int, [P, P, P, P]),
+    "bp_gapped_destroy": (None, [P]),
     "bp_engine_set_upload_wait": (ctypes.c_int, [P, ctypes.c_uint32]),
     "bp_engine_drop_chunk_flag": (ctypes.c_int, [P, ctypes.c_int32]),
     "bp_db_create": (ctypes.c_int, [P, P, i64, P, i32, P]),

@@ -9,11 +9,23 @@ import ctypes
 import numpy as np
 
 from . import _lib
-from ._lib import (COST_FEATURES, BpAutotuneOptions, BpAutotuneTrial, BpBatchOptions, BpParams, BpServerMetrics,
-                   BpServerOptions, check, lib)
+from ._lib import (COST_FEATURES, BpAutotuneOptions, BpAutotuneTrial, BpBatchOptions, BpGappedParams, BpParams,
+                   BpServerMetrics, BpServerOptions, check, lib)
 
 HSP_DTYPE = np.dtype([("hsp_q", "<i4"), ("hsp_s", "<i4"), ("query_offset", "<i4"),
                       ("subject_offset", "<i4"), ("hsp_len", "<i4"), ("score", "<i4")])
+
+
+GAPPED_DTYPE = np.dtype([("score", "<i4"), ("q_start", "<i4"), ("q_end", "<i4"), ("s_start", "<i4"),
+                         ("s_end", "<i4"), ("q_seed", "<i4"), ("s_seed", "<i4"), ("ungapped", "<i4")])
+
+
+def gapped_params(**kw) -> BpGappedParams:
+    p = BpGappedParams()
+    lib().bp_gapped_params_default(ctypes.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
 
 
 def _p(a):
@@ -323,6 +335,20 @@ class Query:
             pass
 
 
+class GappedResult:
+    """Per-subject counters (ungapped HSPs, gapped HSPs reported, extensions
+    run) and the gapped HSPs as CSR, in processing order."""
+
+    def __init__(self, counters, off, hsps, ms):
+        self.counters = counters
+        self.off = off
+        self.hsps = hsps
+        self.ms = ms
+
+    def hsps_as_array(self):
+        return self.hsps.view(np.int32).reshape(-1, 8)
+
+
 class PendingResult:
     def __init__(self, engine: Engine, h, keep=()):
         self.engine = engine
@@ -342,6 +368,27 @@ class PendingResult:
         hsps = np.zeros(max(k, 1), dtype=HSP_DTYPE)
         check(lib().bp_result_copy(self.h, _p(counters), _p(hoff), _p(hsps)), self.engine.h)
         return Result(counters, hoff, hsps[:k])
+
+    def gapped(self, params: BpGappedParams | None = None, ring_columns: int = 0) -> "GappedResult":
+        """The gapped stage on this result (bp_gapped_run)."""
+        self.wait()
+        h = ctypes.c_void_p()
+        p = params or gapped_params()
+        if ring_columns:
+            check(lib().bp_gapped_run_ring(self.h, ctypes.byref(p), int(ring_columns), ctypes.byref(h)),
+                  self.engine.h)
+        else:
+            check(lib().bp_gapped_run(self.h, ctypes.byref(p), ctypes.byref(h)), self.engine.h)
+        try:
+            n = lib().bp_result_subjects(self.h)
+            k = int(lib().bp_gapped_hsps(h))
+            counters = np.zeros((n, 3), dtype=np.int32)
+            off = np.zeros(n + 1, dtype=np.int64)
+            hsps = np.zeros(max(k, 1), dtype=GAPPED_DTYPE)
+            check(lib().bp_gapped_copy(h, _p(counters), _p(off), _p(hsps)), self.engine.h)
+            return GappedResult(counters, off, hsps[:k], float(lib().bp_gapped_ms(h)))
+        finally:
+            lib().bp_gapped_destroy(h)
 
     def digest(self) -> tuple:
         """128-bit device-side digest of the result (bp_result_digest)."""

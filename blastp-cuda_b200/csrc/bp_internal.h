@@ -281,6 +281,10 @@ cudaError_t bp_launch_order(bp_engine* e, int32_t n, const int32_t* d_counters, 
                             const HspRec* d_recs, uint32_t rec_cap, const uint32_t* d_rec_count,
                             int32_t* d_fill, bp_hsp* d_out, int32_t* d_keys, int64_t* d_blocksums);
 int32_t bp_order_blocksums_needed(int32_t n);
+// CSR offsets (n+1) from the second of every three int32 counters per
+// subject (the ordering pass's first three launches), on `st`.
+cudaError_t bp_launch_offsets(bp_engine* e, cudaStream_t st, int32_t n, const int32_t* d_counters, int64_t* d_off,
+                              int32_t* d_fill, int64_t* d_blocksums);
 bp_status bp_run_search(bp_engine* e, bp_result* r);
 // Digest of one query's result in device memory: counters (3n), CSR offsets
 // (n+1, taken relative to d_hsp_off[0]) and the records they cover; waits

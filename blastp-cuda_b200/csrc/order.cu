@@ -137,6 +137,17 @@ __global__ void sort_segments(int32_t n, const int64_t* __restrict__ off, const 
 
 int32_t bp_order_blocksums_needed(int32_t n) { return (n + kScanTile - 1) / kScanTile + 1; }
 
+cudaError_t bp_launch_offsets(bp_engine* e, cudaStream_t st, int32_t n, const int32_t* d_counters, int64_t* d_off,
+                              int32_t* d_fill, int64_t* d_blocksums) {
+    const int32_t nb = (n + kScanTile - 1) / kScanTile;
+    if (nb == 0) return cudaMemsetAsync(d_off, 0, sizeof(int64_t), st);
+    tile_sums<<<nb, kScanThreads, 0, st>>>(d_counters, n, d_blocksums);
+    scan_sums<<<1, 1024, 0, st>>>(d_blocksums, nb);
+    tile_scan<<<nb, kScanThreads, 0, st>>>(d_counters, n, d_blocksums, nb, d_off, d_fill);
+    e->launches += 3;
+    return cudaGetLastError();
+}
+
 cudaError_t bp_launch_order(bp_engine* e, int32_t n, const int32_t* d_counters, int64_t* d_hsp_off,
                             const HspRec* d_recs, uint32_t rec_cap, const uint32_t* d_rec_count,
                             int32_t* d_fill, bp_hsp* d_out, int32_t* d_keys, int64_t* d_blocksums) {

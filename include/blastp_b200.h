@@ -153,6 +153,61 @@ bp_status bp_result_copy(bp_result* r, int32_t* counters, int64_t* hsp_off, bp_h
 bp_status bp_result_digest(bp_result* r, uint64_t out[2]);
 void bp_result_destroy(bp_result* r);
 
+/* ---- Gapped stage: the consumer of the ungapped HSPs -------------------
+ * Replaces the call the reference makes after ingesting the ungapped HSPs,
+ * aux_struct->GetGappedScore (ncbi_blast_files/blast_engine.c:588-591), which
+ * is NCBI BLAST+ code not shipped with the reference.  Score-only gapped
+ * X-drop extension with affine gaps (Altschul et al. 1997), on the device,
+ * from each ungapped HSP of a finished single-context search:
+ *  - a subject's ungapped HSPs are taken by descending score (equal scores in
+ *    discovery order); one whose query and subject ranges both lie inside a
+ *    gapped HSP already reported for the subject is skipped;
+ *  - seed: the middle letter of an HSP of at most 11 letters, else offset 5
+ *    of its first highest-scoring 11-letter window;
+ *  - two dynamic programmes from the seed: leftwards over the letters up to
+ *    and including the seed pair, rightwards over the letters after it, each
+ *    with H = max(diagonal + S, E, F), E/F = max(H - open, E/F) - extend
+ *    (a k-letter gap costs open + k * extend), cells below the best score so
+ *    far minus x_dropoff dead (tested once per query row, after the row), a
+ *    row's band running from the previous row's first live column to one past
+ *    its last, then on while the horizontal-gap score stays >= best -
+ *    x_dropoff; each returns its best score and the first cell (lowest row,
+ *    then column) reaching it;
+ *  - the gapped HSP (score = left + right) is reported when score >=
+ *    cutoff_score.
+ * Defaults: open 11, extend 1 (BLOSUM62's usual costs), x_dropoff 38 (15
+ * bits at the gapped lambda 0.267), cutoff 0. */
+typedef struct bp_gapped bp_gapped;
+typedef struct bp_gapped_params {
+    int32_t gap_open;         /* 0..65535 */
+    int32_t gap_extend;       /* 1..255 */
+    int32_t x_dropoff;        /* raw, 0..2^20 */
+    int32_t cutoff_score;     /* raw */
+} bp_gapped_params;
+typedef struct bp_gapped_hsp {
+    int32_t score;
+    int32_t q_start, q_end;   /* query range, end exclusive */
+    int32_t s_start, s_end;   /* subject range, end exclusive */
+    int32_t q_seed, s_seed;   /* the seed pair */
+    int32_t ungapped;         /* the ungapped HSP it came from (index within its subject) */
+} bp_gapped_hsp;
+void bp_gapped_params_default(bp_gapped_params* p);
+/* Runs the gapped stage on r (waits for it).  The search's database and
+ * query must still exist.  Per subject out: counters {ungapped HSPs, gapped
+ * HSPs reported, extensions run}, and the reported HSPs as CSR in processing
+ * order.  Bands of up to 2,048 columns run in the main launch; a subject
+ * with a wider band is redone by a second launch with a ring spanning it. */
+bp_status bp_gapped_run(bp_result* r, const bp_gapped_params* p, bp_gapped** out);
+/* The same with a given band ring width (a power of two >= 64), for tests of
+ * the wide-band path. */
+bp_status bp_gapped_run_ring(bp_result* r, const bp_gapped_params* p, int32_t ring_columns, bp_gapped** out);
+int64_t bp_gapped_hsps(const bp_gapped* g);
+float bp_gapped_ms(const bp_gapped* g);              /* device time of the stage */
+/* Copies to host memory (any pointer may be NULL): counters int32[3*n],
+ * off int64[n+1], hsps bp_gapped_hsp[bp_gapped_hsps()]. */
+bp_status bp_gapped_copy(bp_gapped* g, int32_t* counters, int64_t* off, bp_gapped_hsp* hsps);
+void bp_gapped_destroy(bp_gapped* g);
+
 /* One call from host buffers to host buffers: uploads the database and the
  * query, searches, and copies the results back (the end-to-end form).
  * hsps may be NULL to only size the result (n_hsps out).  The upload runs

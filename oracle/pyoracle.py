@@ -114,3 +114,75 @@ def scan_subject(subj, query, cells, matrix, contexts, window, diag_mask):
                 hsps.append((hq, hs, q, s, ln, sc))
             state[d] = ("ext", s_last - (WORD - 1)) if rext else ("hit", s)
     return (hits, len(hsps), ext), hsps
+
+
+# ---- gapped stage (conventions of oracle/gapped.h), for small cases -------
+
+GNEG = -(1 << 28)
+GWINDOW = 11
+
+
+def gapped_extend(M, A, B, xdrop, go, ge):
+    """One extension over A, B (walk order), rows kept as dicts of live cells."""
+    best, bi, bj = 0, 0, 0
+    row, frow = {0: 0}, {0: GNEG}
+    e, hl = GNEG, 0
+    for j in range(1, len(B) + 1):
+        e = max(max(hl - go, e) - ge, GNEG)
+        if e < -xdrop:
+            break
+        row[j], frow[j], hl = e, GNEG, e
+    prev_h, prev_f = row, frow
+    for i in range(1, len(A) + 1):
+        lo, last = min(prev_h), max(prev_h)
+        floor_prev = best - xdrop
+        cur_h, cur_f = {}, {}
+        e, hl = GNEG, GNEG
+        j = lo
+        while j <= len(B):
+            up_h, up_f = prev_h.get(j, GNEG), prev_f.get(j, GNEG)
+            f = max(max(up_h - go, up_f) - ge, GNEG)
+            e = max(max(hl - go, e) - ge, GNEG)
+            dg = prev_h.get(j - 1, GNEG)
+            d = GNEG if dg == GNEG else dg + M[A[i - 1]][B[j - 1]]
+            if j > last + 1 and e < floor_prev:
+                break
+            h = max(d, e, f)
+            cur_h[j], cur_f[j], hl = h, f, h
+            j += 1
+        rmax = max(cur_h.values())
+        rj = min(k for k, v in cur_h.items() if v == rmax)
+        if rmax > best:
+            best, bi, bj = rmax, i, rj
+        fl = best - xdrop
+        prev_h = {k: v for k, v in cur_h.items() if v >= fl}
+        prev_f = {k: cur_f[k] for k in prev_h}
+        if not prev_h:
+            break
+    return best, bi, bj
+
+
+def gapped_seed(M, q, s, hq, hs, ln):
+    if ln <= GWINDOW:
+        return hq + ln // 2, hs + ln // 2
+    wins = [sum(M[q[hq + k + t]][s[hs + k + t]] for t in range(GWINDOW)) for k in range(ln - GWINDOW + 1)]
+    k = wins.index(max(wins))
+    return hq + k + GWINDOW // 2, hs + k + GWINDOW // 2
+
+
+def gapped_subject(M, q, s, hsps, go=11, ge=1, xdrop=38, cutoff=0):
+    """hsps: the subject's ungapped HSPs (hsp_q, hsp_s, q_off, s_off, len,
+    score) in discovery order.  Returns the gapped HSPs as tuples
+    (score, q_start, q_end, s_start, s_end, q_seed, s_seed, ungapped)."""
+    order = sorted(range(len(hsps)), key=lambda k: -hsps[k][5])   # stable: discovery order among equals
+    out = []
+    for k in order:
+        hq, hs, _, _, ln, _ = hsps[k]
+        if any(g[1] <= hq and hq + ln <= g[2] and g[3] <= hs and hs + ln <= g[4] for g in out):
+            continue
+        qs, ss = gapped_seed(M, q, s, hq, hs, ln)
+        L, li, lj = gapped_extend(M, q[qs::-1], s[ss::-1], xdrop, go, ge)
+        R, ri, rj = gapped_extend(M, q[qs + 1:], s[ss + 1:], xdrop, go, ge)
+        if L + R >= cutoff:
+            out.append((L + R, qs + 1 - li, qs + 1 + ri, ss + 1 - lj, ss + 1 + rj, qs, ss, k))
+    return out
