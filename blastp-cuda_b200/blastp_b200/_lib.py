@@ -61,8 +61,8 @@ class BpServerMetrics(ctypes.Structure):
 
 
 REQ_STATES = {-1: "unknown", 0: "queued", 1: "admitted", 2: "running", 3: "done", 4: "failed"}
-SCHED_DYNAMIC, SCHED_STATIC, SCHED_COSTS = 0, 1, 2
-SCHED_NAMES = {0: "dynamic", 1: "static", 2: "learned"}
+SCHED_DYNAMIC, SCHED_STATIC, SCHED_COSTS, SCHED_COST_ORDER = 0, 1, 2, 3
+SCHED_NAMES = {0: "dynamic", 1: "static", 2: "learned", 3: "learned_order"}
 COST_FEATURES = 24
 
 

@@ -65,6 +65,7 @@ struct bp_batch {
         int64_t max_entries = 0;
         int32_t item_lo = 0, item_hi = 0;      // its items in d_items
         int32_t queue_lo = 0;                  // its queue offsets start at d_queue_off[queue_lo]
+        int32_t order_lo = 0;                  // BP_SCHED_COST_ORDER: its items in cursor order at d_queue_items[order_lo]
         int32_t grid = 0;
         double est = 0;                        // expected word hits, to order the launches
         bool packed = false;                   // its units are packed tables
@@ -151,8 +152,10 @@ bp_status enqueue(bp_batch* b) {
         a.n_queries = b->nq;
         a.items = b->d_items + k.item_lo;
         a.n_items = k.item_hi - k.item_lo;
-        a.queue_off = b->opt.schedule == BP_SCHED_DYNAMIC ? nullptr : b->d_queue_off + k.queue_lo;
+        const bool cursor = b->opt.schedule == BP_SCHED_DYNAMIC || b->opt.schedule == BP_SCHED_COST_ORDER;
+        a.queue_off = cursor ? nullptr : b->d_queue_off + k.queue_lo;
         a.queue_items = b->d_queue_items;
+        a.cursor_order = b->opt.schedule == BP_SCHED_COST_ORDER ? b->d_queue_items + k.order_lo : nullptr;
         a.item_cursor = b->d_counts + 4 + c;
         a.matrix = e->d_matrix;
         a.window = b->queries[0]->p.window;
@@ -372,8 +375,10 @@ bp_status bp_search_batch(bp_engine* e, const bp_db* db, const bp_query* const* 
     bp_batch_options o;
     if (opt) o = *opt;
     else bp_batch_options_default(&o);
-    if (o.schedule == BP_SCHED_COSTS && !o.item_costs)
+    if ((o.schedule == BP_SCHED_COSTS || o.schedule == BP_SCHED_COST_ORDER) && !o.item_costs)
         return bp_set_error(e, BP_ERR_INVALID, "bp_search_batch: cost schedule without item costs");
+    if (o.schedule < BP_SCHED_DYNAMIC || o.schedule > BP_SCHED_COST_ORDER)
+        return bp_set_error(e, BP_ERR_INVALID, "bp_search_batch: unknown schedule");
     int32_t s0 = 0, s1 = 0;
     if (!resolve_range(db, o.subject_first, o.subject_count, &s0, &s1))
         return bp_set_error(e, BP_ERR_INVALID, "bp_search_batch: subject range outside the database");
@@ -529,6 +534,25 @@ bp_status bp_search_batch(bp_engine* e, const bp_db* db, const bp_query* const* 
         k.queue_lo = (int32_t)qoff.size() - 1;
         std::vector<std::vector<int32_t>> qs(k.grid);
         std::vector<double> load(k.grid, 0.0);
+        if (o.schedule == BP_SCHED_COST_ORDER) {
+            // one cursor for the class over its items, longest predicted first
+            // (ties in index order); the CTAs take them dynamically
+            std::vector<int32_t> loc(nk);
+            std::iota(loc.begin(), loc.end(), 0);
+            std::vector<float> cost(nk, 0.f);
+            for (int32_t qi = 0; qi < n_queries; ++qi)
+                for (int32_t c = 0; c < n_chunks; ++c) {
+                    const int32_t pos = item_pos[(size_t)qi * n_chunks + c];
+                    if (pos >= k.item_lo && pos < k.item_hi)
+                        cost[pos - k.item_lo] += std::max(0.f, o.item_costs[(size_t)qi * n_chunks + c]);
+                }
+            std::stable_sort(loc.begin(), loc.end(), [&](int32_t x, int32_t y) { return cost[x] > cost[y]; });
+            k.order_lo = (int32_t)qitems.size();
+            qitems.insert(qitems.end(), loc.begin(), loc.end());
+            qoff.push_back(qoff.back() + nk);
+            b->queue_cost.push_back(0.0);
+            continue;
+        }
         if (o.schedule == BP_SCHED_COSTS) {
             // longest predicted item first, into the least loaded queue; each
             // queue then runs its items in order, query by query, so a CTA
@@ -758,7 +782,8 @@ bp_status bp_batch_predict_costs(bp_engine* e, bp_mlp* model, const float* weigh
 void bp_autotune_options_default(bp_autotune_options* o) {
     memset(o, 0, sizeof(*o));
     o->pack_sizes = nullptr;
-    o->schedules_mask = (1 << BP_SCHED_DYNAMIC) | (1 << BP_SCHED_STATIC) | (1 << BP_SCHED_COSTS);
+    o->schedules_mask = (1 << BP_SCHED_DYNAMIC) | (1 << BP_SCHED_STATIC) | (1 << BP_SCHED_COSTS) |
+                        (1 << BP_SCHED_COST_ORDER);
     o->reps = 2;
 }
 
@@ -798,7 +823,7 @@ bp_status bp_batch_autotune(bp_engine* e, const bp_db* db, const bp_query* const
         bo.max_warps = max_warps;
         bo.subject_first = 0;
         bo.subject_count = sample;
-        if (sched == BP_SCHED_COSTS) {
+        if (sched == BP_SCHED_COSTS || sched == BP_SCHED_COST_ORDER) {
             if (costs_chunk != chunk) {
                 std::vector<int32_t> first;
                 plan_chunks(db, 0, sample, chunk, first);
@@ -850,8 +875,9 @@ bp_status bp_batch_autotune(bp_engine* e, const bp_db* db, const bp_query* const
         }
     // stage 2: the other schedules, then the warp caps, at the best chunk and packing
     const int32_t chunk = best->chunk_residues, pack = best->pack_residues;
-    for (int sched = 0; sched < 3; ++sched) {
-        if (sched == sched0 || !(o.schedules_mask & (1 << sched)) || (sched == BP_SCHED_COSTS && !o.model)) continue;
+    for (int sched = 0; sched <= BP_SCHED_COST_ORDER; ++sched) {
+        const bool needs_model = sched == BP_SCHED_COSTS || sched == BP_SCHED_COST_ORDER;
+        if (sched == sched0 || !(o.schedules_mask & (1 << sched)) || (needs_model && !o.model)) continue;
         bp_status st = trial(chunk, pack, sched, 0);
         if (st != BP_OK) return st;
     }

@@ -211,6 +211,7 @@ struct BatchArgs {
                                   // item indices are relative to `items`
     const int32_t* queue_items;
     uint32_t* item_cursor;        // global cursor when queue_off is null
+    const int32_t* cursor_order;  // when set, the cursor's k-th item is cursor_order[k] (else item k)
     const int8_t* matrix;
     int32_t window;
     int32_t* counters;            // 3 per segment

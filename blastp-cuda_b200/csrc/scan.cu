@@ -1025,7 +1025,7 @@ scan_batch_kernel(BatchArgs b, ScanLayout lay) {
                 if (qpos < qend) it = b.queue_items[qpos++];
             } else {
                 const int k = (int)atomicAdd(b.item_cursor, 1u);
-                if (k < b.n_items) it = k;
+                if (k < b.n_items) it = b.cursor_order ? b.cursor_order[k] : k;
             }
             ctl->item = it;
             ctl->sub_ctr = 0;

@@ -233,7 +233,8 @@ typedef struct bp_batch bp_batch;
 typedef enum {
     BP_SCHED_DYNAMIC = 0,   /* CTAs take items from one global cursor */
     BP_SCHED_STATIC = 1,    /* item i goes to CTA i mod ctas */
-    BP_SCHED_COSTS = 2      /* longest predicted item first into the least loaded CTA */
+    BP_SCHED_COSTS = 2,     /* longest predicted item first into the least loaded CTA */
+    BP_SCHED_COST_ORDER = 3 /* one global cursor over the items, longest predicted first */
 } bp_schedule;
 
 typedef struct {
@@ -242,7 +243,7 @@ typedef struct {
     int32_t ctas;               /* persistent CTAs (0: one per SM) */
     int32_t max_warps;          /* warps per CTA cap (0: as many as shared memory allows) */
     int32_t use_graph;          /* capture the launch sequence once, replay it on bp_batch_run */
-    const float* item_costs;    /* BP_SCHED_COSTS: predicted cost of item q*n_chunks + c */
+    const float* item_costs;    /* BP_SCHED_COSTS, BP_SCHED_COST_ORDER: predicted cost of item q*n_chunks + c */
     int32_t subject_first;      /* subjects [subject_first, subject_first + subject_count) */
     int32_t subject_count;      /* (< 0: to the end of the database) */
     int32_t pack_residues;      /* > 0: queries of at most half this length share tables of up to

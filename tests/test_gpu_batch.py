@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 from blastp_b200 import BpError, default_params, synth
-from blastp_b200._lib import SCHED_COSTS, SCHED_DYNAMIC, SCHED_STATIC
+from blastp_b200._lib import SCHED_COST_ORDER, SCHED_COSTS, SCHED_DYNAMIC, SCHED_STATIC
 from helpers import assert_same, oracle_search
 
 pytestmark = pytest.mark.gpu
@@ -58,14 +58,14 @@ def test_one_query_vs_oracle(engine, matrix, workload):
     b.close()
 
 
-@pytest.mark.parametrize("schedule", [SCHED_DYNAMIC, SCHED_STATIC, SCHED_COSTS])
+@pytest.mark.parametrize("schedule", [SCHED_DYNAMIC, SCHED_STATIC, SCHED_COSTS, SCHED_COST_ORDER])
 @pytest.mark.parametrize("chunk", [1 << 12, 1 << 18, 1 << 30])
 def test_schedules_and_chunks(engine, workload, singles, schedule, chunk):
     qs, db = workload
     d = engine.database(db.residues, db.offsets)
     hs = [engine.query(q) for q in qs]
     costs = None
-    if schedule == SCHED_COSTS:
+    if schedule in (SCHED_COSTS, SCHED_COST_ORDER):
         n_items = len(qs) * (len(engine.plan_chunks(d, chunk)) - 1)
         costs = np.random.default_rng(chunk).random(n_items).astype(np.float32)
     b = engine.search_batch(d, hs, chunk_residues=chunk, schedule=schedule, item_costs=costs)
@@ -178,14 +178,14 @@ def test_autotune_picks_a_measured_candidate(engine, workload, singles):
 
 
 @pytest.mark.parametrize("pack", [256, 2048, 8000])
-@pytest.mark.parametrize("schedule", [SCHED_DYNAMIC, SCHED_COSTS])
+@pytest.mark.parametrize("schedule", [SCHED_DYNAMIC, SCHED_COSTS, SCHED_COST_ORDER])
 def test_packed_tables(engine, workload, singles, pack, schedule):
     # short queries share packed tables; every query's result stays its own
     qs, db = workload
     d = engine.database(db.residues, db.offsets)
     hs = [engine.query(q) for q in qs]
     costs = None
-    if schedule == SCHED_COSTS:
+    if schedule in (SCHED_COSTS, SCHED_COST_ORDER):
         costs = np.random.default_rng(pack).random(len(qs) * (len(engine.plan_chunks(d, 1 << 16)) - 1))
     b = engine.search_batch(d, hs, chunk_residues=1 << 16, schedule=schedule, item_costs=costs,
                             pack_residues=pack)

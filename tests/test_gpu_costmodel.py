@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 from blastp_b200 import Mlp, costmodel, synth
-from blastp_b200._lib import SCHED_COSTS, SCHED_DYNAMIC, SCHED_STATIC
+from blastp_b200._lib import SCHED_COST_ORDER, SCHED_COSTS, SCHED_DYNAMIC, SCHED_STATIC
 from helpers import assert_same
 from mlp_ref import forward, loss_grad
 
@@ -133,7 +133,7 @@ def test_library_costs_match_python_costs(engine, matrix):
     assert np.allclose(lib_costs, py_costs, rtol=1e-4)
     best, trials = engine.autotune(d, hq, model=model, planted_density=0.01, sample_subjects=1000,
                                    chunk_sizes=[1 << 15], warp_caps=[0], reps=1)
-    assert {t["schedule"] for t in trials} == {SCHED_DYNAMIC, SCHED_STATIC, SCHED_COSTS}
+    assert {t["schedule"] for t in trials} == {SCHED_DYNAMIC, SCHED_STATIC, SCHED_COSTS, SCHED_COST_ORDER}
 
 
 def test_cosched_split_from_model(engine, matrix):
@@ -147,3 +147,61 @@ def test_cosched_split_from_model(engine, matrix):
     assert all(0 <= s <= 20_000 for s in splits)
     assert splits == sorted(splits)                 # a slower CPU leaves more to the device
     assert 8_000 <= splits[1] <= 12_000             # equal speeds: about half the residues each
+
+
+def _device_ms(engine, b, reps=5):
+    """Device time of each of `reps` replays of a batch (CUDA events on the
+    engine stream around the replay; results are not read back)."""
+    import torch
+    stream = torch.cuda.ExternalStream(engine.stream)
+    out = []
+    for _ in range(reps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        b.run()
+        e1.record(stream)
+        b.wait()
+        torch.cuda.synchronize()
+        out.append(e0.elapsed_time(e1))
+    return np.array(out)
+
+
+def test_learned_queues_beat_static_on_the_device(engine, matrix):
+    # 32 queries, one item each (a single chunk spans the database), on 8
+    # CTAs: static round robin gives CTA q mod 8 the queries q = 0, 8, 16, 24
+    # -- here the 500-letter ones for q mod 8 in {0, 1}, 200 letters otherwise
+    # (one launch class: both take 32 warps and queue their extensions) -- so
+    # CTAs 0 and 1 scan four long queries each.  The learned queues (costs
+    # predicted by the packaged model through the library, longest first into
+    # the least loaded CTA) give every CTA one long query and three short
+    # ones.  Device time of the whole batched launch, min of 5 replays each,
+    # must improve by more than the run-to-run spread; results stay identical
+    # to the static schedule's.
+    model = costmodel.CostModel.load(engine)
+    rng = np.random.default_rng(91)
+    qs = [synth.residues(rng, 500 if q % 8 in (0, 1) else 200) for q in range(32)]
+    db = synth.make_database(rng, 6000, qs[:2], 0.002, (60, 150), (0.3, 0.5), matrix)
+    d = engine.database(db.residues, db.offsets)
+    hq = [engine.query(q) for q in qs]
+    chunk = 1 << 30
+    first = engine.plan_chunks(d, chunk)
+    assert len(first) - 1 == 1
+    pred = engine.predict_costs(model, d, hq, first, 0.002)
+    assert min(pred[[q for q in range(32) if q % 8 in (0, 1)]]) > max(pred[[q for q in range(32) if q % 8 > 1]])
+    ctas = 8
+    b_static = engine.search_batch(d, hq, chunk_residues=chunk, schedule=SCHED_STATIC, ctas=ctas, pack_residues=0)
+    b_learn = engine.search_batch(d, hq, chunk_residues=chunk, schedule=SCHED_COSTS, ctas=ctas, item_costs=pred,
+                                  pack_residues=0)
+    for b in (b_static, b_learn):
+        b.wait()
+    t_static = _device_ms(engine, b_static)
+    t_learn = _device_ms(engine, b_learn)
+    spread = max(t_static.max() - t_static.min(), t_learn.max() - t_learn.min())
+    assert t_static.min() - t_learn.min() > spread, (t_static.tolist(), t_learn.tolist())
+    for i in range(len(qs)):
+        a, c = b_static.fetch(i), b_learn.fetch(i)
+        assert_same(c, (a.counters, a.hsp_off, a.hsps_as_array()), "learned vs static, query %d" % i)
+    b_static.close()
+    b_learn.close()
