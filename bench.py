@@ -78,6 +78,87 @@ def dist_env():
     return rank, world, local
 
 
+class Ranks:
+    """One process per GPU, as torchrun starts them: the process group, the
+    barriers and the max-over-ranks reduction of the timing.  The GPU path
+    uses NCCL and CUDA tensors; tests drive the same code with gloo on CPU."""
+
+    def __init__(self, backend="nccl", device="cuda", timeout_s=300):
+        import torch
+        self.torch = torch
+        self.rank, self.world, self.local = dist_env()
+        self.device = device
+        if self.world > 1:
+            import datetime
+            torch.distributed.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
+
+    def barrier(self, sync=None):
+        if self.world > 1:
+            self.torch.distributed.barrier()
+        if sync:
+            sync()
+
+    def max(self, x):
+        t = self.torch.tensor([float(x)], dtype=self.torch.float64, device=self.device)
+        if self.world > 1:
+            self.torch.distributed.all_reduce(t, op=self.torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.world > 1:
+            self.torch.distributed.destroy_process_group()
+
+
+class EventTimer:
+    """CUDA events on the stream the work is launched on."""
+
+    def __init__(self, torch, stream):
+        self.stream = stream
+        self.e0 = torch.cuda.Event(enable_timing=True)
+        self.e1 = torch.cuda.Event(enable_timing=True)
+
+    def start(self):
+        self.e0.record(self.stream)
+
+    def mark(self):
+        self.e1.record(self.stream)
+
+    def ms(self):
+        return self.e0.elapsed_time(self.e1)
+
+
+class WallTimer:
+    def start(self):
+        self.t0 = time.perf_counter()
+
+    def mark(self):
+        self.t1 = time.perf_counter()
+
+    def ms(self):
+        return 1e3 * (self.t1 - self.t0)
+
+
+def timed_steps(step, steps, warmup, ranks, timer, sync=None, during=None):
+    """W untimed steps, a barrier, K timed steps between timer.start() and
+    timer.mark(), a barrier (after which the device is idle), then the timed
+    region's length as the max over ranks.  `during` (a context manager)
+    brackets the timed steps (the clock sampler).  Returns (the steps'
+    outputs, max ms, this rank's ms)."""
+    import contextlib
+    for _ in range(warmup):
+        step()
+    ranks.barrier(sync)
+    outs = []
+    with (during or contextlib.nullcontext()):
+        timer.start()
+        for _ in range(steps):
+            outs.append(step())
+        timer.mark()
+        ranks.barrier(sync)
+    local_ms = timer.ms()
+    return outs, ranks.max(local_ms), local_ms
+
+
 def load_workload(matrix, rank, n_subjects, qlen):
     from blastp_b200 import synth
     return synth.shape2(matrix, rep=rank, n_subjects=n_subjects, qlen=qlen)
@@ -568,13 +649,8 @@ def run_reference(args):
 def run_ours(args):
     import torch
     rank, world, local = dist_env()
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    else:
-        torch.cuda.set_device(0)
+    torch.cuda.set_device(local if world > 1 else 0)
+    ranks = Ranks("nccl", device="cuda")
     import blastp_b200 as bp
     matrix = bp.blosum62()
     w = load_workload(matrix, rank, args.subjects, args.qlen)
@@ -583,11 +659,6 @@ def run_ours(args):
     db = eng.database(w.db.residues, w.db.offsets)
     qry = eng.query(q)
     stream = torch.cuda.ExternalStream(eng.stream)
-
-    def barrier():
-        if world > 1:
-            torch.distributed.barrier()
-        torch.cuda.synchronize()
 
     def step():
         r = eng.search(db, qry)
@@ -598,23 +669,11 @@ def run_ours(args):
 
     for _ in range(args.warmup):
         step()
-    barrier()
-    scan_ms = []
+    clk = ClockSampler(local if world > 1 else 0)
     launches0 = eng.launches
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local if world > 1 else 0) as clk:
-        ev0.record(stream)
-        for _ in range(args.steps):
-            scan_ms.append(step())
-        ev1.record(stream)
-        barrier()
+    scan_ms, total_ms, _ = timed_steps(step, args.steps, 0, ranks, EventTimer(torch, stream),
+                                       sync=torch.cuda.synchronize, during=clk)
     launches = eng.launches - launches0
-    total_ms = ev0.elapsed_time(ev1)
-    t = torch.tensor([total_ms], device="cuda")
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    total_ms = float(t.item())
     units = w.db.n_residues * world                # DB residues x queries (one query per step)
     value = units * args.steps / (total_ms / 1e3)
 
@@ -644,17 +703,10 @@ def run_ours(args):
                                        len(w.db.residues), off_pin.data_ptr(), n, cnt_pin.data_ptr(),
                                        hoff_pin.data_ptr(), hsp_pin.data_ptr(), cap, ctypes.byref(nh)), eng.h)
 
-        e2e_step()
-        barrier()
-        t0 = time.perf_counter()
-        for _ in range(args.e2e_steps):
-            e2e_step()
-        barrier()
-        e2e_s = time.perf_counter() - t0
-        t = torch.tensor([e2e_s], device="cuda")
-        if world > 1:
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t.item())
+        # (host buffers in and out every step: timed on the host clock between
+        # barriers that leave the device idle)
+        _, e2e_ms, _ = timed_steps(e2e_step, args.e2e_steps, 1, ranks, WallTimer(), sync=torch.cuda.synchronize)
+        e2e_s = e2e_ms / 1e3
         h2d = len(w.db.residues) + 8 * len(w.db.offsets) + len(q)
         # the host link's own rate for the same bytes (pinned, one copy): the floor
         # of the end-to-end step next to the scan kernel's time
@@ -737,8 +789,7 @@ def run_ours(args):
     qry.close()
     db.close()
     eng.close()
-    if world > 1:
-        torch.distributed.destroy_process_group()
+    ranks.close()
     return 0
 
 
