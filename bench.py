@@ -68,6 +68,10 @@ def parse():
     ap.add_argument("--serve-requests", type=int, default=128)
     ap.add_argument("--serve-rate", type=float, default=1000.0, help="offered load, queries/s (Poisson)")
     ap.add_argument("--serve-check", type=int, default=32, help="served requests checked against plain searches")
+    ap.add_argument("--serve-rate-high", type=float, default=5000.0, help="second offered load (0: skip)")
+    ap.add_argument("--serve-lanes", type=int, default=1)
+    ap.add_argument("--serve-depth", type=int, default=4, help="batches queued per lane")
+    ap.add_argument("--serve-batch", type=int, default=2, help="queries per batch")
     return ap.parse_args()
 
 
@@ -556,17 +560,22 @@ def run_serving(eng, matrix, args):
     load["from_memory_gbs"] = load["gb"] / load["from_memory_s"]
     del res
     model = costmodel.CostModel.load(eng)
+    lanes, depth, max_batch = args.serve_lanes, args.serve_depth, args.serve_batch
     out = {"workload": "serve_vs_5M", "subjects": args.serve_subjects, "residues": nres, "db_load": load,
-           "schedule": "learned", "lanes": 2, "max_batch_queries": 32, "memory_budget_gb": 16}
+           "schedule": "learned", "lanes": lanes, "lane_depth": depth, "max_batch_queries": max_batch,
+           "memory_budget_gb": 16}
     runs = {}
     capacity = None
-    for label, rate, n in (("offered", args.serve_rate, args.serve_requests),
-                           ("sustainable", None, max(16, args.serve_requests // 2))):
+    plan = [("offered", args.serve_rate, args.serve_requests),
+            ("sustainable", None, max(16, args.serve_requests // 2))]
+    if args.serve_rate_high > 0:
+        plan.insert(1, ("offered_high", args.serve_rate_high, args.serve_requests))
+    for label, rate, n in plan:
         if rate is None:
             rate = 0.8 * capacity
         qs = synth.serving_queries(rng, n)
-        srv = Server(eng, db, max_batch_queries=32, lanes=2, schedule=SCHED_COSTS, model=model,
-                     chunk_residues=1 << 20)
+        srv = Server(eng, db, max_batch_queries=max_batch, lanes=lanes, lane_depth=depth, schedule=SCHED_COSTS,
+                     model=model, chunk_residues=1 << 20)
         arrivals = serving.poisson_arrivals(rng, rate, n)
         digests = []
         n_check = min(n, args.serve_check)
@@ -578,10 +587,12 @@ def run_serving(eng, matrix, args):
         srv.close()
         # the served results against plain searches of the same queries alone
         same = 0
+        alone_ms = []
         for q, dg in zip(qs[:n_check], digests):
             h = eng.query(q)
             r = eng.search(db, h)
             same += int(r.digest() == dg)
+            alone_ms.append(eng.last_scan_ms)
             r.close()
             h.close()
         qres = float(sum(len(q) for q in qs))
@@ -594,9 +605,10 @@ def run_serving(eng, matrix, args):
                        "submit_lateness_ms_max": float(late.max()) if len(late) else 0.0,
                        "query_residues": qres,
                        "identical_to_plain": same == n_check, "checked_requests": n_check,
+                       "alone_scan_ms_median": float(np.median(alone_ms)) if alone_ms else None,
                        "check": "served result digest (counters, offsets, HSP records) == the query's plain "
                                 "search alone, first %d requests" % n_check}
-        if capacity is None:
+        if label == "offered":
             capacity = st["queries_per_s"]
     out["runs"] = runs
     out["identical_to_plain"] = all(r["identical_to_plain"] for r in runs.values())

@@ -8,9 +8,14 @@
 //    device-memory budget allows (the request's neighbour table, its
 //    per-subject outputs and its share of the HSP record buffer), builds
 //    their tables and launches them as one batched persistent search on a
-//    free lane -- each lane has its own stream and engine scratch, and each
-//    lane's launch takes 1/lanes of the SMs, so a batch that starts while
-//    another is running overlaps it on the device;
+//    lane -- each lane's launch takes 1/lanes of the SMs, so a batch that
+//    starts while another lane's is running overlaps it on the device;
+//  * a lane holds up to lane_depth batches, each in a slot with its own
+//    engine (stream and scratch): the slot's stream waits for the lane's
+//    previous batch (an event), so a lane runs its batches back to back in
+//    admission order while the host builds the next batch's tables and
+//    launches it behind them -- a request admitted while its lane is busy
+//    waits for the batches ahead of it, not for a batch boundary;
 //  * finished batches are noticed by polling their streams; results stay on
 //    the device, in the batch's per-query segments, until the request is
 //    released, which is when its memory returns to the budget.
@@ -55,6 +60,7 @@ struct Req {
 
 struct Job {
     int lane = 0;
+    int slot = 0;             // lane * lane_depth + position
     bp_batch* batch = nullptr;
     std::vector<Req*> reqs;
     int live = 0;             // requests not yet released
@@ -68,8 +74,11 @@ struct bp_server {
     bp_engine* e = nullptr;
     const bp_db* db = nullptr;
     bp_server_options o{};
-    std::vector<bp_engine*> lanes;
-    std::vector<Job*> lane_job;
+    int n_lanes = 0, depth = 1;
+    std::vector<bp_engine*> slots;        // lane l's slots are l * depth .. l * depth + depth - 1
+    std::vector<Job*> slot_job;
+    std::vector<cudaEvent_t> lane_tail;   // recorded after the lane's latest batch
+    std::vector<bool> lane_used;          // lane_tail has been recorded
     std::thread th;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
@@ -108,7 +117,7 @@ void fail_request(bp_server* s, Req* r, bp_status st) {
 // Builds tables and launches one batch on `lane` (called without the lock;
 // the requests are already marked admitted and owned by the dispatcher).
 void launch_job(bp_server* s, Job* job) {
-    bp_engine* le = s->lanes[job->lane];
+    bp_engine* le = s->slots[job->slot];
     std::vector<const bp_query*> qs;
     bp_status st = BP_OK;
     for (Req* r : job->reqs) {
@@ -121,7 +130,7 @@ void launch_job(bp_server* s, Job* job) {
     bo.chunk_residues = s->o.chunk_residues > 0 ? s->o.chunk_residues : (1 << 20);
     bo.schedule = s->o.schedule;
     bo.use_graph = 0;
-    bo.ctas = std::max(1, le->sm_count / std::max(1, (int)s->lanes.size()));
+    bo.ctas = std::max(1, le->sm_count / std::max(1, s->n_lanes));
     std::vector<float> costs;
     if (st == BP_OK && bo.schedule == BP_SCHED_COSTS) {
         if (!s->o.model) {
@@ -138,7 +147,21 @@ void launch_job(bp_server* s, Job* job) {
             bo.item_costs = costs.data();
         }
     }
+    // behind the lane's previous batch on the device, then this one becomes the lane's tail
+    if (st == BP_OK && s->lane_used[job->lane] &&
+        cudaStreamWaitEvent(le->stream, s->lane_tail[job->lane], 0) != cudaSuccess) {
+        cudaGetLastError();
+        st = BP_ERR_CUDA;
+    }
     if (st == BP_OK) st = bp_search_batch(le, s->db, qs.data(), (int32_t)qs.size(), &bo, &job->batch);
+    if (st == BP_OK) {
+        if (cudaEventRecord(s->lane_tail[job->lane], le->stream) == cudaSuccess) {
+            s->lane_used[job->lane] = true;
+        } else {
+            cudaGetLastError();
+            st = BP_ERR_CUDA;
+        }
+    }
     std::lock_guard<std::mutex> lock(s->mu);
     const double t = now_ms();
     for (size_t i = 0; i < job->reqs.size(); ++i) {
@@ -174,12 +197,12 @@ void dispatcher(bp_server* s) {
     std::unique_lock<std::mutex> lock(s->mu);
     while (!s->stop) {
         bool worked = false;
-        // completions
-        for (size_t l = 0; l < s->lanes.size(); ++l) {
-            Job* job = s->lane_job[l];
+        // completions (a slot's stream holds its own batch only)
+        for (size_t l = 0; l < s->slots.size(); ++l) {
+            Job* job = s->slot_job[l];
             if (!job) continue;
             if (!job->done) {
-                if (cudaStreamQuery(s->lanes[l]->stream) == cudaErrorNotReady) continue;
+                if (cudaStreamQuery(s->slots[l]->stream) == cudaErrorNotReady) continue;
                 cudaGetLastError();
                 lock.unlock();
                 const bp_status st = bp_batch_wait(job->batch);   // re-runs on record overflow
@@ -203,14 +226,19 @@ void dispatcher(bp_server* s) {
                 s->cv_done.notify_all();
                 worked = true;
             }
-            s->lane_job[l] = nullptr;   // the lane is free; the job lives until released
+            s->slot_job[l] = nullptr;   // the slot is free; the job lives until released
             if (job->live == 0) retire_job(s, job);
         }
-        // admissions: one batch per free lane, in arrival order, within budget
-        for (size_t l = 0; l < s->lanes.size() && !s->pending.empty(); ++l) {
-            if (s->lane_job[l]) continue;
+        // admissions: one batch per free slot, lanes in turn, in arrival order, within budget
+        for (int pass = 0; pass < s->depth && !s->pending.empty(); ++pass)
+        for (size_t l = 0; l < (size_t)s->n_lanes && !s->pending.empty(); ++l) {
+            int slot = -1;
+            for (int k = 0; k < s->depth && slot < 0; ++k)
+                if (!s->slot_job[l * s->depth + k]) slot = (int)l * s->depth + k;
+            if (slot < 0) continue;
             Job* job = new Job();
             job->lane = (int)l;
+            job->slot = slot;
             while (!s->pending.empty() && (int)job->reqs.size() < s->o.max_batch_queries) {
                 Req* r = s->pending.front();
                 if (s->mem_used + job->bytes + r->bytes > s->o.device_memory_budget && !(job->reqs.empty() &&
@@ -229,7 +257,7 @@ void dispatcher(bp_server* s) {
             job->live = (int)job->reqs.size();
             s->mem_used += job->bytes;
             s->mem_peak = std::max(s->mem_peak, s->mem_used);
-            s->lane_job[l] = job;
+            s->slot_job[slot] = job;
             s->n_batches += 1;
             s->batched_queries += (int64_t)job->reqs.size();
             s->in_flight += (int)job->reqs.size();
@@ -239,7 +267,7 @@ void dispatcher(bp_server* s) {
             lock.lock();
             if (job->done) {                 // failed to launch
                 s->in_flight -= (int)job->reqs.size();
-                s->lane_job[l] = nullptr;
+                s->slot_job[slot] = nullptr;
             }
             worked = true;
         }
@@ -258,6 +286,7 @@ void bp_server_options_default(bp_server_options* o) {
     o->chunk_residues = 1 << 20;
     o->schedule = BP_SCHED_DYNAMIC;
     o->lanes = 2;
+    o->lane_depth = 1;
     o->poll_us = 200;
     bp_params_default(&o->params);
 }
@@ -270,19 +299,33 @@ bp_status bp_server_create(bp_engine* e, const bp_db* db, const bp_server_option
     s->db = db;
     if (opt) s->o = *opt;
     else bp_server_options_default(&s->o);
-    if (s->o.lanes < 1 || s->o.lanes > 16 || s->o.max_batch_queries < 1) {
+    if (s->o.lanes < 1 || s->o.lanes > 16 || s->o.max_batch_queries < 1 || s->o.lane_depth < 1 ||
+        s->o.lane_depth > 16) {
         delete s;
-        return bp_set_error(e, BP_ERR_INVALID, "bp_server_create: lanes must be 1..16, max_batch_queries >= 1");
+        return bp_set_error(e, BP_ERR_INVALID,
+                            "bp_server_create: lanes and lane_depth must be 1..16, max_batch_queries >= 1");
     }
-    for (int l = 0; l < s->o.lanes; ++l) {
+    s->n_lanes = s->o.lanes;
+    s->depth = s->o.lane_depth;
+    for (int l = 0; l < s->n_lanes; ++l) {
+        cudaEvent_t ev = nullptr;
+        if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            bp_server_destroy(s);
+            return bp_set_error(e, BP_ERR_CUDA, "bp_server_create: lane event");
+        }
+        s->lane_tail.push_back(ev);
+        s->lane_used.push_back(false);
+    }
+    for (int k = 0; k < s->n_lanes * s->depth; ++k) {
         bp_engine* le = nullptr;
         const bp_status st = bp_engine_create(e->device, &le);
         if (st != BP_OK) {
             bp_server_destroy(s);
-            return bp_set_error(e, st, "bp_server_create: lane engine");
+            return bp_set_error(e, st, "bp_server_create: slot engine");
         }
-        s->lanes.push_back(le);
-        s->lane_job.push_back(nullptr);
+        s->slots.push_back(le);
+        s->slot_job.push_back(nullptr);
     }
     s->th = std::thread(dispatcher, s);
     *out = s;
@@ -382,7 +425,7 @@ bp_status bp_server_release(bp_server* s, uint64_t ticket) {
         return BP_OK;
     }
     job->live -= 1;
-    const bool on_lane = std::find(s->lane_job.begin(), s->lane_job.end(), job) != s->lane_job.end();
+    const bool on_lane = std::find(s->slot_job.begin(), s->slot_job.end(), job) != s->slot_job.end();
     if (job->live == 0 && job->done && !on_lane) retire_job(s, job);
     s->cv_work.notify_one();
     return BP_OK;
@@ -440,7 +483,8 @@ void bp_server_destroy(bp_server* s) {
         delete j;
     }
     for (auto& kv : s->reqs) delete kv.second;
-    for (bp_engine* le : s->lanes) bp_engine_destroy(le);
+    for (bp_engine* le : s->slots) bp_engine_destroy(le);
+    for (cudaEvent_t ev : s->lane_tail) cudaEventDestroy(ev);
     delete s;
 }
 

@@ -391,6 +391,9 @@ typedef struct {
     float cost_weights[3];
     float planted_density;
     bp_params params;
+    int32_t lane_depth;             /* batches queued per lane (>= 1): a lane runs its batches one
+                                       after the other on the device, in admission order, while the
+                                       next ones are prepared and launched behind them */
 } bp_server_options;
 
 typedef struct {

@@ -108,3 +108,26 @@ def test_served_digests_equal_plain(engine, world):
         h.close()
         srv.release(t)
     srv.close()
+
+
+def test_lane_depth_runs_batches_back_to_back_in_order(engine, world):
+    # one lane holding up to three batches of one query each: requests
+    # submitted together complete in submission order (the lane's batches run
+    # one after the other on the device), more than one batch is in flight on
+    # the lane, and every result equals the query searched alone
+    qs, db, d, alone = world
+    srv = Server(engine, d, max_batch_queries=1, lanes=1, lane_depth=3, chunk_residues=1 << 18)
+    tickets = [srv.submit(q) for q in qs[:12]]
+    lat = []
+    for i, t in enumerate(tickets):
+        srv.wait(t)
+        r, ms = srv.result(t)
+        a = alone[i]
+        assert_same(r, (a.counters, a.hsp_off, a.hsps_as_array()), "depth-3 lane, request %d" % i)
+        lat.append(ms)
+        srv.release(t)
+    st = srv.stats()
+    srv.close()
+    assert st["completed"] == 12 and st["max_in_flight"] >= 2
+    # arrivals were microseconds apart: completion order shows in the latencies
+    assert all(lat[i] <= lat[i + 1] + 0.5 for i in range(len(lat) - 1)), lat
