@@ -169,27 +169,27 @@ def _device_ms(engine, b, reps=5):
 
 
 def test_learned_queues_beat_static_on_the_device(engine, matrix):
-    # 32 queries, one item each (a single chunk spans the database), on 8
-    # CTAs: static round robin gives CTA q mod 8 the queries q = 0, 8, 16, 24
-    # -- here the 500-letter ones for q mod 8 in {0, 1}, 200 letters otherwise
-    # (one launch class: both take 32 warps and queue their extensions) -- so
-    # CTAs 0 and 1 scan four long queries each.  The learned queues (costs
-    # predicted by the packaged model through the library, longest first into
-    # the least loaded CTA) give every CTA one long query and three short
-    # ones.  Device time of the whole batched launch, min of 5 replays each,
-    # must improve by more than the run-to-run spread; results stay identical
-    # to the static schedule's.
+    # Nine queries, one item each (a single chunk spans the database), on 8
+    # CTAs, in one launch class (500 and 200 letters both take 32 warps and
+    # queue their extensions), whose items are ordered longest first.  Round
+    # robin gives CTA 0 items 0 and 8: the 500-letter query and a 200-letter
+    # one, one after the other, while CTAs 1-7 scan one short query each.  The
+    # learned queues (costs predicted by the packaged model through the
+    # library, longest first into the least loaded CTA) put item 8 beside a
+    # short one.  Device time of the whole batched launch, min of 5 replays
+    # each, must improve by more than the run-to-run spread; results stay
+    # identical to the static schedule's.
     model = costmodel.CostModel.load(engine)
     rng = np.random.default_rng(91)
-    qs = [synth.residues(rng, 500 if q % 8 in (0, 1) else 200) for q in range(32)]
-    db = synth.make_database(rng, 6000, qs[:2], 0.002, (60, 150), (0.3, 0.5), matrix)
+    qs = [synth.residues(rng, 500)] + [synth.residues(rng, 200) for _ in range(8)]
+    db = synth.make_database(rng, 40_000, qs[:1], 0.001, (60, 150), (0.3, 0.5), matrix)
     d = engine.database(db.residues, db.offsets)
     hq = [engine.query(q) for q in qs]
     chunk = 1 << 30
     first = engine.plan_chunks(d, chunk)
     assert len(first) - 1 == 1
-    pred = engine.predict_costs(model, d, hq, first, 0.002)
-    assert min(pred[[q for q in range(32) if q % 8 in (0, 1)]]) > max(pred[[q for q in range(32) if q % 8 > 1]])
+    pred = engine.predict_costs(model, d, hq, first, 0.001)
+    assert pred[0] > pred[1:].max()
     ctas = 8
     b_static = engine.search_batch(d, hq, chunk_residues=chunk, schedule=SCHED_STATIC, ctas=ctas, pack_residues=0)
     b_learn = engine.search_batch(d, hq, chunk_residues=chunk, schedule=SCHED_COSTS, ctas=ctas, item_costs=pred,
