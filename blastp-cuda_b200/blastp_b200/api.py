@@ -183,7 +183,7 @@ class Engine:
         return out
 
     def autotune(self, db: "Database", queries, model=None, planted_density: float = 0.0, sample_subjects: int = 0,
-                 chunk_sizes=None, warp_caps=None, schedules=(0, 1, 2), reps: int = 2, pack_sizes=None):
+                 chunk_sizes=None, warp_caps=None, schedules=(0, 1, 2, 3), reps: int = 2, pack_sizes=None):
         """Times candidate batch configurations on a sample of the subjects
         (bp_batch_autotune); returns (best options dict, list of trials)."""
         o = BpAutotuneOptions()

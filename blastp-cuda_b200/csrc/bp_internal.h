@@ -88,6 +88,12 @@ struct bp_db {
     std::vector<int32_t> h_long;
     int32_t* d_long = nullptr;
     int32_t long_min = 0;
+    // chunk composition histograms of the last chunk plan asked for (the
+    // residues never change, so a plan's histograms are computed once; a
+    // server asks for the same plan on every batch)
+    std::mutex hist_mu;
+    std::vector<int32_t> hist_first;
+    std::vector<uint32_t> hist;
 };
 
 struct bp_query {

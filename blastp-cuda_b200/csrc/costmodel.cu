@@ -460,6 +460,15 @@ bp_status bp_db_chunk_histograms(bp_engine* e, const bp_db* db, const int32_t* c
         if (chunk_first[c] < 0 || chunk_first[c] > chunk_first[c + 1] || chunk_first[c + 1] > db->n)
             return bp_set_error(e, BP_ERR_INVALID, "bp_db_chunk_histograms: bad chunk boundaries");
     if (n_chunks == 0) return BP_OK;
+    bp_db* mdb = const_cast<bp_db*>(db);
+    {
+        std::lock_guard<std::mutex> lock(mdb->hist_mu);
+        if (mdb->hist_first.size() == (size_t)n_chunks + 1 &&
+            std::equal(mdb->hist_first.begin(), mdb->hist_first.end(), chunk_first)) {
+            memcpy(counts, mdb->hist.data(), (size_t)n_chunks * 28 * sizeof(uint32_t));
+            return BP_OK;
+        }
+    }
     CKM(cudaSetDevice(e->device), "cudaSetDevice");
     int32_t* d_first = nullptr;
     uint32_t* d_counts = nullptr;
@@ -478,6 +487,9 @@ bp_status bp_db_chunk_histograms(bp_engine* e, const bp_db* db, const int32_t* c
     cudaFreeAsync(d_first, e->stream);
     cudaFreeAsync(d_counts, e->stream);
     CKM(cudaStreamSynchronize(e->stream), "histograms");
+    std::lock_guard<std::mutex> lock(mdb->hist_mu);
+    mdb->hist_first.assign(chunk_first, chunk_first + n_chunks + 1);
+    mdb->hist.assign(counts, counts + (size_t)n_chunks * 28);
     return BP_OK;
 }
 
