@@ -433,18 +433,55 @@ bp_status bp_gapped_run_ring(bp_result* r, const bp_gapped_params* p, int32_t ri
     CKG(cudaMalloc((void**)&d_rings, (size_t)grid * kWarps * ring_columns * sizeof(int2)), "cudaMalloc(rings)");
     scratch.push_back(d_rings);
     g.rings = d_rings;
-    cudaEvent_t t0, t1;
-    cudaEventCreate(&t0);
-    cudaEventCreate(&t1);
-    cudaEventRecord(t0, cs);
+    // the reports never outnumber the ungapped HSPs: the output is sized once
+    CKG(cudaMalloc((void**)&gp->d_hsps, nu * sizeof(bp_gapped_hsp)), "cudaMalloc(gapped hsps)");
+    // kernel, offsets and gather enqueued back to back; one read-back at the
+    // end says whether any subject needs the wide-ring launch (then the
+    // offsets and gather run again behind it)
+    auto finish = [&]() -> cudaError_t {
+        cudaError_t err = bp_launch_offsets(e, cs, n, gp->d_counters, gp->d_off, d_fill, d_sums);
+        if (err == cudaSuccess && n > 0) {
+            gather_gapped<<<e->sm_count * 4, 256, 0, cs>>>(n, r->d_hsp_off, gp->d_counters, gp->d_off, d_staging,
+                                                          gp->d_hsps);
+            e->launches += 1;
+            err = cudaGetLastError();
+        }
+        return err;
+    };
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    CKG(cudaEventCreate(&t0), "cudaEventCreate");
+    CKG(cudaEventCreate(&t1), "cudaEventCreate");
+    struct Events {
+        cudaEvent_t& a;
+        cudaEvent_t& b;
+        ~Events() {
+            if (a) cudaEventDestroy(a);
+            if (b) cudaEventDestroy(b);
+        }
+    } events{t0, t1};
+    uint32_t* h_words = bp_pinned_get(e);
+    if (!h_words) {
+        bp_gapped_destroy(gp);
+        for (void* q : scratch) cudaFree(q);
+        return bp_set_error(e, BP_ERR_NOMEM, "bp_gapped_run: pinned read-back slot");
+    }
+    struct Slot {
+        bp_engine* e;
+        uint32_t* p;
+        ~Slot() { bp_pinned_put(e, p); }
+    } slot{e, h_words};
+    CKG(cudaEventRecord(t0, cs), "cudaEventRecord");
     if (n > 0) {
         gapped_kernel<<<grid, kWarps * 32, 0, cs>>>(g);
         e->launches += 1;
         CKG(cudaGetLastError(), "gapped kernel launch");
     }
-    uint32_t n_over = 0;
-    CKG(cudaMemcpyAsync(&n_over, d_words + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, cs), "read overflow count");
-    CKG(cudaStreamSynchronize(cs), "gapped kernel");
+    CKG(finish(), "gapped offsets and gather");
+    CKG(cudaEventRecord(t1, cs), "cudaEventRecord");
+    CKG(cudaMemcpyAsync(h_words, d_words, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, cs), "read overflow count");
+    CKG(cudaStreamSynchronize(cs), "gapped stage");
+    cudaEventElapsedTime(&gp->ms, t0, t1);
+    const uint32_t n_over = h_words[1];
     if (n_over > 0) {
         // subjects whose band outgrew the ring: again, one warp each, with a
         // ring as wide as the longest of them
@@ -471,29 +508,18 @@ bp_status bp_gapped_run_ring(bp_result* r, const bp_gapped_params* p, int32_t ri
         g2.rings = d_rings2;
         g2.only = d_over;
         g2.n_only = (int32_t)n_over;
+        CKG(cudaEventRecord(t0, cs), "cudaEventRecord");
         gapped_kernel<<<grid2, kWarps * 32, 0, cs>>>(g2);
         e->launches += 1;
         CKG(cudaGetLastError(), "gapped kernel launch (wide rings)");
+        CKG(finish(), "gapped offsets and gather");
+        CKG(cudaEventRecord(t1, cs), "cudaEventRecord");
+        CKG(cudaStreamSynchronize(cs), "gapped stage (wide rings)");
+        float ms2 = 0.f;
+        cudaEventElapsedTime(&ms2, t0, t1);
+        gp->ms += ms2;
     }
-    // dense CSR of the reports: offsets from the per-subject counts, then a gather
-    CKG(bp_launch_offsets(e, cs, n, gp->d_counters, gp->d_off, d_fill, d_sums), "gapped offsets");
-    int64_t total = 0;
-    CKG(cudaMemcpyAsync(&total, gp->d_off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, cs), "read gapped count");
-    CKG(cudaStreamSynchronize(cs), "gapped offsets");
-    gp->n_hsps = total;
-    CKG(cudaMalloc((void**)&gp->d_hsps, (size_t)std::max<int64_t>(total, 1) * sizeof(bp_gapped_hsp)),
-        "cudaMalloc(gapped hsps)");
-    if (n > 0) {
-        gather_gapped<<<e->sm_count * 4, 256, 0, cs>>>(n, r->d_hsp_off, gp->d_counters, gp->d_off, d_staging,
-                                                      gp->d_hsps);
-        e->launches += 1;
-        CKG(cudaGetLastError(), "gapped gather launch");
-    }
-    cudaEventRecord(t1, cs);
-    CKG(cudaStreamSynchronize(cs), "gapped gather");
-    cudaEventElapsedTime(&gp->ms, t0, t1);
-    cudaEventDestroy(t0);
-    cudaEventDestroy(t1);
+    CKG(cudaMemcpy(&gp->n_hsps, gp->d_off + n, sizeof(int64_t), cudaMemcpyDeviceToHost), "read gapped count");
     for (void* q : scratch) cudaFree(q);
     *out = gp;
     return BP_OK;
