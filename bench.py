@@ -71,7 +71,9 @@ def parse():
     ap.add_argument("--serve-rate-high", type=float, default=5000.0, help="second offered load (0: skip)")
     ap.add_argument("--serve-lanes", type=int, default=1)
     ap.add_argument("--serve-depth", type=int, default=4, help="batches queued per lane")
-    ap.add_argument("--serve-batch", type=int, default=2, help="queries per batch")
+    ap.add_argument("--serve-batch", type=int, default=1, help="queries per batch")
+    ap.add_argument("--serve-schedule", default="dynamic", choices=["dynamic", "learned"],
+                    help="item schedule of the served batches")
     return ap.parse_args()
 
 
@@ -527,11 +529,12 @@ def run_batched(eng, matrix, args, torch):
 
 def run_serving(eng, matrix, args):
     """Poisson arrivals of log-normal queries (median 350, sigma 0.7, 20-4000
-    aa) against a resident 5,000,000-subject database, served with continuous
-    batching and the learned schedule; p50/p99 latency and throughput at the
-    offered rate and at 80 % of the measured capacity."""
+    aa) against a resident 5,000,000-subject database, served by one lane of
+    queued batches (first come, first served at full width; the dynamic item
+    schedule unless --serve-schedule learned); p50/p99 latency and throughput
+    at the offered rates and at 80 % of the measured capacity."""
     from blastp_b200 import Server, costmodel, serving, synth
-    from blastp_b200._lib import SCHED_COSTS
+    from blastp_b200._lib import SCHED_COSTS, SCHED_DYNAMIC
     rng = np.random.default_rng(5000)
     lengths = synth.lognormal_lengths(rng, args.serve_subjects, 300, 0.6, 30, 5000)
     off = np.zeros(args.serve_subjects + 1, dtype=np.int64)
@@ -561,8 +564,9 @@ def run_serving(eng, matrix, args):
     del res
     model = costmodel.CostModel.load(eng)
     lanes, depth, max_batch = args.serve_lanes, args.serve_depth, args.serve_batch
+    sched = SCHED_COSTS if args.serve_schedule == "learned" else SCHED_DYNAMIC
     out = {"workload": "serve_vs_5M", "subjects": args.serve_subjects, "residues": nres, "db_load": load,
-           "schedule": "learned", "lanes": lanes, "lane_depth": depth, "max_batch_queries": max_batch,
+           "schedule": args.serve_schedule, "lanes": lanes, "lane_depth": depth, "max_batch_queries": max_batch,
            "memory_budget_gb": 16}
     runs = {}
     capacity = None
@@ -574,7 +578,7 @@ def run_serving(eng, matrix, args):
         if rate is None:
             rate = 0.8 * capacity
         qs = synth.serving_queries(rng, n)
-        srv = Server(eng, db, max_batch_queries=max_batch, lanes=lanes, lane_depth=depth, schedule=SCHED_COSTS,
+        srv = Server(eng, db, max_batch_queries=max_batch, lanes=lanes, lane_depth=depth, schedule=sched,
                      model=model, chunk_residues=1 << 20)
         arrivals = serving.poisson_arrivals(rng, rate, n)
         digests = []

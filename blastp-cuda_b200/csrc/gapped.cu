@@ -112,6 +112,10 @@ __device__ ExtResult extend(const GappedArgs& g, const int8_t* m, const uint8_t*
         int32_t carry_e = kNeg, carry_diag = kNeg;
         int32_t lmax = kNeg, lmax_j = 0x7fffffff;      // this lane's best cell of the row
         int32_t end = -1;
+        // this lane's cells of the row's first block and of its last two
+        // blocks (kNeg where not computed), for the live-range search below
+        int32_t h_first = kNeg, h_last = kNeg, h_prev = kNeg;
+        int32_t b_last = lo;
         for (int32_t b0 = lo;; b0 += 32) {
             if (b0 + 32 > lo + g.ring) {                // the row would wrap onto itself
                 r.over = true;
@@ -145,6 +149,11 @@ __device__ ExtResult extend(const GappedArgs& g, const int8_t* m, const uint8_t*
             const unsigned sm = __ballot_sync(kFull, stop);
             const int first_stop = sm ? __ffs(sm) - 1 : 32;
             const int32_t h = max(t, e);
+            const int32_t hk = lane < first_stop ? h : kNeg;
+            if (b0 == lo) h_first = hk;
+            h_prev = h_last;
+            h_last = hk;
+            b_last = b0;
             if (lane < first_stop) {
                 ring[j & mask] = make_int2(h, f);
                 if (h > lmax) {
@@ -172,8 +181,14 @@ __device__ ExtResult extend(const GappedArgs& g, const int8_t* m, const uint8_t*
         }
         // live range of the row: first and last column >= best - xdrop
         const int32_t floor_now = best - xdrop;
+        // (blocks held in registers answer without the ring: the first block
+        // for the first live column, the last two for the last one)
         int32_t first_live = -1;
-        for (int32_t b0 = lo; b0 < end && first_live < 0; b0 += 32) {
+        {
+            const unsigned lm = __ballot_sync(kFull, h_first >= floor_now);
+            if (lm) first_live = lo + __ffs(lm) - 1;
+        }
+        for (int32_t b0 = lo + 32; b0 < end && first_live < 0; b0 += 32) {
             const int32_t j = b0 + lane;
             const bool live = j < end && ring[j & mask].x >= floor_now;
             const unsigned lm = __ballot_sync(kFull, live);
@@ -181,7 +196,15 @@ __device__ ExtResult extend(const GappedArgs& g, const int8_t* m, const uint8_t*
         }
         if (first_live < 0) break;
         int32_t last_live = -1;
-        for (int32_t b1 = end; last_live < 0; b1 -= 32) {
+        {
+            const unsigned lm = __ballot_sync(kFull, h_last >= floor_now);
+            if (lm) last_live = b_last + (31 - __clz(lm));
+        }
+        if (last_live < 0 && b_last > lo) {
+            const unsigned lm = __ballot_sync(kFull, h_prev >= floor_now);
+            if (lm) last_live = b_last - 32 + (31 - __clz(lm));
+        }
+        for (int32_t b1 = b_last - 32; last_live < 0; b1 -= 32) {
             const int32_t j = b1 - 32 + lane;
             const bool live = j >= first_live && j < end && ring[j & mask].x >= floor_now;
             const unsigned lm = __ballot_sync(kFull, live);
