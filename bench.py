@@ -407,7 +407,7 @@ def run_batched(eng, matrix, args, torch):
     persistent launch under each schedule, the autotuned configuration, and
     the learned schedule; device time with CUDA events on the engine stream."""
     from blastp_b200 import costmodel, synth
-    from blastp_b200._lib import SCHED_COSTS, SCHED_DYNAMIC, SCHED_NAMES, SCHED_STATIC
+    from blastp_b200._lib import SCHED_COST_ORDER, SCHED_COSTS, SCHED_DYNAMIC, SCHED_NAMES, SCHED_STATIC
     w = synth.shape3(matrix, n_subjects=args.batch_subjects, n_queries=args.batch_queries)
     db = eng.database(w.db.residues, w.db.offsets)
     qs = [eng.query(q) for q in w.queries]
@@ -451,7 +451,8 @@ def run_batched(eng, matrix, args, torch):
     variants = {"unpacked_dynamic": dict(chunk_residues=1 << 20, schedule=SCHED_DYNAMIC, pack_residues=0),
                 "static": dict(chunk_residues=1 << 20, schedule=SCHED_STATIC),
                 "dynamic": dict(chunk_residues=1 << 20, schedule=SCHED_DYNAMIC),
-                "learned": dict(chunk_residues=1 << 20, schedule=SCHED_COSTS)}
+                "learned": dict(chunk_residues=1 << 20, schedule=SCHED_COSTS),
+                "learned_order": dict(chunk_residues=1 << 20, schedule=SCHED_COST_ORDER)}
     if args.batch_autotune:
         t0 = time.perf_counter()
         best, trials = eng.autotune(db, qs, model=model, planted_density=planted,
@@ -466,7 +467,7 @@ def run_batched(eng, matrix, args, torch):
     identical_all = True
     res = {}
     for name, kw in variants.items():
-        if kw["schedule"] == SCHED_COSTS:
+        if kw["schedule"] in (SCHED_COSTS, SCHED_COST_ORDER):
             first = eng.plan_chunks(db, kw["chunk_residues"])
             kw["item_costs"] = eng.predict_costs(model, db, qs, first, planted)
         b = eng.search_batch(db, qs, **kw)
