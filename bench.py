@@ -572,7 +572,8 @@ def run_serving(eng, matrix, args):
     runs = {}
     capacity = None
     plan = [("offered", args.serve_rate, args.serve_requests),
-            ("sustainable", None, max(16, args.serve_requests // 2))]
+            ("sustainable", None, max(16, args.serve_requests // 2)),
+            ("sustainable_shortest_first", None, max(16, args.serve_requests // 2))]
     if args.serve_rate_high > 0:
         plan.insert(1, ("offered_high", args.serve_rate_high, args.serve_requests))
     for label, rate, n in plan:
@@ -580,7 +581,7 @@ def run_serving(eng, matrix, args):
             rate = 0.8 * capacity
         qs = synth.serving_queries(rng, n)
         srv = Server(eng, db, max_batch_queries=max_batch, lanes=lanes, lane_depth=depth, schedule=sched,
-                     model=model, chunk_residues=1 << 20)
+                     model=model, chunk_residues=1 << 20, admission=1 if label.endswith("shortest_first") else 0)
         arrivals = serving.poisson_arrivals(rng, rate, n)
         digests = []
         n_check = min(n, args.serve_check)

@@ -51,7 +51,7 @@ class BpServerOptions(ctypes.Structure):
     _fields_ = [("max_batch_queries", i32), ("device_memory_budget", i64), ("chunk_residues", i32),
                 ("schedule", i32), ("lanes", i32), ("poll_us", i32), ("model", P),
                 ("cost_weights", ctypes.c_float * 3), ("planted_density", ctypes.c_float), ("params", BpParams),
-                ("lane_depth", i32)]
+                ("lane_depth", i32), ("admission", i32)]
 
 
 class BpServerMetrics(ctypes.Structure):
@@ -63,6 +63,7 @@ class BpServerMetrics(ctypes.Structure):
 
 REQ_STATES = {-1: "unknown", 0: "queued", 1: "admitted", 2: "running", 3: "done", 4: "failed"}
 SCHED_DYNAMIC, SCHED_STATIC, SCHED_COSTS, SCHED_COST_ORDER = 0, 1, 2, 3
+ADMIT_ARRIVAL, ADMIT_SHORTEST = 0, 1
 SCHED_NAMES = {0: "dynamic", 1: "static", 2: "learned", 3: "learned_order"}
 COST_FEATURES = 24
 

@@ -240,11 +240,16 @@ void dispatcher(bp_server* s) {
             job->lane = (int)l;
             job->slot = slot;
             while (!s->pending.empty() && (int)job->reqs.size() < s->o.max_batch_queries) {
-                Req* r = s->pending.front();
+                // arrival order, or the shortest query waiting (earliest among equals)
+                auto pick = s->pending.begin();
+                if (s->o.admission == BP_ADMIT_SHORTEST)
+                    for (auto it = s->pending.begin(); it != s->pending.end(); ++it)
+                        if ((*it)->residues.size() < (*pick)->residues.size()) pick = it;
+                Req* r = *pick;
                 if (s->mem_used + job->bytes + r->bytes > s->o.device_memory_budget && !(job->reqs.empty() &&
                                                                                           s->mem_used == 0))
                     break;   // wait for memory (a lone request on an idle server always goes)
-                s->pending.pop_front();
+                s->pending.erase(pick);
                 r->state = BP_REQ_ADMITTED;
                 r->job = job;
                 job->reqs.push_back(r);
@@ -287,6 +292,7 @@ void bp_server_options_default(bp_server_options* o) {
     o->schedule = BP_SCHED_DYNAMIC;
     o->lanes = 2;
     o->lane_depth = 1;
+    o->admission = BP_ADMIT_ARRIVAL;
     o->poll_us = 200;
     bp_params_default(&o->params);
 }
@@ -300,7 +306,7 @@ bp_status bp_server_create(bp_engine* e, const bp_db* db, const bp_server_option
     if (opt) s->o = *opt;
     else bp_server_options_default(&s->o);
     if (s->o.lanes < 1 || s->o.lanes > 16 || s->o.max_batch_queries < 1 || s->o.lane_depth < 1 ||
-        s->o.lane_depth > 16) {
+        s->o.lane_depth > 16 || (s->o.admission != BP_ADMIT_ARRIVAL && s->o.admission != BP_ADMIT_SHORTEST)) {
         delete s;
         return bp_set_error(e, BP_ERR_INVALID,
                             "bp_server_create: lanes and lane_depth must be 1..16, max_batch_queries >= 1");

@@ -394,7 +394,12 @@ typedef struct {
     int32_t lane_depth;             /* batches queued per lane (>= 1): a lane runs its batches one
                                        after the other on the device, in admission order, while the
                                        next ones are prepared and launched behind them */
+    int32_t admission;              /* BP_ADMIT_ARRIVAL (default) or BP_ADMIT_SHORTEST: the shortest
+                                       waiting query is admitted first (lower median latency under
+                                       load, longer waits for long queries) */
 } bp_server_options;
+
+enum { BP_ADMIT_ARRIVAL = 0, BP_ADMIT_SHORTEST = 1 };
 
 typedef struct {
     int64_t completed, failed, batches, pending;

@@ -92,3 +92,37 @@ def test_gpu_volume_layout_roundtrip():
         want[:lens[s]] = res[off[s]:off[s + 1]]
         assert (got == want).all()
         assert (flat[poff[s]:poff[s] + glen[g]] == want).all()
+
+
+def test_python_mirrors_match_the_header_layouts(tmp_path):
+    # every ctypes Structure and record dtype the Python layer passes across the
+    # boundary has the size and field offsets the C compiler gives the header's
+    # struct of the same name
+    from blastp_b200.api import GAPPED_DTYPE, HSP_DTYPE
+    mirrors = [("bp_params", _lib.BpParams), ("bp_gapped_params", _lib.BpGappedParams),
+               ("bp_batch_options", _lib.BpBatchOptions), ("bp_autotune_trial", _lib.BpAutotuneTrial),
+               ("bp_autotune_options", _lib.BpAutotuneOptions), ("bp_server_options", _lib.BpServerOptions),
+               ("bp_server_metrics", _lib.BpServerMetrics)]
+    dtypes = [("bp_hsp", HSP_DTYPE), ("bp_gapped_hsp", GAPPED_DTYPE)]
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "blastp_b200.h"', 'int main(void) {']
+    expect = []
+    for cname, cls in mirrors:
+        lines.append('printf("%%zu\\n", sizeof(%s));' % cname)
+        expect.append(ctypes.sizeof(cls))
+        for f in cls._fields_:
+            lines.append('printf("%%zu\\n", offsetof(%s, %s));' % (cname, f[0]))
+            expect.append(getattr(cls, f[0]).offset)
+    for cname, dt in dtypes:
+        lines.append('printf("%%zu\\n", sizeof(%s));' % cname)
+        expect.append(dt.itemsize)
+        for name in dt.names:
+            lines.append('printf("%%zu\\n", offsetof(%s, %s));' % (cname, name))
+            expect.append(dt.fields[name][1])
+    lines += ["return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    import subprocess
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    assert got == expect

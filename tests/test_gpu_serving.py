@@ -131,3 +131,50 @@ def test_lane_depth_runs_batches_back_to_back_in_order(engine, world):
     assert st["completed"] == 12 and st["max_in_flight"] >= 2
     # arrivals were microseconds apart: completion order shows in the latencies
     assert all(lat[i] <= lat[i + 1] + 0.5 for i in range(len(lat) - 1)), lat
+
+
+def test_shortest_first_admission(engine, matrix):
+    # one lane, one query per batch: a long request runs while six more wait,
+    # submitted longest first; arrival order completes them longest first,
+    # shortest-first admission completes them shortest first. Each result's
+    # digest equals its plain search's.
+    import time
+    from blastp_b200._lib import ADMIT_ARRIVAL, ADMIT_SHORTEST
+    rng = np.random.default_rng(77)
+    head = synth.residues(rng, 2000)
+    waiting = [synth.residues(rng, n) for n in (900, 700, 500, 300, 150, 60)]
+    db = synth.make_database(rng, 250_000, [head], 0.001, (60, 150), (0.3, 0.5), matrix)
+    d = engine.database(db.residues, db.offsets)
+    plain = []
+    for q in [head] + waiting:
+        h = engine.query(q)
+        r = engine.search(d, h)
+        plain.append(r.digest())
+        r.close()
+        h.close()
+    for policy in (ADMIT_ARRIVAL, ADMIT_SHORTEST):
+        srv = Server(engine, d, max_batch_queries=1, lanes=1, lane_depth=1, admission=policy,
+                     chunk_residues=1 << 20, poll_us=50)
+        t0 = time.perf_counter()
+        first = srv.submit(head)
+        while srv.state(first) == 0:            # queued: wait until the head is admitted
+            pass
+        offs, tickets = [], []
+        for q in waiting:
+            offs.append((time.perf_counter() - t0) * 1e3)
+            tickets.append(srv.submit(q))
+        submitted = (time.perf_counter() - t0) * 1e3
+        srv.wait(first)
+        head_ms = srv.latency(first)
+        done = []
+        for i, t in enumerate(tickets):
+            srv.wait(t)
+            assert srv.digest(t) == plain[1 + i], "policy %d request %d" % (policy, i)
+            done.append(offs[i] + srv.latency(t))
+        srv.close()
+        if head_ms <= submitted:
+            pytest.skip("the head request finished before the others were submitted")
+        order = list(np.argsort(done, kind="stable"))
+        # waiting is longest first: arrival order keeps it, shortest-first reverses it
+        assert order == (list(range(6)) if policy == ADMIT_ARRIVAL else list(range(5, -1, -1))), (policy, done)
+    d.close()
