@@ -785,6 +785,8 @@ def run_ours(args):
                      "frac": achieved / peak, "peak_kind": peak_kind,
                      "traffic": (tpr * w.db.n_residues) if tpr else None,
                      "kernel": "scan_kernel", "kernel_ms": scan_avg_ms,
+                     "kernel_ms_min_median_max": [float(np.min(scan_ms)), float(np.median(scan_ms)),
+                                                  float(np.max(scan_ms))],
                      "algorithmic_bytes": alg_bytes, "issue": issue},
         "rates": rates,
         "hsps": int(len(ref_hsps.hsps)),
