@@ -572,8 +572,8 @@ def run_serving(eng, matrix, args):
     runs = {}
     capacity = None
     plan = [("offered", args.serve_rate, args.serve_requests),
-            ("sustainable", None, max(16, args.serve_requests // 2)),
-            ("sustainable_shortest_first", None, max(16, args.serve_requests // 2))]
+            ("sustainable", None, args.serve_requests),
+            ("sustainable_shortest_first", None, args.serve_requests)]
     if args.serve_rate_high > 0:
         plan.insert(1, ("offered_high", args.serve_rate_high, args.serve_requests))
     for label, rate, n in plan:
