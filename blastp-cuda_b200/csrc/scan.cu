@@ -89,6 +89,7 @@ struct ScanLayout {
     int L;                 // diagonal entries per warp (the longest query's)
     int off_cells, off_entries, off_query, off_members, off_mof, off_warps, off_ctl;
     int off_stream;        // plain and streaming launches: per-warp subject pipeline
+    int off_prof;          // query score profile (0: none): row q holds m[query[q]][0..31]
     int warp_bytes;        // diagonal array + per-lane position table + task queue + blocked list
                            // (+ per-member counters when packed)
     int total;
@@ -108,6 +109,13 @@ struct ExtOut {
 };
 
 __device__ __forceinline__ int msc(const int8_t* m, int a, int b) { return m[a * BP_MROW + b]; }
+
+// The score of query offset q against subject letter s: from the matrix and
+// the query, or (kProf) from the query's score profile, row q.
+template <bool kProf>
+__device__ __forceinline__ int qscore(const int8_t* m, const uint8_t* qry, int q, int s) {
+    return kProf ? m[q * BP_MROW + s] : msc(m, qry[q], s);
+}
 
 __device__ __forceinline__ int warp_incl_sum(int x, int lane) {
 #pragma unroll
@@ -133,8 +141,9 @@ __device__ __forceinline__ int warp_incl_max(int x, int lane) {
 // the first letter where best - run >= xdrop (or, when walking right,
 // run <= 0).  Returns the best score, the index of the letter that first
 // reached it (-1 if none), and the index of the stopping letter (n if the
-// walk ran out of letters).  All lanes return the same values.
-template <bool kRight>
+// walk ran out of letters).  All lanes return the same values.  kProf: m is
+// the query's score profile.
+template <bool kRight, bool kProf>
 __device__ __forceinline__ void warp_xdrop(const int8_t* m, const uint8_t* __restrict__ subj, const uint8_t* qry,
                                            int s0, int q0, int n, int start, int xdrop, int lane, int& best,
                                            int& best_i, int& stop_i) {
@@ -146,7 +155,13 @@ __device__ __forceinline__ void warp_xdrop(const int8_t* m, const uint8_t* __res
         const int i = i0 + lane;
         const bool valid = i < n;
         int v = 0;
-        if (valid) v = kRight ? msc(m, qry[q0 + i], __ldg(subj + s0 + i)) : msc(m, qry[q0 - i], __ldg(subj + s0 - i));
+        if (valid) {
+            if (kProf)
+                v = kRight ? m[(q0 + i) * BP_MROW + __ldg(subj + s0 + i)]
+                           : m[(q0 - i) * BP_MROW + __ldg(subj + s0 - i)];
+            else
+                v = kRight ? msc(m, qry[q0 + i], __ldg(subj + s0 + i)) : msc(m, qry[q0 - i], __ldg(subj + s0 - i));
+        }
         const int run = carry + warp_incl_sum(v, lane);
         const int pm = max(best, warp_incl_max(run, lane));
         const bool stop = valid && ((pm - run >= xdrop) || (kRight && run <= 0));
@@ -171,13 +186,15 @@ __device__ __forceinline__ void warp_xdrop(const int8_t* m, const uint8_t* __res
 // are fetched four letters at a time so the loads overlap the dependent score
 // chain, a group of four is tested for a stop once (the running scores and
 // bests of its letters are all known), and only a group that stops, or the
-// last partial one, is resolved letter by letter.
-template <bool kRight>
+// last partial one, is resolved letter by letter.  kProf: m is the query's
+// score profile, stepped one row per letter.
+template <bool kRight, bool kProf>
 __device__ __forceinline__ void lane_xdrop(const int8_t* m, const uint8_t* __restrict__ subj, const uint8_t* qry,
                                            int s0, int q0, int n, int start, int xdrop, int& best, int& best_i,
                                            int& stop_i) {
     constexpr int D = kRight ? 1 : -1;
     const uint8_t* qp = qry + q0;
+    const int8_t* pp = m + (kProf ? q0 * BP_MROW : 0);
     const uint8_t* sp = subj + s0;
     int run = start;
     best = start;
@@ -187,7 +204,9 @@ __device__ __forceinline__ void lane_xdrop(const int8_t* m, const uint8_t* __res
     for (; i0 + 4 <= n; i0 += 4) {
         int sc[4];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) sc[k] = msc(m, qp[D * (i0 + k)], __ldg(sp + D * (i0 + k)));
+        for (int k = 0; k < 4; ++k)
+            sc[k] = kProf ? pp[D * (i0 + k) * BP_MROW + __ldg(sp + D * (i0 + k))]
+                          : msc(m, qp[D * (i0 + k)], __ldg(sp + D * (i0 + k)));
         // the group's running scores and bests; one test for a stop anywhere in it
         const int r0 = run + sc[0], r1 = r0 + sc[1], r2 = r1 + sc[2], r3 = r2 + sc[3];
         const int b0 = max(best, r0), b1 = max(b0, r1), b2 = max(b1, r2), b3 = max(b2, r3);
@@ -227,7 +246,7 @@ __device__ __forceinline__ void lane_xdrop(const int8_t* m, const uint8_t* __res
         run = r3;
     }
     for (; i0 < n; ++i0) {
-        run += msc(m, qp[D * i0], __ldg(sp + D * i0));
+        run += kProf ? pp[D * i0 * BP_MROW + __ldg(sp + D * i0)] : msc(m, qp[D * i0], __ldg(sp + D * i0));
         if (run > best) {
             best = run;
             best_i = i0;
@@ -244,15 +263,17 @@ __device__ __forceinline__ void lane_xdrop(const int8_t* m, const uint8_t* __res
 // right walk starting from the left score.  The walks stay within query
 // offsets [q_lo, q_hi): the whole query, or one query of a packed table.  kWarp: every lane passes the
 // same arguments, the walks use the whole warp and every lane gets the
-// result; otherwise each lane extends its own hit pair.
-template <bool kWarp>
+// result; otherwise each lane extends its own hit pair.  kProf: every score
+// comes from the query's score profile `prof` instead of m and qry.
+template <bool kWarp, bool kProf = false>
 __device__ __forceinline__ ExtOut extend_two_hit(const int8_t* m, const uint8_t* __restrict__ subj, int slen,
                                                  const uint8_t* qry, int q_lo, int q_hi, int s_left, int s_right,
-                                                 int q_right, int xdrop, int lane) {
+                                                 int q_right, int xdrop, int lane, const int8_t* prof = nullptr) {
+    if (kProf) m = prof;
     int score = 0, left_score = 0, shift = 0;
 #pragma unroll
     for (int i = 0; i < BP_WORD; ++i) {
-        score += msc(m, qry[q_right + i], __ldg(subj + s_right + i));
+        score += qscore<kProf>(m, qry, q_right + i, __ldg(subj + s_right + i));
         if (score > left_score) {
             left_score = score;
             shift = i + 1;
@@ -263,8 +284,10 @@ __device__ __forceinline__ ExtOut extend_two_hit(const int8_t* m, const uint8_t*
 
     int lbest, lbest_k, lstop;
     const int nl = min(s_right, q_right - q_lo);
-    if (kWarp) warp_xdrop<false>(m, subj, qry, s_right - 1, q_right - 1, nl, 0, xdrop, lane, lbest, lbest_k, lstop);
-    else lane_xdrop<false>(m, subj, qry, s_right - 1, q_right - 1, nl, 0, xdrop, lbest, lbest_k, lstop);
+    if (kWarp)
+        warp_xdrop<false, kProf>(m, subj, qry, s_right - 1, q_right - 1, nl, 0, xdrop, lane, lbest, lbest_k, lstop);
+    else
+        lane_xdrop<false, kProf>(m, subj, qry, s_right - 1, q_right - 1, nl, 0, xdrop, lbest, lbest_k, lstop);
     const int left_d = lbest_k + 1;
     left_score = lbest;
 
@@ -276,8 +299,10 @@ __device__ __forceinline__ ExtOut extend_two_hit(const int8_t* m, const uint8_t*
         o.right_ext = 1;
         const int nr = min(slen - s_right, q_hi - q_right);
         int rbest, rbest_i, rstop;
-        if (kWarp) warp_xdrop<true>(m, subj, qry, s_right, q_right, nr, left_score, xdrop, lane, rbest, rbest_i, rstop);
-        else lane_xdrop<true>(m, subj, qry, s_right, q_right, nr, left_score, xdrop, rbest, rbest_i, rstop);
+        if (kWarp)
+            warp_xdrop<true, kProf>(m, subj, qry, s_right, q_right, nr, left_score, xdrop, lane, rbest, rbest_i,
+                                    rstop);
+        else lane_xdrop<true, kProf>(m, subj, qry, s_right, q_right, nr, left_score, xdrop, rbest, rbest_i, rstop);
         right_d = rbest_i + 1;
         right_score = rbest;
         o.s_last = s_right + rstop;
@@ -327,7 +352,9 @@ __device__ __forceinline__ void load_window(const uint8_t* __restrict__ sub, int
 }
 
 // One warp's view of the subject it is scanning.
-template <typename DiagT>
+// kProf: the launch may give the warp the query's score profile (plain and
+// streaming launches; batched launches never do).
+template <typename DiagT, bool kProf = false>
 struct WarpScan {
     const ScanArgs* a;
     const int8_t* m;
@@ -341,6 +368,7 @@ struct WarpScan {
     int nt, nb;            // queued tasks and blocked hits (warp-uniform)
     int ext, succ;         // this lane's share of the subject's counters
     int* wcnt;             // packed: per-member hits, successes, extensions (shared memory)
+    const int8_t* prof;    // the query's score profile, or null
 };
 
 // The query an offset belongs to: its bounds, x-drop and cutoff.  Packed
@@ -420,8 +448,9 @@ __device__ __forceinline__ DiagT diag_after(const ExtOut& x, int hs, int base) {
 // pending, and a hit on a pending diagonal joins the blocked list (needs room
 // for 32 more tasks and 32 more blocked hits).  Otherwise each pair is
 // extended at once by the whole warp, one after the other.
-template <bool kDefer, bool kPacked, typename DiagT>
-__device__ __forceinline__ void apply_hits(WarpScan<DiagT>& w, bool hv, int hs, int hq, int d, int key, bool count) {
+template <bool kDefer, bool kPacked, typename DiagT, bool kProf>
+__device__ __forceinline__ void apply_hits(WarpScan<DiagT, kProf>& w, bool hv, int hs, int hq, int d, int key,
+                                           bool count) {
     using B = DiagBits<DiagT>;
     const unsigned vmask = __ballot_sync(kFull, hv);
     if (!vmask) return;
@@ -490,8 +519,8 @@ __device__ __forceinline__ void apply_hits(WarpScan<DiagT>& w, bool hv, int hs, 
 }
 
 // Walks every queued extension and writes its outcome into its diagonal.
-template <bool kPacked, typename DiagT>
-__device__ void flush_tasks(WarpScan<DiagT>& w) {
+template <bool kPacked, typename DiagT, bool kProf>
+__device__ void flush_tasks(WarpScan<DiagT, kProf>& w) {
     const int nt = w.nt;
     if (nt >= kLaneWalkMin) {
         for (int t0 = 0; t0 < nt; t0 += 32) {
@@ -503,8 +532,12 @@ __device__ void flush_tasks(WarpScan<DiagT>& w) {
                 tk = w.tasks[t];
                 const int hq = (int)(tk.hqx & 0xffffu), diff = (int)(tk.hqx >> 16);
                 const Member mb = member_at<kPacked>(w, hq);
-                x = extend_two_hit<false>(w.m, w.sub, w.slen, w.qs, mb.q_lo, mb.q_hi, tk.hs - diff + BP_WORD, tk.hs,
-                                          hq, mb.xdrop, w.lane);
+                if (kProf && w.prof)
+                    x = extend_two_hit<false, true>(w.m, w.sub, w.slen, w.qs, mb.q_lo, mb.q_hi, tk.hs - diff + BP_WORD,
+                                                    tk.hs, hq, mb.xdrop, w.lane, w.prof);
+                else
+                    x = extend_two_hit<false>(w.m, w.sub, w.slen, w.qs, mb.q_lo, mb.q_hi, tk.hs - diff + BP_WORD,
+                                              tk.hs, hq, mb.xdrop, w.lane);
                 found = x.score >= mb.cutoff;
                 w.diag[tk.d] = diag_after<DiagT>(x, tk.hs, w.base);
             }
@@ -515,8 +548,12 @@ __device__ void flush_tasks(WarpScan<DiagT>& w) {
             const Task tk = w.tasks[t];
             const int hq = (int)(tk.hqx & 0xffffu), diff = (int)(tk.hqx >> 16);
             const Member mb = member_at<kPacked>(w, hq);
-            const ExtOut x = extend_two_hit<true>(w.m, w.sub, w.slen, w.qs, mb.q_lo, mb.q_hi, tk.hs - diff + BP_WORD,
-                                                  tk.hs, hq, mb.xdrop, w.lane);
+            const ExtOut x =
+                (kProf && w.prof)
+                    ? extend_two_hit<true, true>(w.m, w.sub, w.slen, w.qs, mb.q_lo, mb.q_hi, tk.hs - diff + BP_WORD,
+                                                 tk.hs, hq, mb.xdrop, w.lane, w.prof)
+                    : extend_two_hit<true>(w.m, w.sub, w.slen, w.qs, mb.q_lo, mb.q_hi, tk.hs - diff + BP_WORD, tk.hs,
+                                           hq, mb.xdrop, w.lane);
             const bool found = w.lane == 0 && x.score >= mb.cutoff;
             if (w.lane == 0) w.diag[tk.d] = diag_after<DiagT>(x, tk.hs, w.base);
             emit<kPacked>(w, found, tk.key, tk.hs, hq, x);
@@ -529,8 +566,8 @@ __device__ void flush_tasks(WarpScan<DiagT>& w) {
 // Resolves the queued extensions, then replays the blocked hits once, in
 // order.  A replayed hit may queue a new extension (and block the hits after
 // it on its diagonal again); the blocked list is rewritten in place.
-template <bool kPacked, typename DiagT>
-__device__ void resolve(WarpScan<DiagT>& w) {
+template <bool kPacked, typename DiagT, bool kProf>
+__device__ void resolve(WarpScan<DiagT, kProf>& w) {
     flush_tasks<kPacked>(w);
     const int n = w.nb;
     w.nb = 0;
@@ -570,11 +607,11 @@ __device__ __forceinline__ void rebase_diag(DiagT* diag, int n, int delta, int l
 // base + s0 + 128 + qlen (a hit lies before s0 + 128 and a right walk ends
 // within qlen letters of it), so the offset is reset when that bound could
 // reach DiagBits::kMax.  clear_len: entries of the warp's whole array.
-template <typename CellT, bool kDefer, bool kPacked, typename DiagT, bool kCheck = false>
+template <typename CellT, bool kDefer, bool kPacked, typename DiagT, bool kCheck = false, bool kProf = false>
 __device__ void scan_subject(const ScanArgs& a, const int8_t* m, const uint8_t* qs, const CellT* cells,
                              const uint16_t* entries, DiagT* diag, int clear_len, uint32_t* lane_pos, Task* tasks,
                              Task* blocked, int* wcnt, int oid, const uint8_t* __restrict__ sub, int slen, int& base,
-                             int lane) {
+                             int lane, const int8_t* prof = nullptr) {
     using B = DiagBits<DiagT>;
     const int L = a.diag_len;
     if (base + a.qlen + 129 >= B::kMax) {
@@ -583,7 +620,7 @@ __device__ void scan_subject(const ScanArgs& a, const int8_t* m, const uint8_t* 
         __syncwarp();
         base = a.window;
     }
-    WarpScan<DiagT> w;
+    WarpScan<DiagT, kProf> w;
     w.a = &a;
     w.m = m;
     w.qs = qs;
@@ -599,6 +636,7 @@ __device__ void scan_subject(const ScanArgs& a, const int8_t* m, const uint8_t* 
     w.nt = w.nb = 0;
     w.ext = w.succ = 0;
     w.wcnt = wcnt;
+    w.prof = prof;
     if (kPacked) {
         for (int i = lane; i < 3 * a.n_members; i += 32) wcnt[i] = 0;
         __syncwarp();
@@ -756,7 +794,8 @@ __device__ __forceinline__ WarpRegions<DiagT> warp_regions(const ScanLayout& lay
 // shared memory for every warp of the CTA (callers synchronise after).
 template <typename CellT, bool kCellsSmem>
 __device__ __forceinline__ void load_tables(const ScanArgs& a, const ScanLayout& lay, const int8_t*& m,
-                                            const uint8_t*& qs, const CellT*& cells, const uint16_t*& entries) {
+                                            const uint8_t*& qs, const CellT*& cells, const uint16_t*& entries,
+                                            const int8_t*& prof) {
     uint8_t* sm = bp_smem;
     int8_t* mm = reinterpret_cast<int8_t*>(sm);
     uint8_t* q = sm + lay.off_query;
@@ -770,6 +809,13 @@ __device__ __forceinline__ void load_tables(const ScanArgs& a, const ScanLayout&
         for (int i = threadIdx.x; i < a.n_entries; i += blockDim.x) e[i] = a.entries[i];
     }
     for (int i = threadIdx.x; i < a.qlen; i += blockDim.x) q[i] = a.query[i];
+    prof = nullptr;
+    if (lay.off_prof) {
+        int8_t* pf = reinterpret_cast<int8_t*>(sm + lay.off_prof);
+        for (int i = threadIdx.x; i < a.qlen * BP_MROW; i += blockDim.x)
+            pf[i] = a.matrix[(int)__ldg(a.query + i / BP_MROW) * BP_MROW + i % BP_MROW];
+        prof = pf;
+    }
     m = mm;
     qs = q;
     cells = kCellsSmem ? reinterpret_cast<const CellT*>(sm + lay.off_cells) : reinterpret_cast<const CellT*>(a.cells);
@@ -803,7 +849,8 @@ scan_kernel(ScanArgs a, ScanLayout lay) {
     const uint8_t* qs;
     const CellT* cells;
     const uint16_t* entries;
-    load_tables<CellT, kCellsSmem>(a, lay, m, qs, cells, entries);
+    const int8_t* prof;
+    load_tables<CellT, kCellsSmem>(a, lay, m, qs, cells, entries, prof);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const WarpRegions<DiagT> wr = warp_regions<DiagT>(lay, warp, lane);
     for (int i = lane; i < lay.L; i += 32) wr.diag[i] = 0;
@@ -853,9 +900,10 @@ scan_kernel(ScanArgs a, ScanLayout lay) {
         if (go) {
             const StreamSubj& cur = sc->q[i];
             const long long s0 = cur.s, e0 = cur.e;
-            scan_subject<CellT, kDefer, false>(a, m, qs, cells, entries, wr.diag, lay.L, wr.lane_pos, wr.tasks,
+            scan_subject<CellT, kDefer, false, DiagT, false, true>(a, m, qs, cells, entries, wr.diag, lay.L,
+                                                                  wr.lane_pos, wr.tasks,
                                                wr.blocked, wr.wcnt, a.oid_base + (int)(cur.id & ~kSecond), a.db + s0,
-                                               (int)(e0 - s0), base, lane);
+                                               (int)(e0 - s0), base, lane, prof);
         }
         __syncwarp();
         if (lane == 0) sc->q[i].id = slot_subject(a, n_long, atomicAdd(a.cursor, 1u));
@@ -922,7 +970,8 @@ scan_stream_kernel(ScanArgs a, ScanLayout lay) {
     const uint8_t* qs;
     const CellT* cells;
     const uint16_t* entries;
-    load_tables<CellT, kCellsSmem>(a, lay, m, qs, cells, entries);
+    const int8_t* prof;
+    load_tables<CellT, kCellsSmem>(a, lay, m, qs, cells, entries, prof);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const WarpRegions<uint16_t> wr = warp_regions<uint16_t>(lay, warp, lane);
     for (int i = lane; i < lay.L; i += 32) wr.diag[i] = 0;
@@ -971,10 +1020,10 @@ scan_stream_kernel(ScanArgs a, ScanLayout lay) {
         const StreamSubj& cur = sc->q[i];
         if (go) {
             const long long s0 = cur.s, e0 = cur.e;
-            scan_subject<CellT, kDefer, false, uint16_t, true>(a, m, qs, cells, entries, wr.diag, lay.L, wr.lane_pos,
-                                                              wr.tasks, wr.blocked, wr.wcnt,
-                                                              a.oid_base + (int)cur.id, a.db + s0, (int)(e0 - s0),
-                                                              base, lane);
+            scan_subject<CellT, kDefer, false, uint16_t, true, true>(a, m, qs, cells, entries, wr.diag, lay.L,
+                                                                    wr.lane_pos, wr.tasks, wr.blocked, wr.wcnt,
+                                                                    a.oid_base + (int)cur.id, a.db + s0,
+                                                                    (int)(e0 - s0), base, lane, prof);
         }
         __syncwarp();
         if (lane == 0) sc->q[i].id = atomicAdd(a.cursor, 1u);   // becomes the one after next
@@ -1110,7 +1159,7 @@ scan_batch_kernel(BatchArgs b, ScanLayout lay) {
 }
 
 ScanLayout make_layout(int qlen, int L, int64_t n_entries, int warps, int cells_mode, int entries_smem,
-                       bool packed, bool stream = false) {
+                       bool packed, bool stream = false, bool prof = false) {
     ScanLayout l{};
     l.warps = warps;
     l.cells_mode = cells_mode;
@@ -1127,6 +1176,10 @@ ScanLayout make_layout(int qlen, int L, int64_t n_entries, int warps, int cells_
     if (off > big) off = big;
     l.off_query = (int)off;
     off = al(off + qlen, 16);
+    if (prof) {
+        l.off_prof = (int)off;
+        off = al(off + (long long)BP_MROW * qlen, 16);
+    }
     l.off_members = (int)off;
     l.off_mof = (int)off;
     if (packed) {
@@ -1151,7 +1204,13 @@ ScanLayout make_layout(int qlen, int L, int64_t n_entries, int warps, int cells_
 }
 
 // Picks the layout with the most warps, preferring the whole table in shared
-// memory as long as that still leaves at least 16 warps.
+// memory as long as that still leaves at least 16 warps.  Plain and streaming
+// launches of queries whose extensions are queued (one lane walks each) also
+// get the query's score profile when it costs at most one warp and moves
+// nothing out of shared memory: the walks then read one profile byte per
+// letter instead of the query letter and the matrix entry (250 aa: 4.47 ->
+// 4.37 ms, 500 aa: 6.50 -> 6.37 ms per 1M subjects; at 1,000 aa the profile
+// would cost the table its place in shared memory, 12.6 -> 15.3 ms).
 bool choose_layout(int qlen, int L, int64_t n_entries, int smem_optin, ScanLayout* out, bool packed = false,
                    bool stream = false) {
     const int cell_modes[2] = {n_entries < 65536 ? 0 : 1, 2};
@@ -1163,6 +1222,14 @@ bool choose_layout(int qlen, int L, int64_t n_entries, int smem_optin, ScanLayou
                     const ScanLayout l = make_layout(qlen, L, n_entries, w, cm, es, packed, stream);
                     if (l.total <= smem_optin) {
                         *out = l;
+                        if (stream && !packed && qlen >= kDeferMinQlen && L <= kNarrowMaxL)
+                            for (int wp = w; wp >= w - 1 && wp >= 1; --wp) {
+                                const ScanLayout lp = make_layout(qlen, L, n_entries, wp, cm, es, packed, stream, true);
+                                if (lp.total <= smem_optin) {
+                                    *out = lp;
+                                    break;
+                                }
+                            }
                         return true;
                     }
                 }
