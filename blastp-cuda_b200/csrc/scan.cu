@@ -264,12 +264,14 @@ __device__ __forceinline__ void lane_xdrop(const int8_t* m, const uint8_t* __res
 // offsets [q_lo, q_hi): the whole query, or one query of a packed table.  kWarp: every lane passes the
 // same arguments, the walks use the whole warp and every lane gets the
 // result; otherwise each lane extends its own hit pair.  kProf: every score
-// comes from the query's score profile `prof` instead of m and qry.
+// comes from the query's score profile, which the layout places right after
+// the query (at the next 16-byte boundary; plain and streaming launches, one
+// query, so q_hi is its length).
 template <bool kWarp, bool kProf = false>
 __device__ __forceinline__ ExtOut extend_two_hit(const int8_t* m, const uint8_t* __restrict__ subj, int slen,
                                                  const uint8_t* qry, int q_lo, int q_hi, int s_left, int s_right,
-                                                 int q_right, int xdrop, int lane, const int8_t* prof = nullptr) {
-    if (kProf) m = prof;
+                                                 int q_right, int xdrop, int lane) {
+    if (kProf) m = reinterpret_cast<const int8_t*>(qry) + ((q_hi + 15) & ~15);
     int score = 0, left_score = 0, shift = 0;
 #pragma unroll
     for (int i = 0; i < BP_WORD; ++i) {
@@ -352,8 +354,8 @@ __device__ __forceinline__ void load_window(const uint8_t* __restrict__ sub, int
 }
 
 // One warp's view of the subject it is scanning.
-// kProf: the launch may give the warp the query's score profile (plain and
-// streaming launches; batched launches never do).
+// kProf: the launch's layout holds the query's score profile (plain and
+// streaming launches only).
 template <typename DiagT, bool kProf = false>
 struct WarpScan {
     const ScanArgs* a;
@@ -368,7 +370,6 @@ struct WarpScan {
     int nt, nb;            // queued tasks and blocked hits (warp-uniform)
     int ext, succ;         // this lane's share of the subject's counters
     int* wcnt;             // packed: per-member hits, successes, extensions (shared memory)
-    const int8_t* prof;    // the query's score profile, or null
 };
 
 // The query an offset belongs to: its bounds, x-drop and cutoff.  Packed
@@ -532,9 +533,9 @@ __device__ void flush_tasks(WarpScan<DiagT, kProf>& w) {
                 tk = w.tasks[t];
                 const int hq = (int)(tk.hqx & 0xffffu), diff = (int)(tk.hqx >> 16);
                 const Member mb = member_at<kPacked>(w, hq);
-                if (kProf && w.prof)
+                if (kProf)
                     x = extend_two_hit<false, true>(w.m, w.sub, w.slen, w.qs, mb.q_lo, mb.q_hi, tk.hs - diff + BP_WORD,
-                                                    tk.hs, hq, mb.xdrop, w.lane, w.prof);
+                                                    tk.hs, hq, mb.xdrop, w.lane);
                 else
                     x = extend_two_hit<false>(w.m, w.sub, w.slen, w.qs, mb.q_lo, mb.q_hi, tk.hs - diff + BP_WORD,
                                               tk.hs, hq, mb.xdrop, w.lane);
@@ -549,9 +550,9 @@ __device__ void flush_tasks(WarpScan<DiagT, kProf>& w) {
             const int hq = (int)(tk.hqx & 0xffffu), diff = (int)(tk.hqx >> 16);
             const Member mb = member_at<kPacked>(w, hq);
             const ExtOut x =
-                (kProf && w.prof)
+                kProf
                     ? extend_two_hit<true, true>(w.m, w.sub, w.slen, w.qs, mb.q_lo, mb.q_hi, tk.hs - diff + BP_WORD,
-                                                 tk.hs, hq, mb.xdrop, w.lane, w.prof)
+                                                 tk.hs, hq, mb.xdrop, w.lane)
                     : extend_two_hit<true>(w.m, w.sub, w.slen, w.qs, mb.q_lo, mb.q_hi, tk.hs - diff + BP_WORD, tk.hs,
                                            hq, mb.xdrop, w.lane);
             const bool found = w.lane == 0 && x.score >= mb.cutoff;
@@ -611,7 +612,7 @@ template <typename CellT, bool kDefer, bool kPacked, typename DiagT, bool kCheck
 __device__ void scan_subject(const ScanArgs& a, const int8_t* m, const uint8_t* qs, const CellT* cells,
                              const uint16_t* entries, DiagT* diag, int clear_len, uint32_t* lane_pos, Task* tasks,
                              Task* blocked, int* wcnt, int oid, const uint8_t* __restrict__ sub, int slen, int& base,
-                             int lane, const int8_t* prof = nullptr) {
+                             int lane) {
     using B = DiagBits<DiagT>;
     const int L = a.diag_len;
     if (base + a.qlen + 129 >= B::kMax) {
@@ -636,7 +637,6 @@ __device__ void scan_subject(const ScanArgs& a, const int8_t* m, const uint8_t* 
     w.nt = w.nb = 0;
     w.ext = w.succ = 0;
     w.wcnt = wcnt;
-    w.prof = prof;
     if (kPacked) {
         for (int i = lane; i < 3 * a.n_members; i += 32) wcnt[i] = 0;
         __syncwarp();
@@ -794,8 +794,7 @@ __device__ __forceinline__ WarpRegions<DiagT> warp_regions(const ScanLayout& lay
 // shared memory for every warp of the CTA (callers synchronise after).
 template <typename CellT, bool kCellsSmem>
 __device__ __forceinline__ void load_tables(const ScanArgs& a, const ScanLayout& lay, const int8_t*& m,
-                                            const uint8_t*& qs, const CellT*& cells, const uint16_t*& entries,
-                                            const int8_t*& prof) {
+                                            const uint8_t*& qs, const CellT*& cells, const uint16_t*& entries) {
     uint8_t* sm = bp_smem;
     int8_t* mm = reinterpret_cast<int8_t*>(sm);
     uint8_t* q = sm + lay.off_query;
@@ -809,12 +808,10 @@ __device__ __forceinline__ void load_tables(const ScanArgs& a, const ScanLayout&
         for (int i = threadIdx.x; i < a.n_entries; i += blockDim.x) e[i] = a.entries[i];
     }
     for (int i = threadIdx.x; i < a.qlen; i += blockDim.x) q[i] = a.query[i];
-    prof = nullptr;
     if (lay.off_prof) {
         int8_t* pf = reinterpret_cast<int8_t*>(sm + lay.off_prof);
         for (int i = threadIdx.x; i < a.qlen * BP_MROW; i += blockDim.x)
             pf[i] = a.matrix[(int)__ldg(a.query + i / BP_MROW) * BP_MROW + i % BP_MROW];
-        prof = pf;
     }
     m = mm;
     qs = q;
@@ -839,7 +836,7 @@ struct StreamCtl {
     int hint, ready;       // chunk hint of locate(); highest chunk known to be there
 };
 
-template <typename CellT, bool kCellsSmem, bool kDefer, typename DiagT>
+template <typename CellT, bool kCellsSmem, bool kDefer, typename DiagT, bool kProf>
 __global__ void __launch_bounds__(kMaxWarps * 32, 1)
 scan_kernel(ScanArgs a, ScanLayout lay) {
     // an earlier check on the device refused the inputs: nothing to scan
@@ -849,8 +846,7 @@ scan_kernel(ScanArgs a, ScanLayout lay) {
     const uint8_t* qs;
     const CellT* cells;
     const uint16_t* entries;
-    const int8_t* prof;
-    load_tables<CellT, kCellsSmem>(a, lay, m, qs, cells, entries, prof);
+    load_tables<CellT, kCellsSmem>(a, lay, m, qs, cells, entries);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const WarpRegions<DiagT> wr = warp_regions<DiagT>(lay, warp, lane);
     for (int i = lane; i < lay.L; i += 32) wr.diag[i] = 0;
@@ -900,10 +896,10 @@ scan_kernel(ScanArgs a, ScanLayout lay) {
         if (go) {
             const StreamSubj& cur = sc->q[i];
             const long long s0 = cur.s, e0 = cur.e;
-            scan_subject<CellT, kDefer, false, DiagT, false, true>(a, m, qs, cells, entries, wr.diag, lay.L,
+            scan_subject<CellT, kDefer, false, DiagT, false, kProf>(a, m, qs, cells, entries, wr.diag, lay.L,
                                                                   wr.lane_pos, wr.tasks,
                                                wr.blocked, wr.wcnt, a.oid_base + (int)(cur.id & ~kSecond), a.db + s0,
-                                               (int)(e0 - s0), base, lane, prof);
+                                               (int)(e0 - s0), base, lane);
         }
         __syncwarp();
         if (lane == 0) sc->q[i].id = slot_subject(a, n_long, atomicAdd(a.cursor, 1u));
@@ -963,15 +959,14 @@ __device__ __forceinline__ bool locate(const ScanArgs& a, uint32_t id, int& hint
 // line read after a flag can hold bytes loaded before it.  Residue codes are
 // checked as they are read; offsets are checked against their chunk before
 // any residue of the subject is touched.
-template <typename CellT, bool kCellsSmem, bool kDefer>
+template <typename CellT, bool kCellsSmem, bool kDefer, bool kProf>
 __global__ void __launch_bounds__(kMaxWarps * 32, 1)
 scan_stream_kernel(ScanArgs a, ScanLayout lay) {
     const int8_t* m;
     const uint8_t* qs;
     const CellT* cells;
     const uint16_t* entries;
-    const int8_t* prof;
-    load_tables<CellT, kCellsSmem>(a, lay, m, qs, cells, entries, prof);
+    load_tables<CellT, kCellsSmem>(a, lay, m, qs, cells, entries);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const WarpRegions<uint16_t> wr = warp_regions<uint16_t>(lay, warp, lane);
     for (int i = lane; i < lay.L; i += 32) wr.diag[i] = 0;
@@ -1020,10 +1015,10 @@ scan_stream_kernel(ScanArgs a, ScanLayout lay) {
         const StreamSubj& cur = sc->q[i];
         if (go) {
             const long long s0 = cur.s, e0 = cur.e;
-            scan_subject<CellT, kDefer, false, uint16_t, true, true>(a, m, qs, cells, entries, wr.diag, lay.L,
+            scan_subject<CellT, kDefer, false, uint16_t, true, kProf>(a, m, qs, cells, entries, wr.diag, lay.L,
                                                                     wr.lane_pos, wr.tasks, wr.blocked, wr.wcnt,
                                                                     a.oid_base + (int)cur.id, a.db + s0,
-                                                                    (int)(e0 - s0), base, lane, prof);
+                                                                    (int)(e0 - s0), base, lane);
         }
         __syncwarp();
         if (lane == 0) sc->q[i].id = atomicAdd(a.cursor, 1u);   // becomes the one after next
@@ -1176,7 +1171,7 @@ ScanLayout make_layout(int qlen, int L, int64_t n_entries, int warps, int cells_
     if (off > big) off = big;
     l.off_query = (int)off;
     off = al(off + qlen, 16);
-    if (prof) {
+    if (prof) {   // right after the query: the walks find it from the query's address
         l.off_prof = (int)off;
         off = al(off + (long long)BP_MROW * qlen, 16);
     }
@@ -1237,9 +1232,9 @@ bool choose_layout(int qlen, int L, int64_t n_entries, int smem_optin, ScanLayou
     return false;
 }
 
-template <typename CellT, bool kCellsSmem, bool kDefer, typename DiagT>
+template <typename CellT, bool kCellsSmem, bool kDefer, typename DiagT, bool kProf = false>
 cudaError_t launch(bp_engine* e, cudaStream_t stream, const ScanArgs& a, const ScanLayout& lay) {
-    auto kern = scan_kernel<CellT, kCellsSmem, kDefer, DiagT>;
+    auto kern = scan_kernel<CellT, kCellsSmem, kDefer, DiagT, kProf>;
     // the largest allowed size, not this launch's: launches of one instance
     // with different layouts (batch classes, captured graph nodes replayed
     // later) must all stay valid whatever order the attribute was set in
@@ -1253,9 +1248,9 @@ cudaError_t launch(bp_engine* e, cudaStream_t stream, const ScanArgs& a, const S
     return cudaGetLastError();
 }
 
-template <typename CellT, bool kCellsSmem, bool kDefer>
+template <typename CellT, bool kCellsSmem, bool kDefer, bool kProf = false>
 cudaError_t launch_stream(bp_engine* e, cudaStream_t stream, const ScanArgs& a, const ScanLayout& lay) {
-    auto kern = scan_stream_kernel<CellT, kCellsSmem, kDefer>;
+    auto kern = scan_stream_kernel<CellT, kCellsSmem, kDefer, kProf>;
     cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, e->smem_optin);
     if (err != cudaSuccess) return err;
     int grid = e->sm_count;
@@ -1350,6 +1345,11 @@ cudaError_t bp_launch_scan_stream(bp_engine* e, cudaStream_t st, const ScanArgs&
     if (!choose_layout(a.qlen, a.diag_len, a.n_entries, e->smem_optin, &lay, false, true))
         return cudaErrorInvalidValue;
     if (lay.L > kNarrowMaxL || a.n_chunks < 1) return cudaErrorNotSupported;
+    if (a.qlen >= kDeferMinQlen && lay.off_prof) {
+        if (lay.cells_mode == 0) return launch_stream<uint16_t, true, true, true>(e, st, a, lay);
+        if (lay.cells_mode == 1) return launch_stream<uint32_t, true, true, true>(e, st, a, lay);
+        return launch_stream<uint32_t, false, true, true>(e, st, a, lay);
+    }
     if (a.qlen >= kDeferMinQlen) {
         if (lay.cells_mode == 0) return launch_stream<uint16_t, true, true>(e, st, a, lay);
         if (lay.cells_mode == 1) return launch_stream<uint32_t, true, true>(e, st, a, lay);
@@ -1371,6 +1371,11 @@ cudaError_t bp_launch_scan_on(bp_engine* e, cudaStream_t st, const ScanArgs& a) 
         if (lay.cells_mode == 0) return launch<uint16_t, true, true, uint32_t>(e, st, a, lay);
         if (lay.cells_mode == 1) return launch<uint32_t, true, true, uint32_t>(e, st, a, lay);
         return launch<uint32_t, false, true, uint32_t>(e, st, a, lay);
+    }
+    if (a.qlen >= kDeferMinQlen && lay.off_prof) {
+        if (lay.cells_mode == 0) return launch<uint16_t, true, true, N, true>(e, st, a, lay);
+        if (lay.cells_mode == 1) return launch<uint32_t, true, true, N, true>(e, st, a, lay);
+        return launch<uint32_t, false, true, N, true>(e, st, a, lay);
     }
     if (a.qlen >= kDeferMinQlen) {
         if (lay.cells_mode == 0) return launch<uint16_t, true, true, N>(e, st, a, lay);
