@@ -1204,8 +1204,9 @@ ScanLayout make_layout(int qlen, int L, int64_t n_entries, int warps, int cells_
 // get the query's score profile when it costs at most one warp and moves
 // nothing out of shared memory: the walks then read one profile byte per
 // letter instead of the query letter and the matrix entry (250 aa: 4.47 ->
-// 4.37 ms, 500 aa: 6.50 -> 6.37 ms per 1M subjects; at 1,000 aa the profile
-// would cost the table its place in shared memory, 12.6 -> 15.3 ms).
+// 4.38 ms, 500 aa: 6.50 -> 6.38 ms per 1M subjects; at 700 aa it would cost
+// two warps, 8.37 -> 8.76 ms, at 1,000 aa the table's place in shared
+// memory, 12.6 -> 15.3 ms).
 bool choose_layout(int qlen, int L, int64_t n_entries, int smem_optin, ScanLayout* out, bool packed = false,
                    bool stream = false) {
     const int cell_modes[2] = {n_entries < 65536 ? 0 : 1, 2};
