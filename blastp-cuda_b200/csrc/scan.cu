@@ -1042,7 +1042,7 @@ struct BatchCtl {
 // (query, subject) pair sees exactly the plain kernel's sequence of events,
 // so every query's result is its single-query result; counters and records
 // are indexed by segment = query * n_subjects + subject.
-template <typename CellT, bool kCellsSmem, bool kDefer, bool kPacked, typename DiagT>
+template <typename CellT, bool kCellsSmem, bool kDefer, bool kPacked, typename DiagT, bool kProf = false>
 __global__ void __launch_bounds__(kMaxWarps * 32, 1)
 scan_batch_kernel(BatchArgs b, ScanLayout lay) {
     uint8_t* sm = bp_smem;
@@ -1081,6 +1081,13 @@ scan_batch_kernel(BatchArgs b, ScanLayout lay) {
         if (wi.qid != cur_q) {
             const BatchQuery bq = b.queries[wi.qid];
             for (int i = threadIdx.x; i < bq.qlen; i += blockDim.x) qs[i] = bq.query[i];
+            if (kProf) {
+                // this query's profile, right after it (inside the region the
+                // layout sized for the class's longest query)
+                int8_t* pf = reinterpret_cast<int8_t*>(qs + ((bq.qlen + 15) & ~15));
+                for (int i = threadIdx.x; i < bq.qlen * BP_MROW; i += blockDim.x)
+                    pf[i] = b.matrix[(int)__ldg(bq.query + i / BP_MROW) * BP_MROW + i % BP_MROW];
+            }
             if (kCellsSmem) {
                 CellT* c = reinterpret_cast<CellT*>(sm + lay.off_cells);
                 for (int i = threadIdx.x; i <= BP_NC; i += blockDim.x) c[i] = (CellT)bq.cells[i];
@@ -1145,9 +1152,10 @@ scan_batch_kernel(BatchArgs b, ScanLayout lay) {
             if (second && wi.n_long > 0 && eo - so >= b.long_min) continue;   // scanned in the first pass
             // (offset resets clear the launch's whole array, lay.L entries:
             // queries with a longer array than this one read past its end)
-            scan_subject<CellT, kDefer, kPacked>(ctl->args, m, qs, cells, entries, wr.diag, lay.L, wr.lane_pos,
-                                                 wr.tasks, wr.blocked, wr.wcnt, (int)(seg0 + oid - b.subject_first),
-                                                 b.db + so, (int)(eo - so), base, lane);
+            scan_subject<CellT, kDefer, kPacked, DiagT, false, kProf>(ctl->args, m, qs, cells, entries, wr.diag, lay.L,
+                                                                      wr.lane_pos, wr.tasks, wr.blocked, wr.wcnt,
+                                                                      (int)(seg0 + oid - b.subject_first), b.db + so,
+                                                                      (int)(eo - so), base, lane);
         }
         __syncthreads();
     }
@@ -1207,6 +1215,17 @@ ScanLayout make_layout(int qlen, int L, int64_t n_entries, int warps, int cells_
 // 4.38 ms, 500 aa: 6.50 -> 6.38 ms per 1M subjects; at 700 aa it would cost
 // two warps, 8.37 -> 8.76 ms, at 1,000 aa the table's place in shared
 // memory, 12.6 -> 15.3 ms).
+// The same layout with the query's score profile added, at the same warps or
+// one fewer; unchanged when that does not fit (or the array is 32-bit wide).
+ScanLayout with_profile(const ScanLayout& l, int qlen, int64_t n_entries, int smem_optin, bool packed, bool stream) {
+    if (l.L > kNarrowMaxL) return l;
+    for (int wp = l.warps; wp >= l.warps - 1 && wp >= 1; --wp) {
+        const ScanLayout lp = make_layout(qlen, l.L, n_entries, wp, l.cells_mode, l.entries_smem, packed, stream, true);
+        if (lp.total <= smem_optin) return lp;
+    }
+    return l;
+}
+
 bool choose_layout(int qlen, int L, int64_t n_entries, int smem_optin, ScanLayout* out, bool packed = false,
                    bool stream = false) {
     const int cell_modes[2] = {n_entries < 65536 ? 0 : 1, 2};
@@ -1218,14 +1237,8 @@ bool choose_layout(int qlen, int L, int64_t n_entries, int smem_optin, ScanLayou
                     const ScanLayout l = make_layout(qlen, L, n_entries, w, cm, es, packed, stream);
                     if (l.total <= smem_optin) {
                         *out = l;
-                        if (stream && !packed && qlen >= kDeferMinQlen && L <= kNarrowMaxL)
-                            for (int wp = w; wp >= w - 1 && wp >= 1; --wp) {
-                                const ScanLayout lp = make_layout(qlen, L, n_entries, wp, cm, es, packed, stream, true);
-                                if (lp.total <= smem_optin) {
-                                    *out = lp;
-                                    break;
-                                }
-                            }
+                        if (stream && !packed && qlen >= kDeferMinQlen)
+                            *out = with_profile(l, qlen, n_entries, smem_optin, packed, stream);
                         return true;
                     }
                 }
@@ -1262,9 +1275,9 @@ cudaError_t launch_stream(bp_engine* e, cudaStream_t stream, const ScanArgs& a, 
     return cudaGetLastError();
 }
 
-template <typename CellT, bool kCellsSmem, bool kDefer, bool kPacked, typename DiagT>
+template <typename CellT, bool kCellsSmem, bool kDefer, bool kPacked, typename DiagT, bool kProf = false>
 cudaError_t launch_batch(bp_engine* e, cudaStream_t stream, const BatchArgs& b, const ScanLayout& lay, int grid) {
-    auto kern = scan_batch_kernel<CellT, kCellsSmem, kDefer, kPacked, DiagT>;
+    auto kern = scan_batch_kernel<CellT, kCellsSmem, kDefer, kPacked, DiagT, kProf>;
     // the largest allowed size, not this launch's: launches of one instance
     // with different layouts (batch classes, captured graph nodes replayed
     // later) must all stay valid whatever order the attribute was set in
@@ -1302,6 +1315,13 @@ cudaError_t launch_batch_layout(bp_engine* e, cudaStream_t stream, const BatchAr
         return launch_batch<uint32_t, false, true, false, uint32_t>(e, stream, b, lay, grid);
     }
     if (lay.L > kNarrowMaxL) return cudaErrorInvalidValue;   // packed tables are short
+    if constexpr (!kPacked) {
+        if (defer && lay.off_prof) {
+            if (lay.cells_mode == 0) return launch_batch<uint16_t, true, true, false, N, true>(e, stream, b, lay, grid);
+            if (lay.cells_mode == 1) return launch_batch<uint32_t, true, true, false, N, true>(e, stream, b, lay, grid);
+            return launch_batch<uint32_t, false, true, false, N, true>(e, stream, b, lay, grid);
+        }
+    }
     if (defer) {
         if (lay.cells_mode == 0) return launch_batch<uint16_t, true, true, kPacked, N>(e, stream, b, lay, grid);
         if (lay.cells_mode == 1) return launch_batch<uint32_t, true, true, kPacked, N>(e, stream, b, lay, grid);
@@ -1320,6 +1340,7 @@ cudaError_t bp_launch_scan_batch(bp_engine* e, cudaStream_t stream, const BatchA
         lay = make_layout(max_qlen, max_diag_len, max_entries, max_warps, lay.cells_mode, lay.entries_smem, packed);
     }
     const bool defer = max_qlen >= kDeferMinQlen;
+    if (!packed && defer) lay = with_profile(lay, max_qlen, max_entries, e->smem_optin, false, false);
     return packed ? launch_batch_layout<true>(e, stream, b, lay, grid, defer)
                   : launch_batch_layout<false>(e, stream, b, lay, grid, defer);
 }
