@@ -72,6 +72,8 @@ def parse():
     ap.add_argument("--serve-lanes", type=int, default=1)
     ap.add_argument("--serve-depth", type=int, default=4, help="batches queued per lane")
     ap.add_argument("--serve-batch", type=int, default=1, help="queries per batch")
+    ap.add_argument("--serve-segments", type=int, default=8,
+                    help="subject ranges per request in the preemptive run (<= 1: no preemptive run)")
     ap.add_argument("--serve-schedule", default="dynamic", choices=["dynamic", "learned"],
                     help="item schedule of the served batches")
     return ap.parse_args()
@@ -571,18 +573,30 @@ def run_serving(eng, matrix, args):
            "memory_budget_gb": 16}
     runs = {}
     capacity = None
-    plan = [("offered", args.serve_rate, args.serve_requests),
-            ("sustainable", None, args.serve_requests),
-            ("sustainable_shortest_first", None, args.serve_requests)]
+    # (label, offered rate or None for 80 % of the measured capacity, admission, segments)
+    plan = [("offered", args.serve_rate, 0, 1),
+            ("sustainable", None, 0, 1),
+            ("sustainable_shortest_first", None, 1, 1),
+            ("sustainable_preemptive", None, 1, args.serve_segments)]
     if args.serve_rate_high > 0:
-        plan.insert(1, ("offered_high", args.serve_rate_high, args.serve_requests))
-    for label, rate, n in plan:
+        plan.insert(1, ("offered_high", args.serve_rate_high, 0, 1))
+    sustained = None        # the sustainable runs share one set of queries and arrival times
+    n = args.serve_requests
+    for label, rate, admission, segments in plan:
+        if segments > 1 and args.serve_segments <= 1:
+            continue
         if rate is None:
-            rate = 0.8 * capacity
-        qs = synth.serving_queries(rng, n)
-        srv = Server(eng, db, max_batch_queries=max_batch, lanes=lanes, lane_depth=depth, schedule=sched,
-                     model=model, chunk_residues=1 << 20, admission=1 if label.endswith("shortest_first") else 0)
-        arrivals = serving.poisson_arrivals(rng, rate, n)
+            if sustained is None:
+                sustained = (synth.serving_queries(rng, n), serving.poisson_arrivals(rng, 0.8 * capacity, n),
+                             0.8 * capacity)
+            qs, arrivals, rate = sustained
+        else:
+            qs = synth.serving_queries(rng, n)
+            arrivals = serving.poisson_arrivals(rng, rate, n)
+        # ranges of a preemptive run queue at most one behind the running one
+        run_depth = min(depth, 2) if segments > 1 else depth
+        srv = Server(eng, db, max_batch_queries=max_batch, lanes=lanes, lane_depth=run_depth, schedule=sched,
+                     model=model, chunk_residues=1 << 20, admission=admission, segments=segments)
         digests = []
         n_check = min(n, args.serve_check)
         t0 = time.perf_counter()
@@ -602,7 +616,9 @@ def run_serving(eng, matrix, args):
             r.close()
             h.close()
         qres = float(sum(len(q) for q in qs))
-        runs[label] = {"offered_qps": rate, "requests": n, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+        runs[label] = {"offered_qps": rate, "requests": n, "admission": ["arrival", "shortest"][admission],
+                       "segments": segments, "lane_depth": run_depth,
+                       "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
                        "max_ms": st["max_ms"], "throughput_qps": st["queries_per_s"],
                        "value": st["queries_per_s"] * nres, "unit": UNIT,
                        "residue_pairs_per_s": st["resq_per_s"], "batches": st["batches"],

@@ -699,6 +699,20 @@ bp_status bp_batch_digest(bp_batch* b, int32_t qi, uint64_t out[2]) {
     return bp_digest_range(b->e, b->e->stream, b->d_counters + 3 * s0, b->n, b->d_hsp_off + s0, b->d_hsps, out);
 }
 
+}  // extern "C"
+
+bp_status bp_batch_digest_sums(bp_batch* b, int32_t qi, int64_t first, int64_t rec_base, bool last,
+                               uint64_t sums[2]) {
+    if (!b || qi < 0 || qi >= b->nq || !sums) return BP_ERR_INVALID;
+    bp_status st = bp_batch_wait(b);
+    if (st != BP_OK) return st;
+    const size_t s0 = (size_t)qi * b->n;
+    return bp_digest_sums(b->e, b->e->stream, b->d_counters + 3 * s0, b->n, b->d_hsp_off + s0, b->d_hsps, first,
+                          rec_base, last, sums);
+}
+
+extern "C" {
+
 bp_status bp_batch_queue_costs(const bp_batch* b, double* costs, int32_t* n_queues) {
     if (!b || !n_queues) return BP_ERR_INVALID;
     *n_queues = (int32_t)b->queue_cost.size();

@@ -298,3 +298,14 @@ bp_status bp_run_search(bp_engine* e, bp_result* r);
 // for `st` (see digest.cu).
 bp_status bp_digest_range(bp_engine* e, cudaStream_t st, const int32_t* d_counters, int32_t n,
                           const int64_t* d_hsp_off, const bp_hsp* d_hsps, uint64_t out[2]);
+// The raw digest sums of one piece of a result (subjects [first, first + n)
+// of the whole, after rec_base of its records; `last`: the piece ends the
+// result), and the digest of a whole result of n_subjects from the summed
+// sums of its pieces.
+bp_status bp_digest_sums(bp_engine* e, cudaStream_t st, const int32_t* d_counters, int32_t n,
+                         const int64_t* d_hsp_off, const bp_hsp* d_hsps, int64_t first, int64_t rec_base, bool last,
+                         uint64_t sums[2]);
+void bp_digest_finish(const uint64_t sums[2], int64_t n_subjects, uint64_t out[2]);
+// Query qi of a batch as one piece of a larger result (bp_digest_sums).
+bp_status bp_batch_digest_sums(bp_batch* b, int32_t qi, int64_t first, int64_t rec_base, bool last,
+                               uint64_t sums[2]);

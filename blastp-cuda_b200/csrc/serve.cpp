@@ -18,7 +18,13 @@
 //    waits for the batches ahead of it, not for a batch boundary;
 //  * finished batches are noticed by polling their streams; results stay on
 //    the device, in the batch's per-query segments, until the request is
-//    released, which is when its memory returns to the budget.
+//    released, which is when its memory returns to the budget;
+//  * with `segments` > 1, a request is admitted on its own and searched as
+//    that many jobs over consecutive subject ranges; each free slot takes the
+//    next range of the request the admission policy picks (the oldest, or the
+//    one with the least work left), so a short request arriving while a long
+//    one runs waits for one range of it, not for all of it.  Its result stays
+//    in pieces, one per range, and is read back (or digested) piece by piece.
 // Every query's result is its single-query result (the batched kernel scans
 // each (query, subject) pair exactly as the plain kernel does).
 #include <string.h>
@@ -56,6 +62,9 @@ struct Req {
     Job* job = nullptr;
     int index = -1;
     bool released = false;
+    // segment mode: one job per subject range, launched in range order
+    std::vector<Job*> segs;
+    int seg_next = 0, seg_done = 0;
 };
 
 struct Job {
@@ -66,6 +75,7 @@ struct Job {
     int live = 0;             // requests not yet released
     int64_t bytes = 0;
     bool done = false;
+    int seg = -1;             // segment mode: the subject range searched
 };
 
 }  // namespace
@@ -83,6 +93,8 @@ struct bp_server {
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     std::deque<Req*> pending;
+    std::vector<int32_t> seg_first;       // segment mode: range k is subjects [seg_first[k], seg_first[k + 1])
+    std::vector<Req*> active;             // segment mode: admitted requests with ranges left to launch
     std::unordered_map<uint64_t, Req*> reqs;
     uint64_t next_id = 1;
     int64_t mem_used = 0, mem_peak = 0;
@@ -180,6 +192,108 @@ void launch_job(bp_server* s, Job* job) {
     }
 }
 
+// Segment mode: builds the request's table with its first range, then
+// launches one range of it on the job's slot (called without the lock).
+void launch_seg_job(bp_server* s, Job* job) {
+    bp_engine* le = s->slots[job->slot];
+    Req* r = job->reqs[0];
+    bp_status st = BP_OK;
+    if (!r->query) st = bp_query_create(le, r->residues.data(), (int32_t)r->residues.size(), &s->o.params, &r->query);
+    bp_batch_options bo;
+    bp_batch_options_default(&bo);
+    bo.chunk_residues = s->o.chunk_residues > 0 ? s->o.chunk_residues : (1 << 20);
+    bo.schedule = s->o.schedule;
+    bo.use_graph = 0;
+    bo.ctas = std::max(1, le->sm_count / std::max(1, s->n_lanes));
+    bo.subject_first = s->seg_first[job->seg];
+    bo.subject_count = s->seg_first[job->seg + 1] - s->seg_first[job->seg];
+    std::vector<float> costs;
+    if (st == BP_OK && bo.schedule == BP_SCHED_COSTS) {
+        if (!s->o.model) {
+            bo.schedule = BP_SCHED_STATIC;
+        } else {
+            int32_t nc = 0;
+            st = bp_batch_plan(s->db, bo.subject_first, bo.subject_count, bo.chunk_residues, nullptr, &nc);
+            std::vector<int32_t> first((size_t)nc + 1);
+            if (st == BP_OK)
+                st = bp_batch_plan(s->db, bo.subject_first, bo.subject_count, bo.chunk_residues, first.data(), &nc);
+            costs.resize((size_t)nc);
+            const bp_query* q = r->query;
+            if (st == BP_OK)
+                st = bp_batch_predict_costs(le, s->o.model, s->o.cost_weights, s->db, &q, 1, first.data(), nc,
+                                            s->o.planted_density, costs.data());
+            bo.item_costs = costs.data();
+        }
+    }
+    if (st == BP_OK && s->lane_used[job->lane] &&
+        cudaStreamWaitEvent(le->stream, s->lane_tail[job->lane], 0) != cudaSuccess) {
+        cudaGetLastError();
+        st = BP_ERR_CUDA;
+    }
+    const bp_query* q = r->query;
+    if (st == BP_OK) st = bp_search_batch(le, s->db, &q, 1, &bo, &job->batch);
+    if (st == BP_OK) {
+        if (cudaEventRecord(s->lane_tail[job->lane], le->stream) == cudaSuccess) {
+            s->lane_used[job->lane] = true;
+        } else {
+            cudaGetLastError();
+            st = BP_ERR_CUDA;
+        }
+    }
+    std::lock_guard<std::mutex> lock(s->mu);
+    r->index = 0;
+    if (st == BP_OK) {
+        if (r->state == BP_REQ_ADMITTED) {
+            r->state = BP_REQ_RUNNING;
+            r->t_start = now_ms();
+        }
+        return;
+    }
+    job->done = true;
+    if (r->state == BP_REQ_ADMITTED || r->state == BP_REQ_RUNNING) {
+        fail_request(s, r, st);
+        s->in_flight -= 1;
+        s->active.erase(std::remove(s->active.begin(), s->active.end(), r), s->active.end());
+    }
+    s->cv_done.notify_all();
+}
+
+// Segment mode: every launched range of the request has finished.
+bool segs_finished(const Req* r) {
+    for (const Job* j : r->segs)
+        if (!j->done) return false;
+    return true;
+}
+
+// Segment mode: frees a released request whose launched ranges have all finished.
+void retire_segmented(bp_server* s, Req* r) {
+    for (Job* j : r->segs) {
+        bp_batch_destroy(j->batch);
+        delete j;
+    }
+    r->segs.clear();
+    bp_query_destroy(r->query);
+    r->query = nullptr;
+    s->mem_used -= r->bytes;
+    s->reqs.erase(r->id);
+    delete r;
+}
+
+// Segment mode: the request whose next range a free slot takes -- the
+// earliest admitted, or the one with the least work left (ranges left x
+// query length plus the per-letter-independent share of a scan, about 64
+// letters' worth), earliest among equals.
+Req* next_segment_request(bp_server* s) {
+    if (s->active.empty()) return nullptr;
+    const int n_seg = (int)s->seg_first.size() - 1;
+    Req* best = s->active.front();
+    if (s->o.admission != BP_ADMIT_SHORTEST) return best;
+    auto left = [n_seg](const Req* r) { return (double)(n_seg - r->seg_next) * ((double)r->residues.size() + 64.0); };
+    for (Req* r : s->active)
+        if (left(r) < left(best)) best = r;
+    return best;
+}
+
 // Frees a job whose requests have all been released.
 void retire_job(bp_server* s, Job* job) {
     bp_batch_destroy(job->batch);
@@ -193,9 +307,105 @@ void retire_job(bp_server* s, Job* job) {
     delete job;
 }
 
+// Segment mode: a slot still holds one of the request's jobs.
+bool seg_on_slot(const bp_server* s, const Req* r) {
+    for (const Job* j : r->segs)
+        if (std::find(s->slot_job.begin(), s->slot_job.end(), j) != s->slot_job.end()) return true;
+    return false;
+}
+
+// Segment mode: one dispatcher round -- finished ranges, admissions (every
+// queued request that fits the budget), and a range for every free slot.
+bool dispatch_segments(bp_server* s, std::unique_lock<std::mutex>& lock) {
+    bool worked = false;
+    const int n_seg = (int)s->seg_first.size() - 1;
+    for (size_t l = 0; l < s->slots.size(); ++l) {
+        Job* job = s->slot_job[l];
+        if (!job) continue;
+        Req* r = job->reqs[0];
+        if (!job->done) {
+            if (cudaStreamQuery(s->slots[l]->stream) == cudaErrorNotReady) continue;
+            cudaGetLastError();
+            lock.unlock();
+            const bp_status st = bp_batch_wait(job->batch);   // re-runs on record overflow
+            lock.lock();
+            job->done = true;
+            if (r->state == BP_REQ_RUNNING || r->state == BP_REQ_ADMITTED) {
+                if (st != BP_OK) {
+                    fail_request(s, r, st);
+                    s->in_flight -= 1;
+                    s->active.erase(std::remove(s->active.begin(), s->active.end(), r), s->active.end());
+                } else if (++r->seg_done == n_seg) {
+                    const double t = now_ms();
+                    r->state = BP_REQ_DONE;
+                    r->t_done = t;
+                    s->latency_ms.push_back(r->t_done - r->t_arrive);
+                    s->n_done += 1;
+                    s->resq += (double)r->residues.size() * (double)s->db->nres;
+                    s->t_last = std::max(s->t_last, t);
+                    s->in_flight -= 1;
+                }
+            }
+            s->cv_done.notify_all();
+            worked = true;
+        }
+        s->slot_job[l] = nullptr;
+        if (r->released && segs_finished(r) && !seg_on_slot(s, r)) retire_segmented(s, r);
+    }
+    while (!s->pending.empty()) {
+        auto pick = s->pending.begin();
+        if (s->o.admission == BP_ADMIT_SHORTEST)
+            for (auto it = s->pending.begin(); it != s->pending.end(); ++it)
+                if ((*it)->residues.size() < (*pick)->residues.size()) pick = it;
+        Req* r = *pick;
+        if (s->mem_used + r->bytes > s->o.device_memory_budget && s->mem_used > 0) break;
+        s->pending.erase(pick);
+        r->state = BP_REQ_ADMITTED;
+        s->mem_used += r->bytes;
+        s->mem_peak = std::max(s->mem_peak, s->mem_used);
+        s->in_flight += 1;
+        s->max_in_flight = std::max(s->max_in_flight, s->in_flight);
+        s->active.push_back(r);
+        worked = true;
+    }
+    for (int pass = 0; pass < s->depth && !s->active.empty(); ++pass)
+        for (size_t l = 0; l < (size_t)s->n_lanes && !s->active.empty(); ++l) {
+            int slot = -1;
+            for (int k = 0; k < s->depth && slot < 0; ++k)
+                if (!s->slot_job[l * s->depth + k]) slot = (int)l * s->depth + k;
+            if (slot < 0) continue;
+            Req* r = next_segment_request(s);
+            Job* job = new Job();
+            job->lane = (int)l;
+            job->slot = slot;
+            job->reqs.push_back(r);
+            job->live = 1;
+            job->seg = r->seg_next++;
+            r->segs.push_back(job);
+            if (r->seg_next == n_seg) s->active.erase(std::find(s->active.begin(), s->active.end(), r));
+            s->slot_job[slot] = job;
+            s->n_batches += 1;
+            s->batched_queries += 1;
+            lock.unlock();
+            launch_seg_job(s, job);
+            lock.lock();
+            if (job->done) {                 // failed to launch
+                s->slot_job[slot] = nullptr;
+                if (r->released && segs_finished(r) && !seg_on_slot(s, r)) retire_segmented(s, r);
+            }
+            worked = true;
+        }
+    return worked;
+}
+
 void dispatcher(bp_server* s) {
     std::unique_lock<std::mutex> lock(s->mu);
     while (!s->stop) {
+        if (s->seg_first.size() > 2) {
+            if (!dispatch_segments(s, lock))
+                s->cv_work.wait_for(lock, std::chrono::microseconds(s->o.poll_us > 0 ? s->o.poll_us : 200));
+            continue;
+        }
         bool worked = false;
         // completions (a slot's stream holds its own batch only)
         for (size_t l = 0; l < s->slots.size(); ++l) {
@@ -293,6 +503,7 @@ void bp_server_options_default(bp_server_options* o) {
     o->lanes = 2;
     o->lane_depth = 1;
     o->admission = BP_ADMIT_ARRIVAL;
+    o->segments = 1;
     o->poll_us = 200;
     bp_params_default(&o->params);
 }
@@ -306,10 +517,24 @@ bp_status bp_server_create(bp_engine* e, const bp_db* db, const bp_server_option
     if (opt) s->o = *opt;
     else bp_server_options_default(&s->o);
     if (s->o.lanes < 1 || s->o.lanes > 16 || s->o.max_batch_queries < 1 || s->o.lane_depth < 1 ||
-        s->o.lane_depth > 16 || (s->o.admission != BP_ADMIT_ARRIVAL && s->o.admission != BP_ADMIT_SHORTEST)) {
+        s->o.lane_depth > 16 || (s->o.admission != BP_ADMIT_ARRIVAL && s->o.admission != BP_ADMIT_SHORTEST) ||
+        s->o.segments < 1 || s->o.segments > 64) {
         delete s;
         return bp_set_error(e, BP_ERR_INVALID,
-                            "bp_server_create: lanes and lane_depth must be 1..16, max_batch_queries >= 1");
+                            "bp_server_create: lanes and lane_depth must be 1..16, max_batch_queries >= 1, "
+                            "segments 1..64");
+    }
+    if (s->o.segments > 1 && db->n > 0) {
+        // consecutive subject ranges of about equal residues (empty ones dropped)
+        s->seg_first.push_back(0);
+        for (int k = 1; k <= s->o.segments; ++k) {
+            const int64_t target = db->nres * k / s->o.segments;
+            int32_t i = (int32_t)(std::lower_bound(db->h_off.begin(), db->h_off.end(), target) - db->h_off.begin());
+            if (k == s->o.segments) i = db->n;
+            i = std::min(std::max(i, s->seg_first.back()), db->n);
+            if (i > s->seg_first.back()) s->seg_first.push_back(i);
+        }
+        if (s->seg_first.back() != db->n) s->seg_first.push_back(db->n);
     }
     s->n_lanes = s->o.lanes;
     s->depth = s->o.lane_depth;
@@ -383,6 +608,7 @@ bp_status bp_server_result(bp_server* s, uint64_t ticket, int32_t* counters, int
     if (!s) return BP_ERR_INVALID;
     Job* job = nullptr;
     int index = -1;
+    std::vector<bp_batch*> pieces;
     {
         std::lock_guard<std::mutex> lock(s->mu);
         auto it = s->reqs.find(ticket);
@@ -393,15 +619,32 @@ bp_status bp_server_result(bp_server* s, uint64_t ticket, int32_t* counters, int
         if (latency_ms) *latency_ms = r->t_done - r->t_arrive;
         job = r->job;
         index = r->index;
+        for (Job* j : r->segs) pieces.push_back(j->batch);
     }
-    // the job cannot be retired before this request is released
-    return bp_batch_copy_query(job->batch, index, counters, hsp_off, hsps, n_hsps);
+    // the jobs cannot be retired before this request is released
+    if (pieces.empty()) return bp_batch_copy_query(job->batch, index, counters, hsp_off, hsps, n_hsps);
+    // segment mode: range k's piece goes to subjects [seg_first[k], seg_first[k + 1]), its
+    // records after those of the ranges before it
+    int64_t base = 0;
+    for (size_t k = 0; k < pieces.size(); ++k) {
+        const int32_t f = s->seg_first[k];
+        int64_t nh = 0;
+        const bp_status st = bp_batch_copy_query(pieces[k], 0, counters ? counters + 3 * (int64_t)f : nullptr,
+                                                 hsp_off ? hsp_off + f : nullptr, hsps ? hsps + base : nullptr, &nh);
+        if (st != BP_OK) return st;
+        if (hsp_off)
+            for (int32_t i = f; i <= s->seg_first[k + 1]; ++i) hsp_off[i] += base;
+        base += nh;
+    }
+    if (n_hsps) *n_hsps = base;
+    return BP_OK;
 }
 
 bp_status bp_server_digest(bp_server* s, uint64_t ticket, uint64_t out[2]) {
     if (!s || !out) return BP_ERR_INVALID;
     Job* job = nullptr;
     int index = -1;
+    std::vector<bp_batch*> pieces;
     {
         std::lock_guard<std::mutex> lock(s->mu);
         auto it = s->reqs.find(ticket);
@@ -411,8 +654,24 @@ bp_status bp_server_digest(bp_server* s, uint64_t ticket, uint64_t out[2]) {
         if (r->state != BP_REQ_DONE) return BP_ERR_NOT_READY;
         job = r->job;
         index = r->index;
+        for (Job* j : r->segs) pieces.push_back(j->batch);
     }
-    return bp_batch_digest(job->batch, index, out);
+    if (pieces.empty()) return bp_batch_digest(job->batch, index, out);
+    // segment mode: the pieces' sums at their places in the whole result
+    uint64_t sums[2] = {0, 0};
+    int64_t base = 0;
+    for (size_t k = 0; k < pieces.size(); ++k) {
+        int64_t nh = 0;
+        bp_status st = bp_batch_copy_query(pieces[k], 0, nullptr, nullptr, nullptr, &nh);
+        uint64_t part[2];
+        if (st == BP_OK) st = bp_batch_digest_sums(pieces[k], 0, s->seg_first[k], base, k + 1 == pieces.size(), part);
+        if (st != BP_OK) return st;
+        sums[0] += part[0];
+        sums[1] += part[1];
+        base += nh;
+    }
+    bp_digest_finish(sums, s->db->n, out);
+    return BP_OK;
 }
 
 bp_status bp_server_release(bp_server* s, uint64_t ticket) {
@@ -424,6 +683,11 @@ bp_status bp_server_release(bp_server* s, uint64_t ticket) {
     if (r->state != BP_REQ_DONE && r->state != BP_REQ_FAILED) return BP_ERR_NOT_READY;
     if (r->released) return BP_ERR_INVALID;
     r->released = true;
+    if (!r->segs.empty()) {                      // segment mode
+        if (segs_finished(r) && !seg_on_slot(s, r)) retire_segmented(s, r);
+        s->cv_work.notify_one();
+        return BP_OK;
+    }
     Job* job = r->job;
     if (!job) {                                  // failed before admission
         s->reqs.erase(it);
@@ -475,6 +739,19 @@ void bp_server_destroy(bp_server* s) {
     s->cv_work.notify_all();
     if (s->th.joinable()) s->th.join();
     // release everything still held
+    std::vector<Req*> segmented;
+    for (auto& kv : s->reqs)
+        if (!kv.second->segs.empty()) segmented.push_back(kv.second);
+    for (Req* r : segmented) {
+        for (Job* j : r->segs) {
+            bp_batch_destroy(j->batch);
+            delete j;
+        }
+        r->segs.clear();
+        bp_query_destroy(r->query);
+        s->reqs.erase(r->id);
+        delete r;
+    }
     std::vector<Job*> jobs;
     for (auto& kv : s->reqs)
         if (kv.second->job && std::find(jobs.begin(), jobs.end(), kv.second->job) == jobs.end())

@@ -397,6 +397,15 @@ typedef struct {
     int32_t admission;              /* BP_ADMIT_ARRIVAL (default) or BP_ADMIT_SHORTEST: the shortest
                                        waiting query is admitted first (lower median latency under
                                        load, longer waits for long queries) */
+    int32_t segments;               /* 1 (default): a request's search is one job over the whole
+                                       database.  2..64: it runs as this many jobs over consecutive
+                                       subject ranges of about equal residues, one query each, and
+                                       every free slot takes the next range of the request chosen by
+                                       `admission` -- arrival order, or (BP_ADMIT_SHORTEST) the least
+                                       remaining work (ranges left x query length), so a short
+                                       request that arrives while a long one runs goes ahead of the
+                                       long one's remaining ranges.  max_batch_queries is not used.
+                                       Results are the same either way. */
 } bp_server_options;
 
 enum { BP_ADMIT_ARRIVAL = 0, BP_ADMIT_SHORTEST = 1 };

@@ -178,3 +178,76 @@ def test_shortest_first_admission(engine, matrix):
         # waiting is longest first: arrival order keeps it, shortest-first reverses it
         assert order == (list(range(6)) if policy == ADMIT_ARRIVAL else list(range(5, -1, -1))), (policy, done)
     d.close()
+
+
+@pytest.mark.parametrize("admission", [0, 1])
+def test_segmented_requests_equal_alone(engine, world, admission):
+    # each request searched as 4 jobs over consecutive subject ranges, the
+    # ranges of different requests interleaved on one lane: every result (read
+    # back piece by piece) and every digest equals the plain search alone
+    qs, db, d, alone = world
+    srv = Server(engine, d, lanes=1, lane_depth=2, segments=4, admission=admission, chunk_residues=1 << 16)
+    arr = serving.poisson_arrivals(np.random.default_rng(5), 3000.0, 12)
+    digs = []
+    results, lat, _ = serving.drive(srv, qs[:12], arr, digests=digs, digest_first=12)
+    _check(results, alone[:12], "segmented")
+    for i in range(12):
+        h = engine.query(qs[i])
+        r = engine.search(d, h)
+        assert digs[i] == r.digest(), "request %d" % i
+        r.close()
+        h.close()
+    st = srv.stats()
+    assert st["completed"] == 12 and st["failed"] == 0
+    assert st["batches"] == 12 * 4            # one job per range
+    assert st["mem_used"] == 0
+    srv.close()
+
+
+def test_segmented_shortest_first_preempts_a_long_request(engine, matrix):
+    # a long request running range by range while six short ones arrive:
+    # with the least-work-left policy the short ones go ahead of the long
+    # one's remaining ranges and all finish before it; in arrival order the
+    # long one finishes first
+    import time
+    from blastp_b200._lib import ADMIT_ARRIVAL, ADMIT_SHORTEST
+    rng = np.random.default_rng(78)
+    head = synth.residues(rng, 2000)
+    short = [synth.residues(rng, n) for n in (120, 90, 150, 60, 100, 80)]
+    db = synth.make_database(rng, 400_000, [head], 0.001, (60, 150), (0.3, 0.5), matrix)
+    d = engine.database(db.residues, db.offsets)
+    plain = []
+    for q in [head] + short:
+        h = engine.query(q)
+        r = engine.search(d, h)
+        plain.append(r.digest())
+        r.close()
+        h.close()
+    for policy in (ADMIT_ARRIVAL, ADMIT_SHORTEST):
+        srv = Server(engine, d, lanes=1, lane_depth=1, segments=8, admission=policy, chunk_residues=1 << 20,
+                     poll_us=50)
+        t0 = time.perf_counter()
+        first = srv.submit(head)
+        while srv.state(first) < 2:             # until its first range runs
+            pass
+        offs, tickets = [], []
+        for q in short:
+            offs.append((time.perf_counter() - t0) * 1e3)
+            tickets.append(srv.submit(q))
+        submitted = (time.perf_counter() - t0) * 1e3
+        srv.wait(first)
+        head_end = srv.latency(first)
+        assert srv.digest(first) == plain[0]
+        ends = []
+        for i, t in enumerate(tickets):
+            srv.wait(t)
+            assert srv.digest(t) == plain[1 + i], "policy %d request %d" % (policy, i)
+            ends.append(offs[i] + srv.latency(t))
+        srv.close()
+        if head_end <= submitted:
+            pytest.skip("the long request finished before the short ones were submitted")
+        if policy == ADMIT_SHORTEST:
+            assert max(ends) < head_end, (ends, head_end)
+        else:
+            assert min(ends) > head_end, (ends, head_end)
+    d.close()
