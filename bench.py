@@ -67,6 +67,8 @@ def parse():
     ap.add_argument("--serve-subjects", type=int, default=5_000_000)
     ap.add_argument("--serve-requests", type=int, default=128)
     ap.add_argument("--serve-rate", type=float, default=1000.0, help="offered load, queries/s (Poisson)")
+    ap.add_argument("--serve-sustained-requests", type=int, default=384,
+                    help="requests of each run at 80 %% of the measured capacity")
     ap.add_argument("--serve-check", type=int, default=32, help="served requests checked against plain searches")
     ap.add_argument("--serve-rate-high", type=float, default=5000.0, help="second offered load (0: skip)")
     ap.add_argument("--serve-lanes", type=int, default=1)
@@ -581,8 +583,8 @@ def run_serving(eng, matrix, args):
     if args.serve_rate_high > 0:
         plan.insert(1, ("offered_high", args.serve_rate_high, 0, 1))
     sustained = None        # the sustainable runs share one set of queries and arrival times
-    n = args.serve_requests
     for label, rate, admission, segments in plan:
+        n = args.serve_requests if rate is not None else args.serve_sustained_requests
         if segments > 1 and args.serve_segments <= 1:
             continue
         if rate is None:

@@ -55,6 +55,7 @@ struct bp_batch {
     int64_t* d_blocksums = nullptr;          // later search may regrow
     uint32_t* d_counts = nullptr;            // [0] records, [1] item cursor
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t wait_first = nullptr;   // the first launch's device work waits for this event
     uint64_t launches_per_run = 0;
     float last_ms = 0.f;
     uint32_t* h_count = nullptr;
@@ -254,6 +255,12 @@ bp_status capture(bp_batch* b) {
 bp_status launch_batch(bp_batch* b) {
     bp_engine* e = b->e;
     b->n_hsps = -1;
+    if (b->wait_first) {
+        // after the host tables' copies: those come from pageable memory and
+        // would hold the host until the stream reached them
+        CKB(cudaStreamWaitEvent(e->stream, b->wait_first, 0), "cudaStreamWaitEvent");
+        b->wait_first = nullptr;
+    }
     if (b->opt.use_graph) {
         if (!b->exec) {
             bp_status st = capture(b);
@@ -370,6 +377,13 @@ bp_status bp_batch_plan(const bp_db* db, int32_t subject_first, int32_t subject_
 
 bp_status bp_search_batch(bp_engine* e, const bp_db* db, const bp_query* const* queries, int32_t n_queries,
                           const bp_batch_options* opt, bp_batch** out) {
+    return bp_search_batch_behind(e, db, queries, n_queries, opt, nullptr, out);
+}
+
+}  // extern "C"
+
+bp_status bp_search_batch_behind(bp_engine* e, const bp_db* db, const bp_query* const* queries, int32_t n_queries,
+                                 const bp_batch_options* opt, cudaEvent_t after, bp_batch** out) {
     if (!e || !db || !queries || n_queries < 0 || !out) return bp_set_error(e, BP_ERR_INVALID, "bp_search_batch: bad argument");
     *out = nullptr;
     bp_batch_options o;
@@ -620,6 +634,7 @@ bp_status bp_search_batch(bp_engine* e, const bp_db* db, const bp_query* const* 
         return bp_set_cuda_error(e, err, "bp_search_batch: allocate");
     }
     bp_status st = prepare(b);
+    b->wait_first = after;
     if (st == BP_OK) st = launch_batch(b);
     if (st != BP_OK) {
         bp_batch_destroy(b);
@@ -628,6 +643,8 @@ bp_status bp_search_batch(bp_engine* e, const bp_db* db, const bp_query* const* 
     *out = b;
     return BP_OK;
 }
+
+extern "C" {
 
 bp_status bp_batch_run(bp_batch* b) {
     if (!b) return BP_ERR_INVALID;
@@ -658,8 +675,14 @@ bp_status bp_batch_wait(bp_batch* b) {
         bp_status st = prepare(b);
         if (st == BP_OK && b->opt.use_graph) st = capture(b);   // buffers moved: capture again
         if (st == BP_OK) st = launch_batch(b);
-        if (st != BP_OK) return st;
+        if (st != BP_OK) {
+            cudaStreamSynchronize(e->stream);   // nothing of the batch left running
+            cudaGetLastError();
+            return st;
+        }
     }
+    cudaStreamSynchronize(e->stream);
+    cudaGetLastError();
     return bp_set_error(e, BP_ERR_CUDA, "bp_batch_wait: record buffer kept overflowing");
 }
 
@@ -733,6 +756,18 @@ void bp_batch_destroy(bp_batch* b) {
         cudaSetDevice(e->device);
         cudaStreamSynchronize(e->stream);
     }
+    bp_batch_destroy_finished(b);
+}
+
+}  // extern "C"
+
+// The batch's work has completed (bp_batch_wait returned): its memory goes
+// back stream-ordered without waiting for whatever the engine's stream runs
+// now.
+void bp_batch_destroy_finished(bp_batch* b) {
+    if (!b) return;
+    bp_engine* e = b->e;
+    if (e) cudaSetDevice(e->device);
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
     for (void* p : {(void*)b->d_queries, (void*)b->d_items, (void*)b->d_queue_off, (void*)b->d_queue_items,
@@ -750,9 +785,6 @@ void bp_batch_destroy(bp_batch* b) {
     cudaGetLastError();
     delete b;
 }
-
-
-}  // extern "C"
 
 // ---- cost prediction and autotuning ---------------------------------------
 

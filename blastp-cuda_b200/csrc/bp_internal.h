@@ -306,6 +306,14 @@ bp_status bp_digest_sums(bp_engine* e, cudaStream_t st, const int32_t* d_counter
                          const int64_t* d_hsp_off, const bp_hsp* d_hsps, int64_t first, int64_t rec_base, bool last,
                          uint64_t sums[2]);
 void bp_digest_finish(const uint64_t sums[2], int64_t n_subjects, uint64_t out[2]);
+// bp_search_batch whose device work starts only after `after` (an event
+// recorded on another stream; null: none); the host-side setup and the
+// uploads of its tables do not wait for it.
+bp_status bp_search_batch_behind(bp_engine* e, const bp_db* db, const bp_query* const* queries, int32_t n_queries,
+                                 const bp_batch_options* opt, cudaEvent_t after, bp_batch** out);
+// Frees a batch whose work has completed without synchronising its engine's
+// stream (which may already run other work).
+void bp_batch_destroy_finished(bp_batch* b);
 // Query qi of a batch as one piece of a larger result (bp_digest_sums).
 bp_status bp_batch_digest_sums(bp_batch* b, int32_t qi, int64_t first, int64_t rec_base, bool last,
                                uint64_t sums[2]);

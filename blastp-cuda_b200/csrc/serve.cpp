@@ -160,12 +160,9 @@ void launch_job(bp_server* s, Job* job) {
         }
     }
     // behind the lane's previous batch on the device, then this one becomes the lane's tail
-    if (st == BP_OK && s->lane_used[job->lane] &&
-        cudaStreamWaitEvent(le->stream, s->lane_tail[job->lane], 0) != cudaSuccess) {
-        cudaGetLastError();
-        st = BP_ERR_CUDA;
-    }
-    if (st == BP_OK) st = bp_search_batch(le, s->db, qs.data(), (int32_t)qs.size(), &bo, &job->batch);
+    if (st == BP_OK)
+        st = bp_search_batch_behind(le, s->db, qs.data(), (int32_t)qs.size(), &bo,
+                                    s->lane_used[job->lane] ? s->lane_tail[job->lane] : nullptr, &job->batch);
     if (st == BP_OK) {
         if (cudaEventRecord(s->lane_tail[job->lane], le->stream) == cudaSuccess) {
             s->lane_used[job->lane] = true;
@@ -225,13 +222,10 @@ void launch_seg_job(bp_server* s, Job* job) {
             bo.item_costs = costs.data();
         }
     }
-    if (st == BP_OK && s->lane_used[job->lane] &&
-        cudaStreamWaitEvent(le->stream, s->lane_tail[job->lane], 0) != cudaSuccess) {
-        cudaGetLastError();
-        st = BP_ERR_CUDA;
-    }
     const bp_query* q = r->query;
-    if (st == BP_OK) st = bp_search_batch(le, s->db, &q, 1, &bo, &job->batch);
+    if (st == BP_OK)
+        st = bp_search_batch_behind(le, s->db, &q, 1, &bo, s->lane_used[job->lane] ? s->lane_tail[job->lane] : nullptr,
+                                    &job->batch);
     if (st == BP_OK) {
         if (cudaEventRecord(s->lane_tail[job->lane], le->stream) == cudaSuccess) {
             s->lane_used[job->lane] = true;
@@ -268,7 +262,7 @@ bool segs_finished(const Req* r) {
 // Segment mode: frees a released request whose launched ranges have all finished.
 void retire_segmented(bp_server* s, Req* r) {
     for (Job* j : r->segs) {
-        bp_batch_destroy(j->batch);
+        bp_batch_destroy_finished(j->batch);
         delete j;
     }
     r->segs.clear();
@@ -296,7 +290,7 @@ Req* next_segment_request(bp_server* s) {
 
 // Frees a job whose requests have all been released.
 void retire_job(bp_server* s, Job* job) {
-    bp_batch_destroy(job->batch);
+    bp_batch_destroy_finished(job->batch);   // the slot's stream may already run another batch
     for (Req* r : job->reqs) {
         bp_query_destroy(r->query);
         r->query = nullptr;
