@@ -30,28 +30,55 @@ def drive(server, queries, arrivals, keep_results: bool = True, release: bool = 
           digest_first: int = 0):
     """Submits queries[i] at arrivals[i] (seconds after the call), waits for
     all, and returns (results or None, latencies in ms, submit lateness in ms).
-    With a list as `digests`, the result digests of the first `digest_first`
-    requests are appended to it (taken after every request was submitted, so
-    they do not delay submissions)."""
-    t0 = time.perf_counter()
-    tickets, late = [], []
-    for q, at in zip(queries, arrivals):
-        d = at - (time.perf_counter() - t0)
-        if d > 0:
-            time.sleep(d)
-        late.append(max(0.0, (time.perf_counter() - t0 - at) * 1e3))
-        tickets.append(server.submit(q))
-    results, lat = [], []
-    for i, t in enumerate(tickets):
-        server.wait(t)
+    With `release`, every request is collected (result or latency, digest)
+    and released as soon as it finishes, also between submissions, the way a
+    serving client frees what it has read: results held by the server count
+    against its device-memory budget.  With a list as `digests`, the result
+    digests of the first `digest_first` requests are appended to it, in
+    request order."""
+    n = len(queries)
+    results = [None] * n
+    lat = np.zeros(n)
+    got = {}
+    tickets, late, open_ = [], [], []
+
+    def collect(i):
+        t = tickets[i]
         if digests is not None and i < digest_first:
-            digests.append(server.digest(t))
+            got[i] = server.digest(t)
         if keep_results:
-            r, ms = server.result(t)
-            results.append(r)
+            results[i], lat[i] = server.result(t)
         else:
-            ms = server.latency(t)
-        lat.append(ms)
+            lat[i] = server.latency(t)
         if release:
             server.release(t)
-    return (results if keep_results else None), np.array(lat), np.array(late)
+
+    def poll():
+        still = []
+        for i in open_:
+            if server.state(tickets[i]) >= 3:      # done or failed
+                collect(i)
+            else:
+                still.append(i)
+        open_[:] = still
+
+    t0 = time.perf_counter()
+    for i, (q, at) in enumerate(zip(queries, arrivals)):
+        while True:
+            d = at - (time.perf_counter() - t0)
+            if d <= 0:
+                break
+            if release and open_:
+                poll()
+                d = at - (time.perf_counter() - t0)
+            if d > 0:
+                time.sleep(min(d, 0.001) if release and open_ else d)
+        late.append(max(0.0, (time.perf_counter() - t0 - at) * 1e3))
+        tickets.append(server.submit(q))
+        open_.append(i)
+    for i in open_:
+        server.wait(tickets[i])
+        collect(i)
+    if digests is not None:
+        digests.extend(got[i] for i in range(min(digest_first, n)))
+    return (results if keep_results else None), lat, np.array(late)

@@ -724,14 +724,18 @@ bp_status bp_batch_digest(bp_batch* b, int32_t qi, uint64_t out[2]) {
 
 }  // extern "C"
 
-bp_status bp_batch_digest_sums(bp_batch* b, int32_t qi, int64_t first, int64_t rec_base, bool last,
-                               uint64_t sums[2]) {
+bp_status bp_batch_digest_sums(bp_batch* b, int32_t qi, bp_engine* e, cudaStream_t st, int64_t first,
+                               int64_t rec_base, bool last, uint64_t sums[2]) {
     if (!b || qi < 0 || qi >= b->nq || !sums) return BP_ERR_INVALID;
-    bp_status st = bp_batch_wait(b);
-    if (st != BP_OK) return st;
+    bp_status s = bp_batch_wait(b);
+    if (s != BP_OK) return s;
+    if (!e) {
+        e = b->e;
+        st = e->stream;
+    }
     const size_t s0 = (size_t)qi * b->n;
-    return bp_digest_sums(b->e, b->e->stream, b->d_counters + 3 * s0, b->n, b->d_hsp_off + s0, b->d_hsps, first,
-                          rec_base, last, sums);
+    return bp_digest_sums(e, st, b->d_counters + 3 * s0, b->n, b->d_hsp_off + s0, b->d_hsps, first, rec_base, last,
+                          sums);
 }
 
 extern "C" {

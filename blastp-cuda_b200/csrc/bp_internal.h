@@ -314,6 +314,8 @@ bp_status bp_search_batch_behind(bp_engine* e, const bp_db* db, const bp_query* 
 // Frees a batch whose work has completed without synchronising its engine's
 // stream (which may already run other work).
 void bp_batch_destroy_finished(bp_batch* b);
-// Query qi of a batch as one piece of a larger result (bp_digest_sums).
-bp_status bp_batch_digest_sums(bp_batch* b, int32_t qi, int64_t first, int64_t rec_base, bool last,
-                               uint64_t sums[2]);
+// Query qi of a finished batch as one piece of a larger result
+// (bp_digest_sums), computed with engine e's scratch on stream st (e null:
+// the batch's own engine and stream).
+bp_status bp_batch_digest_sums(bp_batch* b, int32_t qi, bp_engine* e, cudaStream_t st, int64_t first,
+                               int64_t rec_base, bool last, uint64_t sums[2]);

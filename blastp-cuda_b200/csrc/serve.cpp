@@ -95,6 +95,8 @@ struct bp_server {
     std::deque<Req*> pending;
     std::vector<int32_t> seg_first;       // segment mode: range k is subjects [seg_first[k], seg_first[k + 1])
     std::vector<Req*> active;             // segment mode: admitted requests with ranges left to launch
+    cudaStream_t readback = nullptr;      // digests of finished requests (with e's scratch)
+    std::mutex readback_mu;
     std::unordered_map<uint64_t, Req*> reqs;
     uint64_t next_id = 1;
     int64_t mem_used = 0, mem_peak = 0;
@@ -187,6 +189,31 @@ void launch_job(bp_server* s, Job* job) {
         job->done = true;
         s->cv_done.notify_all();
     }
+}
+
+// The queued request to admit next, or pending.end() when none may go now
+// (`extra`: bytes already taken by the batch being formed).  Arrival order:
+// the oldest, when it fits the budget.  Shortest first: the shortest, when it
+// fits together with every request queued before it -- so memory stays for
+// the older requests it overtakes, and a client that waits for its requests
+// in submission order (holding the results of later ones) cannot stall the
+// server -- else the oldest.  A lone request on an idle server always goes.
+std::deque<Req*>::iterator pick_pending(bp_server* s, int64_t extra) {
+    auto oldest = s->pending.begin();
+    if (oldest == s->pending.end()) return oldest;
+    const int64_t room = s->o.device_memory_budget - s->mem_used - extra;
+    if (s->o.admission == BP_ADMIT_SHORTEST) {
+        auto best = oldest;
+        for (auto it = s->pending.begin(); it != s->pending.end(); ++it)
+            if ((*it)->residues.size() < (*best)->residues.size()) best = it;
+        if (best != oldest) {
+            int64_t need = (*best)->bytes;
+            for (auto it = oldest; it != best; ++it) need += (*it)->bytes;
+            if (need <= room) return best;
+        }
+    }
+    if ((*oldest)->bytes <= room || (extra == 0 && s->mem_used == 0)) return oldest;
+    return s->pending.end();
 }
 
 // Segment mode: builds the request's table with its first range, then
@@ -347,12 +374,9 @@ bool dispatch_segments(bp_server* s, std::unique_lock<std::mutex>& lock) {
         if (r->released && segs_finished(r) && !seg_on_slot(s, r)) retire_segmented(s, r);
     }
     while (!s->pending.empty()) {
-        auto pick = s->pending.begin();
-        if (s->o.admission == BP_ADMIT_SHORTEST)
-            for (auto it = s->pending.begin(); it != s->pending.end(); ++it)
-                if ((*it)->residues.size() < (*pick)->residues.size()) pick = it;
+        auto pick = pick_pending(s, 0);
+        if (pick == s->pending.end()) break;
         Req* r = *pick;
-        if (s->mem_used + r->bytes > s->o.device_memory_budget && s->mem_used > 0) break;
         s->pending.erase(pick);
         r->state = BP_REQ_ADMITTED;
         s->mem_used += r->bytes;
@@ -444,15 +468,9 @@ void dispatcher(bp_server* s) {
             job->lane = (int)l;
             job->slot = slot;
             while (!s->pending.empty() && (int)job->reqs.size() < s->o.max_batch_queries) {
-                // arrival order, or the shortest query waiting (earliest among equals)
-                auto pick = s->pending.begin();
-                if (s->o.admission == BP_ADMIT_SHORTEST)
-                    for (auto it = s->pending.begin(); it != s->pending.end(); ++it)
-                        if ((*it)->residues.size() < (*pick)->residues.size()) pick = it;
+                auto pick = pick_pending(s, job->bytes);
+                if (pick == s->pending.end()) break;   // wait for memory
                 Req* r = *pick;
-                if (s->mem_used + job->bytes + r->bytes > s->o.device_memory_budget && !(job->reqs.empty() &&
-                                                                                          s->mem_used == 0))
-                    break;   // wait for memory (a lone request on an idle server always goes)
                 s->pending.erase(pick);
                 r->state = BP_REQ_ADMITTED;
                 r->job = job;
@@ -532,6 +550,13 @@ bp_status bp_server_create(bp_engine* e, const bp_db* db, const bp_server_option
     }
     s->n_lanes = s->o.lanes;
     s->depth = s->o.lane_depth;
+    if (cudaSetDevice(e->device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&s->readback, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        s->readback = nullptr;
+        bp_server_destroy(s);
+        return bp_set_error(e, BP_ERR_CUDA, "bp_server_create: read-back stream");
+    }
     for (int l = 0; l < s->n_lanes; ++l) {
         cudaEvent_t ev = nullptr;
         if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
@@ -650,15 +675,25 @@ bp_status bp_server_digest(bp_server* s, uint64_t ticket, uint64_t out[2]) {
         index = r->index;
         for (Job* j : r->segs) pieces.push_back(j->batch);
     }
-    if (pieces.empty()) return bp_batch_digest(job->batch, index, out);
-    // segment mode: the pieces' sums at their places in the whole result
+    // on the server's own read-back stream: a slot's stream may already run
+    // the next batch, which a digest there would wait for
+    std::lock_guard<std::mutex> rb(s->readback_mu);
     uint64_t sums[2] = {0, 0};
+    if (pieces.empty()) {
+        const bp_status st = bp_batch_digest_sums(job->batch, index, s->e, s->readback, 0, 0, true, sums);
+        if (st != BP_OK) return st;
+        bp_digest_finish(sums, s->db->n, out);
+        return BP_OK;
+    }
+    // segment mode: the pieces' sums at their places in the whole result
     int64_t base = 0;
     for (size_t k = 0; k < pieces.size(); ++k) {
         int64_t nh = 0;
         bp_status st = bp_batch_copy_query(pieces[k], 0, nullptr, nullptr, nullptr, &nh);
         uint64_t part[2];
-        if (st == BP_OK) st = bp_batch_digest_sums(pieces[k], 0, s->seg_first[k], base, k + 1 == pieces.size(), part);
+        if (st == BP_OK)
+            st = bp_batch_digest_sums(pieces[k], 0, s->e, s->readback, s->seg_first[k], base, k + 1 == pieces.size(),
+                                      part);
         if (st != BP_OK) return st;
         sums[0] += part[0];
         sums[1] += part[1];
@@ -762,6 +797,7 @@ void bp_server_destroy(bp_server* s) {
     for (auto& kv : s->reqs) delete kv.second;
     for (bp_engine* le : s->slots) bp_engine_destroy(le);
     for (cudaEvent_t ev : s->lane_tail) cudaEventDestroy(ev);
+    if (s->readback) cudaStreamDestroy(s->readback);
     delete s;
 }
 

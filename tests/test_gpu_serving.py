@@ -251,3 +251,31 @@ def test_segmented_shortest_first_preempts_a_long_request(engine, matrix):
         else:
             assert min(ends) > head_end, (ends, head_end)
     d.close()
+
+
+def test_shortest_first_leaves_room_for_the_requests_it_overtakes(engine, world):
+    # a client that reads its requests in submission order and releases each
+    # after reading it: the long request it waits for must be admitted even
+    # though later, shorter requests were admitted ahead of it and hold their
+    # (unread) results -- shortest-first keeps room for the older request
+    qs, db, d, alone = world
+    lens = np.array([len(q) for q in qs])
+    li = int(np.argmax(lens))
+    short = [int(i) for i in np.argsort(lens)[:10]]
+
+    def per(L):   # the server's estimate of a request's device bytes
+        return (19684 * 4 + 40 * L + 4096) + (db.n_subjects * 24 + 8) + int(3e-4 * 1.5 * L / 500.0 * db.n_residues) * 60
+
+    budget = per(lens[li]) + 2 * per(max(lens[i] for i in short))
+    srv = Server(engine, d, max_batch_queries=1, lanes=1, lane_depth=1, admission=1, memory_budget=budget)
+    head = srv.submit(qs[li])
+    a = srv.submit(qs[li])
+    rest = [srv.submit(qs[i]) for i in short]
+    for t, qi in [(head, li), (a, li)] + list(zip(rest, short)):
+        srv.wait(t, 60_000)             # raises if the server stalled
+        r, _ = srv.result(t)
+        _check([r], [alone[qi]], "request %d" % qi)
+        srv.release(t)
+    st = srv.stats()
+    assert st["completed"] == 12 and st["mem_peak"] <= budget and st["mem_used"] == 0
+    srv.close()
