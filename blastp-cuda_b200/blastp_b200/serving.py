@@ -35,7 +35,9 @@ def drive(server, queries, arrivals, keep_results: bool = True, release: bool = 
     serving client frees what it has read: results held by the server count
     against its device-memory budget.  With a list as `digests`, the result
     digests of the first `digest_first` requests are appended to it, in
-    request order."""
+    request order; those requests are held until every request has been
+    submitted (a digest runs on the device and could wait for SMs the
+    running search holds, which would delay submissions)."""
     n = len(queries)
     results = [None] * n
     lat = np.zeros(n)
@@ -56,7 +58,7 @@ def drive(server, queries, arrivals, keep_results: bool = True, release: bool = 
     def poll():
         still = []
         for i in open_:
-            if server.state(tickets[i]) >= 3:      # done or failed
+            if (digests is None or i >= digest_first) and server.state(tickets[i]) >= 3:   # done or failed
                 collect(i)
             else:
                 still.append(i)

@@ -67,13 +67,14 @@ def test_drive_releases_requests_as_they_finish():
     # request 0 runs 0.3 s; requests 1-3 (submitted 0.05 s apart) 0.01 s each:
     # they are read and released while request 0 still runs, before the last
     # submission; results, latencies and digests come back in request order
+    # (a request whose digest is wanted is held until all are submitted)
     srv = FakeServer([0.3, 0.01, 0.01, 0.01])
     digests = []
     res, lat, late = serving.drive(srv, ["a", "b", "c", "d"], [0.0, 0.05, 0.1, 0.15], digests=digests,
-                                   digest_first=3)
+                                   digest_first=1)
     assert [r[1] for r in res] == ["a", "b", "c", "d"]
     assert list(lat) == [300.0, 10.0, 10.0, 10.0]
-    assert digests == [(0, 0), (1, 0), (2, 0)]
+    assert digests == [(0, 0)]
     assert set(srv.released) == {0, 1, 2, 3}
     t_last_submit = srv.submitted[3][0]
     assert srv.released[1] < t_last_submit and srv.released[2] < t_last_submit
@@ -85,3 +86,11 @@ def test_drive_without_release_keeps_everything():
     srv = FakeServer([0.02, 0.01])
     res, lat, _ = serving.drive(srv, ["a", "b"], [0.0, 0.03], keep_results=False, release=False)
     assert res is None and list(lat) == [20.0, 10.0] and srv.released == {}
+
+
+def test_drive_holds_digested_requests_until_all_are_submitted():
+    srv = FakeServer([0.01, 0.01, 0.01])
+    digests = []
+    serving.drive(srv, ["a", "b", "c"], [0.0, 0.05, 0.1], keep_results=False, digests=digests, digest_first=2)
+    assert digests == [(0, 0), (1, 0)]
+    assert srv.released[0] > srv.submitted[2][0] and srv.released[1] > srv.submitted[2][0]
