@@ -627,6 +627,8 @@ def run_serving(eng, matrix, args):
                        "mean_batch": st["mean_batch"], "max_in_flight": st["max_in_flight"],
                        "mem_peak_gb": st["mem_peak"] / 1e9, "wall_s": wall,
                        "submit_lateness_ms_max": float(late.max()) if len(late) else 0.0,
+                       "submit_lateness_ms_p99": serving.percentile(late, 99) if len(late) else 0.0,
+                       "submit_lateness_worst_request": int(np.argmax(late)) if len(late) else -1,
                        "query_residues": qres,
                        "identical_to_plain": same == n_check, "checked_requests": n_check,
                        "alone_scan_ms_median": float(np.median(alone_ms)) if alone_ms else None,
