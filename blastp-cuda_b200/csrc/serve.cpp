@@ -9,7 +9,9 @@
 //    per-subject outputs and its share of the HSP record buffer), builds
 //    their tables and launches them as one batched persistent search on a
 //    lane -- each lane's launch takes 1/lanes of the SMs, so a batch that
-//    starts while another lane's is running overlaps it on the device;
+//    starts while another lane's is running overlaps it on the device (with
+//    one lane, a batch of one request runs as the plain single-query search
+//    instead, which takes every SM);
 //  * a lane holds up to lane_depth batches, each in a slot with its own
 //    engine (stream and scratch): the slot's stream waits for the lane's
 //    previous batch (an event), so a lane runs its batches back to back in
@@ -76,6 +78,7 @@ struct Job {
     int64_t bytes = 0;
     bool done = false;
     int seg = -1;             // segment mode: the subject range searched
+    bp_result* result = nullptr;   // a one-request job runs as the plain search instead of a batch
 };
 
 }  // namespace
@@ -121,6 +124,51 @@ int64_t request_bytes(const bp_server* s, int32_t qlen) {
     return table + outputs + records;
 }
 
+// A job's search is a batch of its requests or, for a single request, the
+// plain search (the single-query scan kernel, no item schedule: 7-8 % faster
+// than a batch of one on the serving database).
+bp_status job_wait(Job* j) { return j->result ? bp_result_wait(j->result) : bp_batch_wait(j->batch); }
+
+// A finished job's result for request `index`; synchronous copies on the
+// legacy stream, which do not wait for what the slot's stream runs now.
+bp_status job_copy(Job* j, int index, int32_t* counters, int64_t* hsp_off, bp_hsp* hsps, int64_t* n_hsps) {
+    if (!j->result) return bp_batch_copy_query(j->batch, index, counters, hsp_off, hsps, n_hsps);
+    bp_result* r = j->result;
+    const bp_status st = bp_result_wait(r);
+    if (st != BP_OK) return st;
+    cudaError_t err = cudaSetDevice(r->e->device);
+    if (n_hsps) *n_hsps = r->n_hsps;
+    if (err == cudaSuccess && counters && r->n > 0)
+        err = cudaMemcpy(counters, r->d_counters, (size_t)r->n * 3 * sizeof(int32_t), cudaMemcpyDeviceToHost);
+    if (err == cudaSuccess && hsp_off)
+        err = cudaMemcpy(hsp_off, r->d_hsp_off, ((size_t)r->n + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost);
+    if (err == cudaSuccess && hsps && r->n_hsps > 0)
+        err = cudaMemcpy(hsps, r->d_hsps, (size_t)r->n_hsps * sizeof(bp_hsp), cudaMemcpyDeviceToHost);
+    if (err != cudaSuccess) return bp_set_cuda_error(r->e, err, "server result copy");
+    return BP_OK;
+}
+
+// A finished job's digest sums for request `index`, as one piece of a
+// result (bp_digest_sums), on the server's read-back stream.
+bp_status job_digest_sums(bp_server* s, Job* j, int index, int64_t first, int64_t rec_base, bool last,
+                          uint64_t sums[2]) {
+    if (!j->result) return bp_batch_digest_sums(j->batch, index, s->e, s->readback, first, rec_base, last, sums);
+    bp_result* r = j->result;
+    const bp_status st = bp_result_wait(r);
+    if (st != BP_OK) return st;
+    return bp_digest_sums(s->e, s->readback, r->d_counters, r->n, r->d_hsp_off, r->d_hsps, first, rec_base, last,
+                          sums);
+}
+
+// Frees a finished job's search, stream-ordered (the slot's stream may
+// already run another job).
+void job_free(Job* j) {
+    bp_batch_destroy_finished(j->batch);
+    j->batch = nullptr;
+    if (j->result) bp_result_destroy(j->result);
+    j->result = nullptr;
+}
+
 void fail_request(bp_server* s, Req* r, bp_status st) {
     r->state = BP_REQ_FAILED;
     r->status = st;
@@ -146,7 +194,7 @@ void launch_job(bp_server* s, Job* job) {
     bo.use_graph = 0;
     bo.ctas = std::max(1, le->sm_count / std::max(1, s->n_lanes));
     std::vector<float> costs;
-    if (st == BP_OK && bo.schedule == BP_SCHED_COSTS) {
+    if (st == BP_OK && bo.schedule == BP_SCHED_COSTS && !(qs.size() == 1 && s->n_lanes == 1)) {
         if (!s->o.model) {
             bo.schedule = BP_SCHED_STATIC;   // no model: the static schedule
         } else {
@@ -161,10 +209,18 @@ void launch_job(bp_server* s, Job* job) {
             bo.item_costs = costs.data();
         }
     }
-    // behind the lane's previous batch on the device, then this one becomes the lane's tail
-    if (st == BP_OK)
+    // behind the lane's previous job on the device, then this one becomes the lane's tail
+    const bool plain = qs.size() == 1 && s->n_lanes == 1;   // (a plain search takes every SM)
+    if (st == BP_OK && plain) {
+        if (s->lane_used[job->lane] && cudaStreamWaitEvent(le->stream, s->lane_tail[job->lane], 0) != cudaSuccess) {
+            cudaGetLastError();
+            st = BP_ERR_CUDA;
+        }
+        if (st == BP_OK) st = bp_search(le, s->db, qs[0], 0, -1, &job->result);
+    } else if (st == BP_OK) {
         st = bp_search_batch_behind(le, s->db, qs.data(), (int32_t)qs.size(), &bo,
                                     s->lane_used[job->lane] ? s->lane_tail[job->lane] : nullptr, &job->batch);
+    }
     if (st == BP_OK) {
         if (cudaEventRecord(s->lane_tail[job->lane], le->stream) == cudaSuccess) {
             s->lane_used[job->lane] = true;
@@ -223,36 +279,15 @@ void launch_seg_job(bp_server* s, Job* job) {
     Req* r = job->reqs[0];
     bp_status st = BP_OK;
     if (!r->query) st = bp_query_create(le, r->residues.data(), (int32_t)r->residues.size(), &s->o.params, &r->query);
-    bp_batch_options bo;
-    bp_batch_options_default(&bo);
-    bo.chunk_residues = s->o.chunk_residues > 0 ? s->o.chunk_residues : (1 << 20);
-    bo.schedule = s->o.schedule;
-    bo.use_graph = 0;
-    bo.ctas = std::max(1, le->sm_count / std::max(1, s->n_lanes));
-    bo.subject_first = s->seg_first[job->seg];
-    bo.subject_count = s->seg_first[job->seg + 1] - s->seg_first[job->seg];
-    std::vector<float> costs;
-    if (st == BP_OK && bo.schedule == BP_SCHED_COSTS) {
-        if (!s->o.model) {
-            bo.schedule = BP_SCHED_STATIC;
-        } else {
-            int32_t nc = 0;
-            st = bp_batch_plan(s->db, bo.subject_first, bo.subject_count, bo.chunk_residues, nullptr, &nc);
-            std::vector<int32_t> first((size_t)nc + 1);
-            if (st == BP_OK)
-                st = bp_batch_plan(s->db, bo.subject_first, bo.subject_count, bo.chunk_residues, first.data(), &nc);
-            costs.resize((size_t)nc);
-            const bp_query* q = r->query;
-            if (st == BP_OK)
-                st = bp_batch_predict_costs(le, s->o.model, s->o.cost_weights, s->db, &q, 1, first.data(), nc,
-                                            s->o.planted_density, costs.data());
-            bo.item_costs = costs.data();
-        }
+    // the plain search over the range, behind the lane's previous job
+    if (st == BP_OK && s->lane_used[job->lane] &&
+        cudaStreamWaitEvent(le->stream, s->lane_tail[job->lane], 0) != cudaSuccess) {
+        cudaGetLastError();
+        st = BP_ERR_CUDA;
     }
-    const bp_query* q = r->query;
     if (st == BP_OK)
-        st = bp_search_batch_behind(le, s->db, &q, 1, &bo, s->lane_used[job->lane] ? s->lane_tail[job->lane] : nullptr,
-                                    &job->batch);
+        st = bp_search(le, s->db, r->query, s->seg_first[job->seg],
+                       s->seg_first[job->seg + 1] - s->seg_first[job->seg], &job->result);
     if (st == BP_OK) {
         if (cudaEventRecord(s->lane_tail[job->lane], le->stream) == cudaSuccess) {
             s->lane_used[job->lane] = true;
@@ -289,7 +324,7 @@ bool segs_finished(const Req* r) {
 // Segment mode: frees a released request whose launched ranges have all finished.
 void retire_segmented(bp_server* s, Req* r) {
     for (Job* j : r->segs) {
-        bp_batch_destroy_finished(j->batch);
+        job_free(j);
         delete j;
     }
     r->segs.clear();
@@ -317,7 +352,7 @@ Req* next_segment_request(bp_server* s) {
 
 // Frees a job whose requests have all been released.
 void retire_job(bp_server* s, Job* job) {
-    bp_batch_destroy_finished(job->batch);   // the slot's stream may already run another batch
+    job_free(job);
     for (Req* r : job->reqs) {
         bp_query_destroy(r->query);
         r->query = nullptr;
@@ -348,7 +383,7 @@ bool dispatch_segments(bp_server* s, std::unique_lock<std::mutex>& lock) {
             if (cudaStreamQuery(s->slots[l]->stream) == cudaErrorNotReady) continue;
             cudaGetLastError();
             lock.unlock();
-            const bp_status st = bp_batch_wait(job->batch);   // re-runs on record overflow
+            const bp_status st = job_wait(job);   // re-runs on record overflow
             lock.lock();
             job->done = true;
             if (r->state == BP_REQ_RUNNING || r->state == BP_REQ_ADMITTED) {
@@ -433,7 +468,7 @@ void dispatcher(bp_server* s) {
                 if (cudaStreamQuery(s->slots[l]->stream) == cudaErrorNotReady) continue;
                 cudaGetLastError();
                 lock.unlock();
-                const bp_status st = bp_batch_wait(job->batch);   // re-runs on record overflow
+                const bp_status st = job_wait(job);   // re-runs on record overflow
                 lock.lock();
                 const double t = now_ms();
                 for (Req* r : job->reqs) {
@@ -627,7 +662,7 @@ bp_status bp_server_result(bp_server* s, uint64_t ticket, int32_t* counters, int
     if (!s) return BP_ERR_INVALID;
     Job* job = nullptr;
     int index = -1;
-    std::vector<bp_batch*> pieces;
+    std::vector<Job*> pieces;
     {
         std::lock_guard<std::mutex> lock(s->mu);
         auto it = s->reqs.find(ticket);
@@ -638,18 +673,18 @@ bp_status bp_server_result(bp_server* s, uint64_t ticket, int32_t* counters, int
         if (latency_ms) *latency_ms = r->t_done - r->t_arrive;
         job = r->job;
         index = r->index;
-        for (Job* j : r->segs) pieces.push_back(j->batch);
+        pieces = r->segs;
     }
     // the jobs cannot be retired before this request is released
-    if (pieces.empty()) return bp_batch_copy_query(job->batch, index, counters, hsp_off, hsps, n_hsps);
+    if (pieces.empty()) return job_copy(job, index, counters, hsp_off, hsps, n_hsps);
     // segment mode: range k's piece goes to subjects [seg_first[k], seg_first[k + 1]), its
     // records after those of the ranges before it
     int64_t base = 0;
     for (size_t k = 0; k < pieces.size(); ++k) {
         const int32_t f = s->seg_first[k];
         int64_t nh = 0;
-        const bp_status st = bp_batch_copy_query(pieces[k], 0, counters ? counters + 3 * (int64_t)f : nullptr,
-                                                 hsp_off ? hsp_off + f : nullptr, hsps ? hsps + base : nullptr, &nh);
+        const bp_status st = job_copy(pieces[k], 0, counters ? counters + 3 * (int64_t)f : nullptr,
+                                      hsp_off ? hsp_off + f : nullptr, hsps ? hsps + base : nullptr, &nh);
         if (st != BP_OK) return st;
         if (hsp_off)
             for (int32_t i = f; i <= s->seg_first[k + 1]; ++i) hsp_off[i] += base;
@@ -663,7 +698,7 @@ bp_status bp_server_digest(bp_server* s, uint64_t ticket, uint64_t out[2]) {
     if (!s || !out) return BP_ERR_INVALID;
     Job* job = nullptr;
     int index = -1;
-    std::vector<bp_batch*> pieces;
+    std::vector<Job*> pieces;
     {
         std::lock_guard<std::mutex> lock(s->mu);
         auto it = s->reqs.find(ticket);
@@ -673,14 +708,14 @@ bp_status bp_server_digest(bp_server* s, uint64_t ticket, uint64_t out[2]) {
         if (r->state != BP_REQ_DONE) return BP_ERR_NOT_READY;
         job = r->job;
         index = r->index;
-        for (Job* j : r->segs) pieces.push_back(j->batch);
+        pieces = r->segs;
     }
     // on the server's own read-back stream: a slot's stream may already run
     // the next batch, which a digest there would wait for
     std::lock_guard<std::mutex> rb(s->readback_mu);
     uint64_t sums[2] = {0, 0};
     if (pieces.empty()) {
-        const bp_status st = bp_batch_digest_sums(job->batch, index, s->e, s->readback, 0, 0, true, sums);
+        const bp_status st = job_digest_sums(s, job, index, 0, 0, true, sums);
         if (st != BP_OK) return st;
         bp_digest_finish(sums, s->db->n, out);
         return BP_OK;
@@ -689,11 +724,9 @@ bp_status bp_server_digest(bp_server* s, uint64_t ticket, uint64_t out[2]) {
     int64_t base = 0;
     for (size_t k = 0; k < pieces.size(); ++k) {
         int64_t nh = 0;
-        bp_status st = bp_batch_copy_query(pieces[k], 0, nullptr, nullptr, nullptr, &nh);
+        bp_status st = job_copy(pieces[k], 0, nullptr, nullptr, nullptr, &nh);
         uint64_t part[2];
-        if (st == BP_OK)
-            st = bp_batch_digest_sums(pieces[k], 0, s->e, s->readback, s->seg_first[k], base, k + 1 == pieces.size(),
-                                      part);
+        if (st == BP_OK) st = job_digest_sums(s, pieces[k], 0, s->seg_first[k], base, k + 1 == pieces.size(), part);
         if (st != BP_OK) return st;
         sums[0] += part[0];
         sums[1] += part[1];
@@ -767,13 +800,18 @@ void bp_server_destroy(bp_server* s) {
     }
     s->cv_work.notify_all();
     if (s->th.joinable()) s->th.join();
-    // release everything still held
+    // release everything still held, once nothing runs
+    for (bp_engine* le : s->slots) {
+        cudaSetDevice(le->device);
+        cudaStreamSynchronize(le->stream);
+    }
+    cudaGetLastError();
     std::vector<Req*> segmented;
     for (auto& kv : s->reqs)
         if (!kv.second->segs.empty()) segmented.push_back(kv.second);
     for (Req* r : segmented) {
         for (Job* j : r->segs) {
-            bp_batch_destroy(j->batch);
+            job_free(j);
             delete j;
         }
         r->segs.clear();
@@ -786,7 +824,7 @@ void bp_server_destroy(bp_server* s) {
         if (kv.second->job && std::find(jobs.begin(), jobs.end(), kv.second->job) == jobs.end())
             jobs.push_back(kv.second->job);
     for (Job* j : jobs) {
-        bp_batch_destroy(j->batch);
+        job_free(j);
         for (Req* r : j->reqs) {
             bp_query_destroy(r->query);
             s->reqs.erase(r->id);

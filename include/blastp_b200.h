@@ -404,8 +404,10 @@ typedef struct {
                                        `admission` -- arrival order, or (BP_ADMIT_SHORTEST) the least
                                        remaining work (ranges left x query length), so a short
                                        request that arrives while a long one runs goes ahead of the
-                                       long one's remaining ranges.  max_batch_queries is not used.
-                                       Results are the same either way. */
+                                       long one's remaining ranges.  max_batch_queries is not used;
+                                       each range runs as the plain single-query search (as does,
+                                       with one lane, any batch of one request).  Results are the
+                                       same either way. */
 } bp_server_options;
 
 enum { BP_ADMIT_ARRIVAL = 0, BP_ADMIT_SHORTEST = 1 };
