@@ -147,8 +147,13 @@ bp_status bp_run_search(bp_engine* e, bp_result* r) {
     const bp_db* db = r->db;
     const bp_query* q = r->q;
     const int32_t n = r->n;
+    // record capacity from the expected word hits (2.5e-4 HSPs per hit, as
+    // batched searches size theirs), so a long query rarely runs twice
+    double span = (double)db->nres;
+    if (db->h_off.size() == (size_t)db->n + 1) span = (double)(db->h_off[r->first + n] - db->h_off[r->first]);
+    const size_t want = (size_t)std::min<double>(1 << 28, std::max(65536.0, 2.5e-4 * q->hits_per_residue * span));
     size_t cap = e->rec_cap;
-    CK(grow(&e->d_recs, &cap, std::max<size_t>(r->cap, 65536)), "cudaMalloc(records)");
+    CK(grow(&e->d_recs, &cap, std::max<size_t>(r->cap, want)), "cudaMalloc(records)");
     e->rec_cap = (uint32_t)cap;
     size_t fcap = (size_t)e->fill_cap;
     CK(grow(&e->d_fill, &fcap, (size_t)std::max(n, 1)), "cudaMalloc(fill)");
