@@ -65,7 +65,7 @@ def parse():
     ap.add_argument("--batch-autotune", type=int, default=1, help="run the autotuner (0: skip it)")
     ap.add_argument("--serve", type=int, default=1, help="also measure the serving loop (1 GPU runs only)")
     ap.add_argument("--serve-subjects", type=int, default=5_000_000)
-    ap.add_argument("--serve-requests", type=int, default=128)
+    ap.add_argument("--serve-requests", type=int, default=256)
     ap.add_argument("--serve-rate", type=float, default=1000.0, help="offered load, queries/s (Poisson)")
     ap.add_argument("--serve-sustained-requests", type=int, default=384,
                     help="requests of each run at 80 %% of the measured capacity")

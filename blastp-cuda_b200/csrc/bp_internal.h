@@ -293,6 +293,9 @@ int32_t bp_order_blocksums_needed(int32_t n);
 cudaError_t bp_launch_offsets(bp_engine* e, cudaStream_t st, int32_t n, const int32_t* d_counters, int64_t* d_off,
                               int32_t* d_fill, int64_t* d_blocksums);
 bp_status bp_run_search(bp_engine* e, bp_result* r);
+// Grows the engine's search scratch (record buffer, fill cursors, block sums)
+// to at least these sizes now: growing later synchronises the device.
+bp_status bp_engine_reserve(bp_engine* e, int32_t n_subjects, size_t records);
 // Digest of one query's result in device memory: counters (3n), CSR offsets
 // (n+1, taken relative to d_hsp_off[0]) and the records they cover; waits
 // for `st` (see digest.cu).

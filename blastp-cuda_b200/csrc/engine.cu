@@ -143,6 +143,21 @@ void bp_pinned_put(bp_engine* e, uint32_t* p) {
 
 // Enqueues scan + ordering for r (subjects r->first.. of r->db against r->q)
 // on the engine stream.  Scratch is the engine's; outputs are r's.
+bp_status bp_engine_reserve(bp_engine* e, int32_t n_subjects, size_t records) {
+    if (!e || n_subjects < 0) return BP_ERR_INVALID;
+    CK(cudaSetDevice(e->device), "cudaSetDevice");
+    size_t cap = e->rec_cap;
+    CK(grow(&e->d_recs, &cap, std::max<size_t>(records, 65536)), "cudaMalloc(records)");
+    e->rec_cap = (uint32_t)cap;
+    size_t fcap = (size_t)e->fill_cap;
+    CK(grow(&e->d_fill, &fcap, (size_t)std::max(n_subjects, 1)), "cudaMalloc(fill)");
+    e->fill_cap = (int32_t)fcap;
+    size_t bcap = (size_t)e->blocksum_cap;
+    CK(grow(&e->d_blocksums, &bcap, (size_t)bp_order_blocksums_needed(n_subjects)), "cudaMalloc(blocksums)");
+    e->blocksum_cap = (int32_t)bcap;
+    return BP_OK;
+}
+
 bp_status bp_run_search(bp_engine* e, bp_result* r) {
     const bp_db* db = r->db;
     const bp_query* q = r->q;

@@ -611,6 +611,15 @@ bp_status bp_server_create(bp_engine* e, const bp_db* db, const bp_server_option
         }
         s->slots.push_back(le);
         s->slot_job.push_back(nullptr);
+        // scratch for plain searches over the whole database, sized now (a
+        // later growth would synchronise the device under load): records for
+        // two expected word hits per residue, a 1,000-letter query's worth
+        const size_t recs = (size_t)std::min<double>(1 << 28, 2.5e-4 * 2.0 * (double)db->nres);
+        const bp_status rs = bp_engine_reserve(le, db->n, recs);
+        if (rs != BP_OK) {
+            bp_server_destroy(s);
+            return bp_set_error(e, rs, "bp_server_create: slot scratch");
+        }
     }
     s->th = std::thread(dispatcher, s);
     *out = s;
