@@ -279,3 +279,19 @@ def test_shortest_first_leaves_room_for_the_requests_it_overtakes(engine, world)
     st = srv.stats()
     assert st["completed"] == 12 and st["mem_peak"] <= budget and st["mem_used"] == 0
     srv.close()
+
+
+def test_segmented_two_lanes_under_a_memory_budget(engine, world):
+    # ranges of different requests on two lanes at once, shortest first, with a
+    # budget of about three requests: every result equals the plain search and
+    # the budget is never exceeded
+    qs, db, d, alone = world
+    per = 19684 * 4 + 40 * 1500 + 4096 + db.n_subjects * 24 + 8 + int(3e-4 * 1.5 * 3 * db.n_residues) * 60
+    srv = Server(engine, d, lanes=2, lane_depth=2, segments=3, admission=1, memory_budget=3 * per)
+    arr = serving.poisson_arrivals(np.random.default_rng(8), 4000.0, 16)
+    results, _, _ = serving.drive(srv, qs[:16], arr)
+    _check(results, alone[:16], "two lanes, ranges")
+    st = srv.stats()
+    assert st["completed"] == 16 and st["batches"] == 16 * 3
+    assert st["mem_peak"] <= 3 * per and st["mem_used"] == 0
+    srv.close()
