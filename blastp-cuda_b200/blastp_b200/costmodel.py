@@ -15,7 +15,7 @@ per query.  ``BP_SCHED_COSTS`` then places the longest predicted item first
 into the least loaded CTA queue; the static round-robin queues are the
 fallback when no model is available.
 
-The plain kernel stays the judge of results: a schedule only decides which
+Results do not depend on the schedule: a schedule only decides which
 CTA scans which item, never what is computed.
 """
 from __future__ import annotations
