@@ -458,16 +458,18 @@ __device__ __forceinline__ void apply_hits(WarpScan<DiagT, kProf>& w, bool hv, i
     if (kPacked && count && hv) atomicAdd(&w.wcnt[3 * w.a->member_of[hq]], 1);   // word hits per query
     unsigned peers = 0;
     if (hv) peers = __match_any_sync(vmask, d);
-    bool pending = hv, found = false;
+    // a hit goes in the round of its rank among the chunk's hits on its
+    // diagonal (the lanes before it with the same d), so every diagonal sees
+    // its hits in lane order and one round holds one hit per diagonal
+    const int rank = hv ? __popc(peers & w.lt) : -1;
+    const int rounds = (int)__reduce_max_sync(kFull, (unsigned)(rank + 1));
+    bool found = false;
     ExtOut res{0, 0, 0, 0, 0, 0};
     const int window = w.a->window;
-    for (;;) {
-        const unsigned pend = __ballot_sync(kFull, pending);
-        if (!pend) break;
+    for (int round = 0; round < rounds; ++round) {
         bool need = false, blk = false;
         int diff = 0;
-        if (pending && (peers & pend & w.lt) == 0) {
-            pending = false;
+        if (rank == round) {
             const uint32_t v = w.diag[d];
             const int stamp = hs + w.base;
             if (kDefer && (v & B::kPend)) {
