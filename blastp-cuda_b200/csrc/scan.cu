@@ -461,15 +461,27 @@ __device__ __forceinline__ void apply_hits(WarpScan<DiagT, kProf>& w, bool hv, i
     // a hit goes in the round of its rank among the chunk's hits on its
     // diagonal (the lanes before it with the same d), so every diagonal sees
     // its hits in lane order and one round holds one hit per diagonal
-    const int rank = hv ? __popc(peers & w.lt) : -1;
-    const int rounds = (int)__reduce_max_sync(kFull, (unsigned)(rank + 1));
-    bool found = false;
+    // (packed tables keep asking each round which hits are still pending:
+    // there the rank's registers cost the kernel more than the ballots)
+    const int rank = (!kPacked && hv) ? __popc(peers & w.lt) : -1;
+    const int rounds = kPacked ? 0 : (int)__reduce_max_sync(kFull, (unsigned)(rank + 1));
+    bool pending = kPacked && hv, found = false;
     ExtOut res{0, 0, 0, 0, 0, 0};
     const int window = w.a->window;
-    for (int round = 0; round < rounds; ++round) {
+    for (int round = 0;; ++round) {
+        bool go;
+        if (kPacked) {
+            const unsigned pend = __ballot_sync(kFull, pending);
+            if (!pend) break;
+            go = pending && (peers & pend & w.lt) == 0;
+            if (go) pending = false;
+        } else {
+            if (round >= rounds) break;
+            go = rank == round;
+        }
         bool need = false, blk = false;
         int diff = 0;
-        if (rank == round) {
+        if (go) {
             const uint32_t v = w.diag[d];
             const int stamp = hs + w.base;
             if (kDefer && (v & B::kPend)) {
