@@ -456,7 +456,9 @@ def run_batched(eng, matrix, args, torch):
                 "static": dict(chunk_residues=1 << 20, schedule=SCHED_STATIC),
                 "dynamic": dict(chunk_residues=1 << 20, schedule=SCHED_DYNAMIC),
                 "learned": dict(chunk_residues=1 << 20, schedule=SCHED_COSTS),
-                "learned_order": dict(chunk_residues=1 << 20, schedule=SCHED_COST_ORDER)}
+                "learned_order": dict(chunk_residues=1 << 20, schedule=SCHED_COST_ORDER),
+                "plain_unpacked": dict(chunk_residues=1 << 20, schedule=SCHED_DYNAMIC, pack_residues=1024,
+                                       plain_unpacked=1)}
     if args.batch_autotune:
         t0 = time.perf_counter()
         best, trials = eng.autotune(db, qs, model=model, planted_density=planted,
@@ -464,8 +466,9 @@ def run_batched(eng, matrix, args, torch):
         out["autotune"] = {"sample_subjects": max(1, w.db.n_subjects // 16), "seconds": time.perf_counter() - t0,
                            "best": dict(best, schedule=SCHED_NAMES[best["schedule"]]),
                            "trials": [[t["chunk_residues"], t["pack_residues"], SCHED_NAMES[t["schedule"]],
-                                       t["max_warps"], round(t["ms"], 3)] for t in trials],
-                           "trial_fields": ["chunk_residues", "pack_residues", "schedule", "max_warps", "ms"]}
+                                       t["max_warps"], t["plain_unpacked"], round(t["ms"], 3)] for t in trials],
+                           "trial_fields": ["chunk_residues", "pack_residues", "schedule", "max_warps",
+                                            "plain_unpacked", "ms"]}
         variants["autotuned"] = dict(best)
     identical = True
     identical_all = True
@@ -487,7 +490,8 @@ def run_batched(eng, matrix, args, torch):
                      "speedup_vs_plain": plain_ms / ms,
                      "chunk_residues": kw["chunk_residues"], "schedule": SCHED_NAMES[kw["schedule"]],
                      "pack_residues": kw.get("pack_residues", 512),
-                     "max_warps": kw.get("max_warps", 0), "items": b.n_items,
+                     "max_warps": kw.get("max_warps", 0), "plain_unpacked": kw.get("plain_unpacked", 0),
+                     "items": b.n_items,
                      "launches_per_run": (eng.launches - launches0) // max(1, args.batch_reps)}
         if b.n_hsps != sum(plain_counts):
             identical = False

@@ -32,12 +32,12 @@ class BpGappedParams(ctypes.Structure):
 class BpBatchOptions(ctypes.Structure):
     _fields_ = [("chunk_residues", i32), ("schedule", i32), ("ctas", i32), ("max_warps", i32),
                 ("use_graph", i32), ("item_costs", P), ("subject_first", i32), ("subject_count", i32),
-                ("pack_residues", i32)]
+                ("pack_residues", i32), ("plain_unpacked", i32)]
 
 
 class BpAutotuneTrial(ctypes.Structure):
     _fields_ = [("chunk_residues", i32), ("schedule", i32), ("max_warps", i32), ("ms", ctypes.c_float),
-                ("pack_residues", i32)]
+                ("pack_residues", i32), ("plain_unpacked", i32)]
 
 
 class BpAutotuneOptions(ctypes.Structure):

@@ -127,7 +127,8 @@ class Engine:
 
     def search_batch(self, db: "Database", queries, chunk_residues: int = 1 << 18, schedule: int = 0,
                      ctas: int = 0, max_warps: int = 0, use_graph: bool = True, item_costs=None,
-                     first: int = 0, count: int = -1, pack_residues: int = 512) -> "Batch":
+                     first: int = 0, count: int = -1, pack_residues: int = 512,
+                     plain_unpacked: int = 0) -> "Batch":
         """Many queries against db in one persistent launch; each query's
         result equals its single-query search."""
         o = BpBatchOptions()
@@ -140,6 +141,7 @@ class Engine:
         o.subject_first = first
         o.subject_count = count
         o.pack_residues = pack_residues
+        o.plain_unpacked = plain_unpacked
         costs = None
         if item_costs is not None:
             costs = np.ascontiguousarray(item_costs, dtype=np.float32)
@@ -219,9 +221,10 @@ class Engine:
         check(lib().bp_batch_autotune(self.h, db.h, arr, len(queries), ctypes.byref(o), ctypes.byref(best), trials,
                                       256, ctypes.byref(nt)), self.h)
         out = [{"chunk_residues": t.chunk_residues, "schedule": t.schedule, "max_warps": t.max_warps,
-                "pack_residues": t.pack_residues, "ms": float(t.ms)} for t in trials[:min(nt.value, 256)]]
+                "pack_residues": t.pack_residues, "plain_unpacked": t.plain_unpacked, "ms": float(t.ms)}
+               for t in trials[:min(nt.value, 256)]]
         return ({"chunk_residues": best.chunk_residues, "schedule": best.schedule, "max_warps": best.max_warps,
-                 "pack_residues": best.pack_residues}, out)
+                 "pack_residues": best.pack_residues, "plain_unpacked": best.plain_unpacked}, out)
 
     def blastp_host(self, query, params, residues, offsets, hsp_cap=None, counters=None, hsp_off=None):
         """End-to-end: host buffers in, host buffers out (one C call).

@@ -70,7 +70,9 @@ struct bp_batch {
         int32_t grid = 0;
         double est = 0;                        // expected word hits, to order the launches
         bool packed = false;                   // its units are packed tables
+        std::vector<int32_t> units;            // its units (indices into h_units)
     };
+    std::vector<BatchQuery> h_units;         // every unit's tables (plain_unpacked launches)
     std::vector<Class> classes;
     std::vector<cudaStream_t> side;          // one per class after the first
     std::vector<cudaEvent_t> ev_join;
@@ -135,7 +137,8 @@ bool resolve_range(const bp_db* db, int32_t first, int32_t count, int32_t* s0, i
 bp_status enqueue(bp_batch* b) {
     bp_engine* e = b->e;
     const uint64_t l0 = e->launches;
-    CKB(cudaMemsetAsync(b->d_counts, 0, (4 + b->classes.size()) * sizeof(uint32_t), e->stream), "memset(counts)");
+    CKB(cudaMemsetAsync(b->d_counts, 0, (4 + b->classes.size() + b->h_units.size()) * sizeof(uint32_t), e->stream),
+        "memset(counts)");
     // inside a capture a timing event must be an external record node
     const unsigned rec_flags = b->capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
     CKB(cudaEventRecordWithFlags(b->ev0, e->stream, rec_flags), "cudaEventRecord");
@@ -166,10 +169,44 @@ bp_status enqueue(bp_batch* b) {
         a.rec_count = b->d_counts;
         a.long_ids = b->db->d_long;
         a.long_min = b->db->long_min;
-        if (a.n_items > 0)
+        if (b->opt.plain_unpacked && !k.packed) {
+            // each query of the class as the plain single-query scan over the
+            // batch's subjects (its own cursor), into the same segments
+            for (int32_t ui : k.units) {
+                const BatchQuery& u = b->h_units[(size_t)ui];
+                ScanArgs p{};
+                p.db = b->db->d_res;
+                p.db_bytes = ((b->db->nres + 15) & ~15LL) + 32;   // the allocation's zero padding included
+                p.db_off = b->db->d_off;
+                p.first = b->first;
+                p.n = b->n;
+                p.query = u.query;
+                p.qlen = u.qlen;
+                p.cells = u.cells;
+                p.entries = u.entries;
+                p.n_entries = u.n_entries;
+                p.ctx = u.ctx;
+                p.n_ctx = u.n_ctx;
+                p.matrix = e->d_matrix;
+                p.window = a.window;
+                p.diag_len = u.diag_len;
+                p.counters = b->d_counters;
+                p.oid_base = u.seg_query * b->n;
+                p.recs = b->d_recs;
+                p.rec_cap = b->cap;
+                p.rec_count = b->d_counts;
+                p.cursor = b->d_counts + 4 + b->classes.size() + ui;
+                int32_t long_lo = 0;
+                bp_long_slice(b->db->h_long, b->first, b->n, &long_lo, &p.n_long);
+                p.long_ids = b->db->d_long ? b->db->d_long + long_lo : nullptr;
+                p.long_min = b->db->long_min;
+                if (p.n > 0) CKB(bp_launch_scan_on(e, st, p), "plain scan launch");
+            }
+        } else if (a.n_items > 0) {
             CKB(bp_launch_scan_batch(e, st, a, k.max_qlen, k.max_len, k.max_entries, k.grid, b->opt.max_warps,
                                      k.packed),
                 "batched scan launch");
+        }
         if (c > 0) {
             CKB(cudaEventRecord(b->ev_join[c - 1], st), "cudaEventRecord");
             CKB(cudaStreamWaitEvent(e->stream, b->ev_join[c - 1], 0), "cudaStreamWaitEvent");
@@ -189,7 +226,9 @@ bp_status enqueue(bp_batch* b) {
 bp_status prepare(bp_batch* b) {
     bp_engine* e = b->e;
     if (!b->d_counts) {
-        CKB(cudaMallocAsync((void**)&b->d_counts, (4 + b->classes.size()) * sizeof(uint32_t), e->stream), "cudaMalloc(counts)");
+        CKB(cudaMallocAsync((void**)&b->d_counts, (4 + b->classes.size() + b->h_units.size()) * sizeof(uint32_t),
+                            e->stream),
+            "cudaMalloc(counts)");
         CKB(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming), "cudaEventCreate");
         for (size_t c = 1; c < b->classes.size(); ++c) {
             cudaStream_t st = nullptr;
@@ -484,6 +523,7 @@ bp_status bp_search_batch_behind(bp_engine* e, const bp_db* db, const bp_query* 
     }
     const int32_t n_units = (int32_t)units.size();
     b->n_units = n_units;
+    b->h_units = units;
     // classes: a launch's layout is sized for its longest unit, so units share
     // a launch only when that leaves each of them the warps per CTA it would
     // get alone, and when they extend the same way; longest first
@@ -521,6 +561,7 @@ bp_status bp_search_batch_behind(bp_engine* e, const bp_db* db, const bp_query* 
             k.max_len = std::max(k.max_len, u.diag_len);
             k.max_qlen = std::max(k.max_qlen, u.qlen);
             k.max_entries = std::max<int64_t>(k.max_entries, u.n_entries);
+            k.units.push_back(ui);
             if (ui == u0) warps = own_warps(ui);
             for (int32_t qi : unit_queries[ui]) k.est += queries[qi]->hits_per_residue;
             for (int32_t c = 0; c < n_chunks; ++c) {
@@ -864,11 +905,12 @@ bp_status bp_batch_autotune(bp_engine* e, const bp_db* db, const bp_query* const
     int32_t nt = 0;
     std::vector<float> costs;
     int32_t costs_chunk = -1;
-    auto trial = [&](int32_t chunk, int32_t pack, int sched, int32_t max_warps) -> bp_status {
+    auto trial = [&](int32_t chunk, int32_t pack, int sched, int32_t max_warps, int32_t plain = 0) -> bp_status {
         bp_batch_options bo;
         bp_batch_options_default(&bo);
         bo.chunk_residues = chunk;
         bo.pack_residues = pack;
+        bo.plain_unpacked = plain;
         bo.schedule = sched;
         bo.max_warps = max_warps;
         bo.subject_first = 0;
@@ -903,6 +945,7 @@ bp_status bp_batch_autotune(bp_engine* e, const bp_db* db, const bp_query* const
             trials[nt].max_warps = max_warps;
             trials[nt].ms = ms;
             trials[nt].pack_residues = pack;
+            trials[nt].plain_unpacked = plain;
         }
         ++nt;
         if (ms < best_ms) {
@@ -935,6 +978,12 @@ bp_status bp_batch_autotune(bp_engine* e, const bp_db* db, const bp_query* const
     for (int wi = 0; wi < n_warp_caps; ++wi) {
         if (warps[wi] == 0) continue;
         bp_status st = trial(chunk, pack, sched, warps[wi]);
+        if (st != BP_OK) return st;
+    }
+    // stage 3: the queries that are not packed as plain single-query scans
+    {
+        const bp_batch_options b0 = *best;
+        bp_status st = trial(b0.chunk_residues, b0.pack_residues, b0.schedule, b0.max_warps, 1);
         if (st != BP_OK) return st;
     }
     if (n_trials) *n_trials = nt;

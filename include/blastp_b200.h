@@ -250,6 +250,10 @@ typedef struct {
                                    this many offsets (32 queries at most), so one word scan of a
                                    subject serves all of them; 0: every query alone.
                                    Default 512. */
+    int32_t plain_unpacked;     /* 1: every query that is not packed runs as the plain single-query
+                                   scan over the batch's subjects (subject cursor, longest first),
+                                   the packed tables as batched items; the item schedule then
+                                   applies to the packed tables only.  Default 0. */
 } bp_batch_options;
 
 void bp_batch_options_default(bp_batch_options* o);
@@ -335,11 +339,13 @@ bp_status bp_cosched_split(bp_engine* e, bp_mlp* model, const float* weights, co
  * Times candidate batch configurations on the first sample_subjects subjects
  * with the whole query set and returns the fastest: first every subject-chunk
  * size with every packing size (dynamic schedule, all warps), then, at the
- * best of those, the other schedules and the warp caps. */
+ * best of those, the other schedules and the warp caps, and last the best
+ * one with plain_unpacked set. */
 typedef struct {
     int32_t chunk_residues, schedule, max_warps;
     float ms;                   /* best scan time of the candidate on the sample */
     int32_t pack_residues;
+    int32_t plain_unpacked;
 } bp_autotune_trial;
 
 typedef struct {

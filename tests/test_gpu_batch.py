@@ -168,10 +168,11 @@ def test_autotune_picks_a_measured_candidate(engine, workload, singles):
     hs = [engine.query(q) for q in qs]
     best, trials = engine.autotune(d, hs, sample_subjects=3000, chunk_sizes=[1 << 14, 1 << 18], warp_caps=[0, 8],
                                    schedules=(SCHED_DYNAMIC, SCHED_STATIC), reps=1)
-    assert len(trials) == 8
+    assert len(trials) == 9                    # 2 chunks x 3 packings, 1 schedule, 1 warp cap, plain
+    assert [t["plain_unpacked"] for t in trials] == [0] * 8 + [1]
     fastest = min(trials, key=lambda t: t["ms"])
-    assert (best["chunk_residues"], best["schedule"], best["max_warps"]) == (
-        fastest["chunk_residues"], fastest["schedule"], fastest["max_warps"])
+    assert (best["chunk_residues"], best["schedule"], best["max_warps"], best["plain_unpacked"]) == (
+        fastest["chunk_residues"], fastest["schedule"], fastest["max_warps"], fastest["plain_unpacked"])
     b = engine.search_batch(d, hs, **best)
     _check(b, singles, "autotuned")
     b.close()
@@ -233,3 +234,20 @@ def test_digests_match_plain_and_tell_results_apart(engine, workload):
     for h in hs:
         h.close()
     d.close()
+
+
+@pytest.mark.parametrize("pack", [0, 1024])
+@pytest.mark.parametrize("use_graph", [False, True])
+def test_plain_unpacked(engine, workload, singles, pack, use_graph):
+    # the queries that are not packed run as plain single-query scans inside
+    # the batch (packed tables, if any, as batched items): every query's
+    # result equals its single-query search, on replays too
+    qs, db = workload
+    d = engine.database(db.residues, db.offsets)
+    hs = [engine.query(q) for q in qs]
+    b = engine.search_batch(d, hs, chunk_residues=1 << 16, pack_residues=pack, plain_unpacked=1,
+                            use_graph=use_graph)
+    _check(b, singles, "plain unpacked, pack %d" % pack)
+    b.run()
+    _check(b, singles, "plain unpacked, replayed")
+    b.close()
