@@ -193,6 +193,7 @@ void launch_job(bp_server* s, Job* job) {
     bo.schedule = s->o.schedule;
     bo.use_graph = 0;
     bo.ctas = std::max(1, le->sm_count / std::max(1, s->n_lanes));
+    bo.plain_unpacked = s->n_lanes == 1 ? 1 : 0;   // (a plain scan takes every SM)
     std::vector<float> costs;
     if (st == BP_OK && bo.schedule == BP_SCHED_COSTS && !(qs.size() == 1 && s->n_lanes == 1)) {
         if (!s->o.model) {
