@@ -74,6 +74,8 @@ def parse():
     ap.add_argument("--serve-lanes", type=int, default=1)
     ap.add_argument("--serve-depth", type=int, default=4, help="batches queued per lane")
     ap.add_argument("--serve-batch", type=int, default=1, help="queries per batch")
+    ap.add_argument("--serve-max-wait-ms", type=int, default=250,
+                    help="the wait after which a request goes first, in the capped preemptive run")
     ap.add_argument("--serve-segments", type=int, default=8,
                     help="subject ranges per request in the preemptive run (<= 1: no preemptive run)")
     ap.add_argument("--serve-schedule", default="dynamic", choices=["dynamic", "learned"],
@@ -583,7 +585,8 @@ def run_serving(eng, matrix, args):
     plan = [("offered", args.serve_rate, 0, 1),
             ("sustainable", None, 0, 1),
             ("sustainable_shortest_first", None, 1, 1),
-            ("sustainable_preemptive", None, 1, args.serve_segments)]
+            ("sustainable_preemptive", None, 1, args.serve_segments),
+            ("sustainable_preemptive_wait_capped", None, 1, args.serve_segments)]
     if args.serve_rate_high > 0:
         plan.insert(1, ("offered_high", args.serve_rate_high, 0, 1))
     sustained = None        # the sustainable runs share one set of queries and arrival times
@@ -602,7 +605,8 @@ def run_serving(eng, matrix, args):
         # ranges of a preemptive run queue at most one behind the running one
         run_depth = min(depth, 2) if segments > 1 else depth
         srv = Server(eng, db, max_batch_queries=max_batch, lanes=lanes, lane_depth=run_depth, schedule=sched,
-                     model=model, chunk_residues=1 << 20, admission=admission, segments=segments)
+                     model=model, chunk_residues=1 << 20, admission=admission, segments=segments,
+                     max_wait_ms=args.serve_max_wait_ms if label.endswith("wait_capped") else 0)
         digests = []
         n_check = min(n, args.serve_check)
         t0 = time.perf_counter()
@@ -623,6 +627,7 @@ def run_serving(eng, matrix, args):
             h.close()
         qres = float(sum(len(q) for q in qs))
         runs[label] = {"offered_qps": rate, "requests": n, "admission": ["arrival", "shortest"][admission],
+                       "max_wait_ms": args.serve_max_wait_ms if label.endswith("wait_capped") else 0,
                        "segments": segments, "lane_depth": run_depth,
                        "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
                        "max_ms": st["max_ms"], "throughput_qps": st["queries_per_s"],

@@ -51,7 +51,8 @@ class BpServerOptions(ctypes.Structure):
     _fields_ = [("max_batch_queries", i32), ("device_memory_budget", i64), ("chunk_residues", i32),
                 ("schedule", i32), ("lanes", i32), ("poll_us", i32), ("model", P),
                 ("cost_weights", ctypes.c_float * 3), ("planted_density", ctypes.c_float), ("params", BpParams),
-                ("lane_depth", i32), ("admission", i32), ("segments", i32)]
+                ("lane_depth", i32), ("admission", i32), ("segments", i32),
+                ("max_wait_ms", i32)]
 
 
 class BpServerMetrics(ctypes.Structure):

@@ -551,7 +551,7 @@ class Server:
     def __init__(self, engine: Engine, db: Database, max_batch_queries: int = 32, memory_budget: int = 16 << 30,
                  chunk_residues: int = 1 << 20, schedule: int = 0, lanes: int = 2, model=None,
                  planted_density: float = 0.0, params: BpParams | None = None, poll_us: int = 200,
-                 lane_depth: int = 1, admission: int = 0, segments: int = 1):
+                 lane_depth: int = 1, admission: int = 0, segments: int = 1, max_wait_ms: int = 0):
         o = BpServerOptions()
         lib().bp_server_options_default(ctypes.byref(o))
         o.max_batch_queries = max_batch_queries
@@ -562,6 +562,7 @@ class Server:
         o.lane_depth = lane_depth
         o.admission = admission
         o.segments = segments
+        o.max_wait_ms = max_wait_ms
         o.poll_us = poll_us
         if model is not None:
             o.model = model.mlp.h.value

@@ -259,7 +259,8 @@ std::deque<Req*>::iterator pick_pending(bp_server* s, int64_t extra) {
     auto oldest = s->pending.begin();
     if (oldest == s->pending.end()) return oldest;
     const int64_t room = s->o.device_memory_budget - s->mem_used - extra;
-    if (s->o.admission == BP_ADMIT_SHORTEST) {
+    const bool overdue = s->o.max_wait_ms > 0 && now_ms() - (*oldest)->t_arrive >= s->o.max_wait_ms;
+    if (s->o.admission == BP_ADMIT_SHORTEST && !overdue) {
         auto best = oldest;
         for (auto it = s->pending.begin(); it != s->pending.end(); ++it)
             if ((*it)->residues.size() < (*best)->residues.size()) best = it;
@@ -337,7 +338,8 @@ void retire_segmented(bp_server* s, Req* r) {
 }
 
 // Segment mode: the request whose next range a free slot takes -- the
-// earliest admitted, or the one with the least work left (ranges left x
+// earliest admitted, or (past max_wait_ms, the oldest waiting so long, else)
+// the one with the least work left (ranges left x
 // query length plus the per-letter-independent share of a scan, about 64
 // letters' worth), earliest among equals.
 Req* next_segment_request(bp_server* s) {
@@ -345,6 +347,13 @@ Req* next_segment_request(bp_server* s) {
     const int n_seg = (int)s->seg_first.size() - 1;
     Req* best = s->active.front();
     if (s->o.admission != BP_ADMIT_SHORTEST) return best;
+    if (s->o.max_wait_ms > 0) {
+        // a request waiting past the limit goes first, the oldest of them
+        Req* oldest = best;
+        for (Req* r : s->active)
+            if (r->t_arrive < oldest->t_arrive) oldest = r;
+        if (now_ms() - oldest->t_arrive >= s->o.max_wait_ms) return oldest;
+    }
     auto left = [n_seg](const Req* r) { return (double)(n_seg - r->seg_next) * ((double)r->residues.size() + 64.0); };
     for (Req* r : s->active)
         if (left(r) < left(best)) best = r;
@@ -552,6 +561,7 @@ void bp_server_options_default(bp_server_options* o) {
     o->lane_depth = 1;
     o->admission = BP_ADMIT_ARRIVAL;
     o->segments = 1;
+    o->max_wait_ms = 0;
     o->poll_us = 200;
     bp_params_default(&o->params);
 }
@@ -566,11 +576,11 @@ bp_status bp_server_create(bp_engine* e, const bp_db* db, const bp_server_option
     else bp_server_options_default(&s->o);
     if (s->o.lanes < 1 || s->o.lanes > 16 || s->o.max_batch_queries < 1 || s->o.lane_depth < 1 ||
         s->o.lane_depth > 16 || (s->o.admission != BP_ADMIT_ARRIVAL && s->o.admission != BP_ADMIT_SHORTEST) ||
-        s->o.segments < 1 || s->o.segments > 64) {
+        s->o.segments < 1 || s->o.segments > 64 || s->o.max_wait_ms < 0) {
         delete s;
         return bp_set_error(e, BP_ERR_INVALID,
                             "bp_server_create: lanes and lane_depth must be 1..16, max_batch_queries >= 1, "
-                            "segments 1..64");
+                            "segments 1..64, max_wait_ms >= 0");
     }
     if (s->o.segments > 1 && db->n > 0) {
         // consecutive subject ranges of about equal residues (empty ones dropped)

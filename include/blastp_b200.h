@@ -414,6 +414,9 @@ typedef struct {
                                        each range runs as the plain single-query search (as does,
                                        with one lane, any batch of one request).  Results are the
                                        same either way. */
+    int32_t max_wait_ms;            /* BP_ADMIT_SHORTEST: a request that has waited this long since
+                                       it arrived goes before shorter ones (oldest first), which
+                                       bounds how long long requests starve; 0 (default): never */
 } bp_server_options;
 
 enum { BP_ADMIT_ARRIVAL = 0, BP_ADMIT_SHORTEST = 1 };
