@@ -24,7 +24,7 @@
 //  * hits of one chunk on the same diagonal are applied in word-position
 //    order (__match_any_sync), the only order the state machine depends on;
 //    distinct diagonals are independent;
-//  * for queries of 200 letters and more, a hit pair that calls for an
+//  * for queries of 150 letters and more, a hit pair that calls for an
 //    extension does not stop the warp: it becomes a task and its diagonal is
 //    marked pending; later hits on a pending diagonal wait, in order, in a
 //    blocked list.  When the queue fills, or the subject ends, the warp walks
@@ -52,11 +52,13 @@ constexpr int kRow = 2 * kP + 1;
 constexpr int kMaxWarps = 32;
 constexpr int kTaskCap = 64;                // queued extensions per warp
 constexpr int kBlkCap = 64;                 // hits waiting behind queued extensions, per warp
-constexpr int kLaneWalkMin = 4;             // from this many queued extensions on, one lane walks each
+constexpr int kLaneWalkMin = 3;             // from this many queued extensions on, one lane walks each
 // Queries at least this long queue their extensions (kDefer); shorter ones
 // have too few extensions per subject for one-lane-per-extension walks to pay
-// for the queue, and extend each pair at once with the whole warp.
-constexpr int kDeferMinQlen = 200;
+// for the queue, and extend each pair at once with the whole warp (with the
+// score profile and rounds by rank, 160 aa: 3.65 -> 3.51 ms per 1M subjects
+// queued; 130 aa gains nothing).
+constexpr int kDeferMinQlen = 150;
 constexpr int kMaxMembers = 32;             // queries per packed table (BP_MAX_PACK_MEMBERS)
 // Diagonal arrays of at most this many entries use 16-bit entries.
 constexpr int kNarrowMaxL = 8192;
