@@ -52,7 +52,7 @@ constexpr int kRow = 2 * kP + 1;
 constexpr int kMaxWarps = 32;
 constexpr int kTaskCap = 64;                // queued extensions per warp
 constexpr int kBlkCap = 64;                 // hits waiting behind queued extensions, per warp
-constexpr int kLaneWalkMin = 3;             // from this many queued extensions on, one lane walks each
+constexpr int kLaneWalkMin = 2;             // from this many queued extensions on, one lane walks each
 // Queries at least this long queue their extensions (kDefer); shorter ones
 // have too few extensions per subject for one-lane-per-extension walks to pay
 // for the queue, and extend each pair at once with the whole warp (with the
